@@ -1,0 +1,87 @@
+"""ctypes binding of libtlr_b200.so (the C ABI declared in include/tlr_b200.h).
+
+The shared library is built in-tree (``python -m adaptive_tlr_pilots_b200.build`` or
+``__graft_entry__.build()``).  There is no fallback: when the library is missing or no CUDA
+device is present, :func:`lib` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtlr_b200.so")
+
+TLR_RULE_FIXED = 0
+TLR_RULE_ADAPTIVE = 1
+
+_lib = None
+
+
+class TlrInfo(ctypes.Structure):
+    _fields_ = [
+        ("completed", ctypes.c_int),
+        ("failed_at", ctypes.c_int),
+        ("stored_sigma", ctypes.c_longlong),
+        ("max_rank_sigma", ctypes.c_int),
+        ("stored_factor", ctypes.c_longlong),
+        ("mean_rank_factor", ctypes.c_double),
+        ("max_rank_factor", ctypes.c_int),
+        ("logdet", ctypes.c_double),
+        ("quad", ctypes.c_double),
+    ]
+
+
+# name -> (restype, argtypes); every symbol declared in include/tlr_b200.h
+SIGNATURES = {
+    "tlr_plan_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_void_p]),
+    "tlr_plan_destroy": (None, [ctypes.c_void_p]),
+    "tlr_morton_order": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                        ctypes.c_void_p]),
+    "tlr_set_data": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "tlr_loglik": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_double,
+                                  ctypes.POINTER(ctypes.c_double), ctypes.POINTER(TlrInfo),
+                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "tlr_loglik_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_double,
+                                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(TlrInfo),
+                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "tlr_get_diag_tile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "tlr_get_offdiag_tile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    "tlr_last_error": (ctypes.c_char_p, []),
+}
+
+
+def load(path: str = LIB_PATH):
+    """Load the shared library and declare its signatures (no GPU needed)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"the CUDA extension {path} is not built; run adaptive_tlr_pilots_b200.build.build()")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    return load().tlr_last_error().decode(errors="replace")
+
+
+class TlrError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"tlr error {code}: {msg}")
+        self.code = code
+
+
+def check(rc: int) -> int:
+    """Raise on rc < 0 (errors); return rc otherwise (0 or the not-PD code k + 1)."""
+    if rc < 0:
+        raise TlrError(rc, last_error())
+    return rc

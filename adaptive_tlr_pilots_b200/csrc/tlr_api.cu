@@ -1,0 +1,417 @@
+// Plan management and the extern "C" entry points declared in include/tlr_b200.h.
+//
+// One evaluation of the log-likelihood is a fixed sequence of kernel launches on the plan's
+// stream (no host synchronisation inside): chunked initial compression with on-device sketch
+// escalation, then nB factorization steps, then one reduction.  The host reads the result
+// (loglik, status, ranks) once at the end.
+#include "../../include/tlr_b200.h"
+#include "tlr_kernels.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+int cuda_check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return 0;
+  return fail(TLR_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+constexpr int kLevels = 4;      // sketch widths 16, 32, 64, 128
+constexpr int kMaxK = 128;
+constexpr int kPowerPasses = 4;  // Z = T^T T P passes per level
+constexpr int kMargin = 8;       // accepted rank must leave k - margin unresolved directions
+
+}  // namespace
+
+struct tlr_plan {
+  int n = 0, b = 0, nB = 0, ntiles = 0, cap = 0, device = 0;
+  cudaStream_t stream = nullptr;
+  bool has_data = false;
+  // data
+  double *xy = nullptr, *y = nullptr, *rhs = nullptr, *z = nullptr;
+  // factor
+  double *D = nullptr, *U = nullptr, *V = nullptr, *Wd = nullptr;
+  int *rank = nullptr, *rank0 = nullptr, *ti = nullptr, *tj = nullptr;
+  // compression chunk
+  int chunk = 0, nblk = 0;
+  int* need = nullptr;
+  double *T = nullptr, *P = nullptr, *Z = nullptr, *C = nullptr, *gscr = nullptr, *gsv = nullptr;
+  double *parts = nullptr, *fparts = nullptr;
+  // recompression scratch
+  int nslots = 0;
+  size_t slot_doubles = 0;
+  double* rcs = nullptr;
+  // results
+  double *ldpart = nullptr, *qpart = nullptr, *out = nullptr;
+  int* status = nullptr;
+  // host copies
+  std::vector<int> h_rank, h_rank0, h_ti, h_tj;
+  std::vector<void*> allocs;
+};
+
+namespace {
+
+template <class T>
+int dalloc(tlr_plan* p, T** ptr, size_t count) {
+  void* q = nullptr;
+  const cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(TLR_ERR_NOMEM, std::string("cudaMalloc of ") + std::to_string(count * sizeof(T)) +
+                                   " bytes failed: " + cudaGetErrorString(e));
+  }
+  p->allocs.push_back(q);
+  *ptr = static_cast<T*>(q);
+  return 0;
+}
+
+void free_all(tlr_plan* p) {
+  for (void* q : p->allocs) cudaFree(q);
+  p->allocs.clear();
+}
+
+#define TRY(x)                      \
+  do {                              \
+    const int _rc = (x);            \
+    if (_rc != 0) return _rc;       \
+  } while (0)
+
+#define TRYK(x)                                                                   \
+  do {                                                                            \
+    const int _rc = (x);                                                          \
+    if (_rc != 0) return fail(TLR_ERR_CUDA, std::string("kernel launch failed: ") + \
+                                                cudaGetErrorString((cudaError_t)_rc)); \
+  } while (0)
+
+int run_compression(tlr_plan* p, double sigma2, double inv_range, int rule_fixed, double thr_rel,
+                    double thr_abs) {
+  cudaStream_t s = p->stream;
+  const int ldp = kMaxK;
+  for (int base = 0; base < p->ntiles; base += p->chunk) {
+    const int nc = std::min(p->chunk, p->ntiles - base);
+    TRYK(tlr::launch_fill_int(p->need, 1, nc, s));
+    TRYK(tlr::launch_gen_offdiag(p->xy, p->n, p->b, base, p->ti, p->tj, p->T, nc, sigma2, inv_range, p->status, s));
+    for (int lev = 0; lev < kLevels; ++lev) {
+      const int k = 16 << lev;
+      double* Pp = p->P;
+      double* Zp = p->Z;
+      for (int it = 0; it < kPowerPasses; ++it) {
+        TRYK(tlr::launch_sketch(p->T, p->n, p->b, k, base, p->ti, p->tj, p->need, Pp, Zp, ldp, it == 0 ? 1 : 0, 0,
+                                nc, p->status, s));
+        TRYK(tlr::launch_orth(Zp, p->n, p->b, k, ldp, base, p->tj, p->need, p->gscr, nc, p->status, s));
+        std::swap(Pp, Zp);
+      }
+      TRYK(tlr::launch_sketch(p->T, p->n, p->b, k, base, p->ti, p->tj, p->need, Pp, p->C, ldp, 0, 1, nc, p->status,
+                              s));
+      TRYK(tlr::launch_resid(p->T, p->n, p->b, k, ldp, base, p->ti, p->tj, p->need, Pp, p->C, p->parts, p->fparts,
+                             p->nblk, nc, p->status, s));
+      TRYK(tlr::launch_finalize(p->n, p->b, k, ldp, p->cap, kMargin, rule_fixed, thr_rel, thr_abs, base, p->ti,
+                                p->tj, p->need, Pp, p->C, p->parts, p->fparts, p->nblk, p->gscr, p->gsv, p->U, p->V,
+                                p->rank, lev == kLevels - 1 ? 1 : 0, nc, p->status, s));
+    }
+  }
+  return 0;
+}
+
+int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugget, int rule_fixed, double thr_rel,
+                      double thr_abs) {
+  cudaStream_t s = p->stream;
+  for (int k = 0; k < p->nB; ++k) {
+    TRYK(tlr::launch_diag_build(p->xy, p->n, p->b, k, sigma2, inv_range, nugget, p->U, p->Wd, p->rank, p->cap, p->D,
+                                p->status, s));
+    TRYK(tlr::launch_potrf(p->D, p->n, p->b, k, p->rhs, p->z, p->ldpart, p->qpart, p->status, s));
+    TRYK(tlr::launch_trsm(p->D, p->n, p->b, k, p->nB, p->U, p->V, p->Wd, p->rank, p->cap, p->z, p->rhs, p->status, s));
+    TRYK(tlr::launch_recompress(p->n, p->b, k, p->nB, p->U, p->V, p->rank, p->cap, rule_fixed, thr_rel, thr_abs,
+                                p->rcs, p->slot_doubles, p->nslots, p->status, s));
+  }
+  TRYK(tlr::launch_finish(p->nB, p->n, p->ldpart, p->qpart, p->out, p->status, s));
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* tlr_last_error(void) { return g_err.c_str(); }
+
+int tlr_plan_create(tlr_plan** plan, int n, int b, int cap, int device, void* stream) {
+  if (!plan) return fail(TLR_ERR_ARG, "plan is NULL");
+  *plan = nullptr;
+  if (n < 1 || b < 1) return fail(TLR_ERR_ARG, "n and b must be positive");
+  if (b > 1024) return fail(TLR_ERR_ARG, "tile size b must be <= 1024");
+  if (cap < 1 || cap > 128) return fail(TLR_ERR_ARG, "rank capacity must be in [1, 128]");
+  TRY(cuda_check(cudaSetDevice(device), "cudaSetDevice"));
+  tlr_plan* p = new tlr_plan();
+  p->n = n;
+  p->b = b;
+  p->nB = (n + b - 1) / b;
+  p->ntiles = p->nB * (p->nB - 1) / 2;
+  p->cap = cap;
+  p->device = device;
+  p->stream = static_cast<cudaStream_t>(stream);
+  const size_t N = (size_t)n, B = (size_t)b;
+  int rc = 0;
+  auto A = [&](int r) {
+    if (rc == 0 && r != 0) rc = r;
+  };
+  A(dalloc(p, &p->xy, 2 * N));
+  A(dalloc(p, &p->y, N));
+  A(dalloc(p, &p->rhs, (size_t)p->nB * B));
+  A(dalloc(p, &p->z, (size_t)p->nB * B));
+  A(dalloc(p, &p->D, (size_t)p->nB * B * B));
+  const size_t nt = std::max(p->ntiles, 1);
+  A(dalloc(p, &p->U, nt * B * cap));
+  A(dalloc(p, &p->V, nt * B * cap));
+  A(dalloc(p, &p->Wd, nt * (size_t)cap * cap));
+  A(dalloc(p, &p->rank, nt));
+  A(dalloc(p, &p->rank0, nt));
+  A(dalloc(p, &p->ti, nt));
+  A(dalloc(p, &p->tj, nt));
+  // compression chunk: bounded so T + panels stay within ~4 GB
+  const size_t per_tile = (B * B + 4 * B * kMaxK + 2 * (size_t)kMaxK * kMaxK) * 8;
+  p->chunk = (int)std::max<size_t>(1, std::min<size_t>(nt, (size_t)4 * 1024 * 1024 * 1024 / per_tile));
+  p->nblk = (b + 63) / 64;
+  const size_t ch = (size_t)p->chunk;
+  A(dalloc(p, &p->need, ch));
+  A(dalloc(p, &p->T, ch * B * B));
+  A(dalloc(p, &p->P, ch * B * kMaxK));
+  A(dalloc(p, &p->Z, ch * B * kMaxK));
+  A(dalloc(p, &p->C, ch * B * kMaxK));
+  A(dalloc(p, &p->gscr, ch * B * kMaxK));
+  A(dalloc(p, &p->gsv, ch * 2 * (size_t)kMaxK * kMaxK));
+  A(dalloc(p, &p->parts, ch * p->nblk));
+  A(dalloc(p, &p->fparts, ch * p->nblk));
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  p->nslots = nsm * 4;
+  p->slot_doubles = tlr::rc_slot_doubles(b, cap);
+  A(dalloc(p, &p->rcs, (size_t)p->nslots * p->slot_doubles));
+  A(dalloc(p, &p->ldpart, (size_t)p->nB));
+  A(dalloc(p, &p->qpart, (size_t)p->nB));
+  A(dalloc(p, &p->out, 4));
+  A(dalloc(p, &p->status, 1));
+  if (rc != 0) {
+    free_all(p);
+    delete p;
+    return rc;
+  }
+  // tile index tables: t = i (i - 1) / 2 + j
+  p->h_ti.resize(nt);
+  p->h_tj.resize(nt);
+  for (int i = 0; i < p->nB; ++i)
+    for (int j = 0; j < i; ++j) {
+      const int t = i * (i - 1) / 2 + j;
+      p->h_ti[t] = i;
+      p->h_tj[t] = j;
+    }
+  if (p->ntiles > 0) {
+    rc = cuda_check(cudaMemcpy(p->ti, p->h_ti.data(), sizeof(int) * p->ntiles, cudaMemcpyHostToDevice), "copy ti");
+    if (!rc) rc = cuda_check(cudaMemcpy(p->tj, p->h_tj.data(), sizeof(int) * p->ntiles, cudaMemcpyHostToDevice), "copy tj");
+  }
+  if (rc != 0) {
+    free_all(p);
+    delete p;
+    return rc;
+  }
+  p->h_rank.resize(nt);
+  p->h_rank0.resize(nt);
+  *plan = p;
+  return 0;
+}
+
+void tlr_plan_destroy(tlr_plan* plan) {
+  if (!plan) return;
+  cudaSetDevice(plan->device);
+  if (plan->stream) cudaStreamSynchronize(plan->stream);
+  free_all(plan);
+  delete plan;
+}
+
+int tlr_morton_order(const double* xy_dev, int n, int order, long long* perm_dev, void* stream) {
+  if (n < 1 || !xy_dev || !perm_dev) return fail(TLR_ERR_ARG, "invalid arguments to tlr_morton_order");
+  if (order < 1 || order > 12) return fail(TLR_ERR_ARG, "order must be in [1, 12]");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t nbuckets = (size_t)1 << (2 * order);
+  unsigned *keys = nullptr, *cnt = nullptr, *off = nullptr, *cur = nullptr;
+  cudaError_t e = cudaMallocAsync(&keys, sizeof(unsigned) * n, s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&cnt, sizeof(unsigned) * nbuckets, s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&off, sizeof(unsigned) * nbuckets, s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&cur, sizeof(unsigned) * nbuckets, s);
+  int rc = 0;
+  if (e != cudaSuccess) rc = fail(TLR_ERR_NOMEM, std::string("morton scratch: ") + cudaGetErrorString(e));
+  if (!rc) {
+    const int lr = tlr::launch_morton(xy_dev, n, order, keys, cnt, off, cur, perm_dev, s);
+    if (lr) rc = fail(TLR_ERR_CUDA, std::string("morton launch: ") + cudaGetErrorString((cudaError_t)lr));
+  }
+  if (keys) cudaFreeAsync(keys, s);
+  if (cnt) cudaFreeAsync(cnt, s);
+  if (off) cudaFreeAsync(off, s);
+  if (cur) cudaFreeAsync(cur, s);
+  if (!rc) rc = cuda_check(cudaStreamSynchronize(s), "morton sync");
+  return rc;
+}
+
+int tlr_set_data(tlr_plan* p, const double* xy_dev, const double* y_dev) {
+  if (!p || !xy_dev || !y_dev) return fail(TLR_ERR_ARG, "invalid arguments to tlr_set_data");
+  TRY(cuda_check(cudaSetDevice(p->device), "cudaSetDevice"));
+  TRY(cuda_check(cudaMemcpyAsync(p->xy, xy_dev, sizeof(double) * 2 * p->n, cudaMemcpyDeviceToDevice, p->stream),
+                 "copy sites"));
+  TRY(cuda_check(cudaMemcpyAsync(p->y, y_dev, sizeof(double) * p->n, cudaMemcpyDeviceToDevice, p->stream),
+                 "copy observations"));
+  p->has_data = true;
+  return 0;
+}
+
+static void fill_info(const tlr_plan* p, int status, const double* out, tlr_info* info, int* factor_ranks,
+                      int* sigma_ranks) {
+  const int nB = p->nB, b = p->b, n = p->n;
+  auto bsz = [&](int i) { return std::min(b, n - i * b); };
+  long long stored0 = 0;
+  int maxr0 = 0;
+  for (int i = 0; i < nB; ++i) {
+    stored0 += (long long)bsz(i) * bsz(i);
+    for (int j = 0; j < i; ++j) {
+      const int r = p->h_rank0[i * (i - 1) / 2 + j];
+      stored0 += 2LL * r * std::max(bsz(i), bsz(j));
+      maxr0 = std::max(maxr0, r);
+    }
+  }
+  if (sigma_ranks) {
+    int q = 0;
+    for (int i = 0; i < nB; ++i)
+      for (int j = 0; j < i; ++j) sigma_ranks[q++] = p->h_rank0[i * (i - 1) / 2 + j];
+  }
+  if (info) {
+    std::memset(info, 0, sizeof(*info));
+    info->stored_sigma = stored0;
+    info->max_rank_sigma = maxr0;
+    info->completed = status == 0 ? 1 : 0;
+    info->failed_at = status > 0 ? status - 1 : -1;
+  }
+  if (status != 0) return;
+  long long stored = 0;
+  long long rsum = 0;
+  int rmax = 0, cnt = 0, q = 0;
+  for (int k = 0; k < nB; ++k) stored += (long long)bsz(k) * bsz(k);
+  for (int k = 0; k < nB; ++k)
+    for (int i = k + 1; i < nB; ++i) {
+      const int r = p->h_rank[i * (i - 1) / 2 + k];
+      stored += 2LL * r * bsz(i);
+      rsum += r;
+      rmax = std::max(rmax, r);
+      ++cnt;
+      if (factor_ranks) factor_ranks[q++] = r;
+    }
+  if (info) {
+    info->stored_factor = stored;
+    info->mean_rank_factor = cnt ? (double)rsum / cnt : 0.0;
+    info->max_rank_factor = rmax;
+    info->logdet = out[1];
+    info->quad = out[2];
+  }
+}
+
+int tlr_loglik(tlr_plan* p, const double theta[3], int rule, double value, double* loglik, tlr_info* info,
+               int* factor_ranks, int* sigma_ranks) {
+  if (!p || !theta) return fail(TLR_ERR_ARG, "invalid arguments to tlr_loglik");
+  if (!p->has_data) return fail(TLR_ERR_NOT_READY, "tlr_set_data has not been called");
+  if (rule != TLR_RULE_FIXED && rule != TLR_RULE_ADAPTIVE) return fail(TLR_ERR_ARG, "rule must be fixed or adaptive");
+  const double sigma2 = theta[0], range = theta[1], eta = theta[2];
+  if (!(range > 0.0) || !std::isfinite(sigma2) || !std::isfinite(eta) || !std::isfinite(range))
+    return fail(TLR_ERR_ARG, "theta must be finite with range > 0");
+  TRY(cuda_check(cudaSetDevice(p->device), "cudaSetDevice"));
+  cudaStream_t s = p->stream;
+  // thresholds: codes/17_tlr_cholesky_pilot.py:143-150 (b = largest tile = b)
+  const int rule_fixed = rule == TLR_RULE_FIXED;
+  const double thr_rel = rule_fixed ? value : 0.0;
+  const double thr_abs = rule_fixed ? 0.0 : value * (double)std::min(p->b, p->n) * sigma2 * eta / (double)p->n;
+  TRY(cuda_check(cudaMemsetAsync(p->status, 0, sizeof(int), s), "reset status"));
+  TRY(cuda_check(cudaMemsetAsync(p->rank, 0, sizeof(int) * std::max(p->ntiles, 1), s), "reset ranks"));
+  TRY(cuda_check(cudaMemcpyAsync(p->rhs, p->y, sizeof(double) * p->n, cudaMemcpyDeviceToDevice, s), "rhs"));
+  TRY(run_compression(p, sigma2, 1.0 / range, rule_fixed, thr_rel, thr_abs));
+  if (p->ntiles > 0)
+    TRY(cuda_check(cudaMemcpyAsync(p->rank0, p->rank, sizeof(int) * p->ntiles, cudaMemcpyDeviceToDevice, s),
+                   "rank0"));
+  TRY(run_factorization(p, sigma2, 1.0 / range, sigma2 * eta, rule_fixed, thr_rel, thr_abs));
+  int status = 0;
+  double out[4] = {0, 0, 0, 0};
+  TRY(cuda_check(cudaMemcpyAsync(&status, p->status, sizeof(int), cudaMemcpyDeviceToHost, s), "status"));
+  TRY(cuda_check(cudaMemcpyAsync(out, p->out, sizeof(double) * 3, cudaMemcpyDeviceToHost, s), "out"));
+  if (p->ntiles > 0) {
+    TRY(cuda_check(cudaMemcpyAsync(p->h_rank.data(), p->rank, sizeof(int) * p->ntiles, cudaMemcpyDeviceToHost, s),
+                   "ranks"));
+    TRY(cuda_check(cudaMemcpyAsync(p->h_rank0.data(), p->rank0, sizeof(int) * p->ntiles, cudaMemcpyDeviceToHost, s),
+                   "ranks0"));
+  }
+  TRY(cuda_check(cudaStreamSynchronize(s), "evaluation"));
+  if (status < 0) {
+    const char* why = status == TLR_ERR_RANK_CAP ? "a tile rank exceeded the plan's rank capacity"
+                      : status == TLR_ERR_COMPRESS ? "a tile needed more than 120 singular directions"
+                                                   : "device error";
+    return fail(status, why);
+  }
+  fill_info(p, status, out, info, factor_ranks, sigma_ranks);
+  if (loglik) *loglik = status == 0 ? out[0] : NAN;
+  return status;
+}
+
+int tlr_loglik_host(tlr_plan* p, const double* xy_host, const double* y_host, const double theta[3], int rule,
+                    double value, double* loglik, tlr_info* info, int* factor_ranks, int* sigma_ranks) {
+  if (!p || !xy_host || !y_host) return fail(TLR_ERR_ARG, "invalid arguments to tlr_loglik_host");
+  TRY(cuda_check(cudaSetDevice(p->device), "cudaSetDevice"));
+  TRY(cuda_check(cudaMemcpyAsync(p->xy, xy_host, sizeof(double) * 2 * p->n, cudaMemcpyHostToDevice, p->stream),
+                 "copy sites"));
+  TRY(cuda_check(cudaMemcpyAsync(p->y, y_host, sizeof(double) * p->n, cudaMemcpyHostToDevice, p->stream),
+                 "copy observations"));
+  p->has_data = true;
+  return tlr_loglik(p, theta, rule, value, loglik, info, factor_ranks, sigma_ranks);
+}
+
+int tlr_get_diag_tile(tlr_plan* p, int k, double* out_host) {
+  if (!p || !out_host || k < 0 || k >= p->nB) return fail(TLR_ERR_ARG, "invalid arguments to tlr_get_diag_tile");
+  const int bk = std::min(p->b, p->n - k * p->b);
+  std::vector<double> tmp((size_t)p->b * p->b);
+  TRY(cuda_check(cudaMemcpyAsync(tmp.data(), p->D + (size_t)k * p->b * p->b, sizeof(double) * p->b * p->b,
+                                 cudaMemcpyDeviceToHost, p->stream),
+                 "copy diag"));
+  TRY(cuda_check(cudaStreamSynchronize(p->stream), "sync"));
+  for (int c = 0; c < bk; ++c)
+    for (int a = 0; a < bk; ++a) out_host[(size_t)c * bk + a] = a >= c ? tmp[(size_t)c * p->b + a] : 0.0;
+  return 0;
+}
+
+int tlr_get_offdiag_tile(tlr_plan* p, int i, int j, double* u_host, double* v_host, int* rank) {
+  if (!p || i <= j || j < 0 || i >= p->nB) return fail(TLR_ERR_ARG, "invalid tile index");
+  const int t = i * (i - 1) / 2 + j;
+  int r = 0;
+  TRY(cuda_check(cudaMemcpyAsync(&r, p->rank + t, sizeof(int), cudaMemcpyDeviceToHost, p->stream), "rank"));
+  TRY(cuda_check(cudaStreamSynchronize(p->stream), "sync"));
+  if (rank) *rank = r;
+  const int bi = std::min(p->b, p->n - i * p->b), bj = std::min(p->b, p->n - j * p->b);
+  std::vector<double> tu((size_t)p->b * p->cap), tv((size_t)p->b * p->cap);
+  TRY(cuda_check(cudaMemcpyAsync(tu.data(), p->U + (size_t)t * p->b * p->cap, sizeof(double) * p->b * p->cap,
+                                 cudaMemcpyDeviceToHost, p->stream), "copy U"));
+  TRY(cuda_check(cudaMemcpyAsync(tv.data(), p->V + (size_t)t * p->b * p->cap, sizeof(double) * p->b * p->cap,
+                                 cudaMemcpyDeviceToHost, p->stream), "copy V"));
+  TRY(cuda_check(cudaStreamSynchronize(p->stream), "sync"));
+  for (int c = 0; c < r; ++c) {
+    if (u_host)
+      for (int a = 0; a < bi; ++a) u_host[(size_t)c * bi + a] = tu[(size_t)c * p->b + a];
+    if (v_host)
+      for (int a = 0; a < bj; ++a) v_host[(size_t)c * bj + a] = tv[(size_t)c * p->b + a];
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,389 @@
+// Initial compression of the off-diagonal covariance tiles (FP64 parity path).
+//
+// Reference: codes/17_tlr_cholesky_pilot.py:151-166 (tile generation) and 107-116
+// (truncate_svd: full SVD of every b x b tile, rank = smallest r with tail[r] <= threshold).
+//
+// B200 design.  A full b x b SVD per tile is O(b^3) and is where the reference spends
+// 54-66% of its time.  Here each tile goes through a batched randomized range finder
+// whose rank decision is exact to rounding:
+//   T        generated once per chunk from the Morton-ordered coordinates (row-major, HBM);
+//   Z = T^T (T P) four times, each followed by a Householder orthonormalisation (P <- Q(Z));
+//   C = T P, rho^2 = ||T - C P^T||_F^2 computed element by element (no cancellation);
+//   R_C from a Householder QR of C, one-sided Jacobi SVD of R_C -> sigma, W;
+//   tail[r]^2 = rho^2 + sum_{t>=r} sigma_t^2 (same accumulation order as the reference);
+//   the rank is accepted when r <= k - margin, so the unresolved directions lie far below
+//   the threshold; otherwise the tile is redone with k doubled (16, 32, 64, 128).
+// The truncated pair is U = C W_r (= Q_C U_w Sigma_r), V = P W_r, so U has orthogonal
+// columns and V orthonormal columns, exactly the structure of the reference's U*s, Vt^T.
+#include "tlr_device.cuh"
+#include "tlr_kernels.h"
+
+namespace tlr {
+
+__device__ __forceinline__ double omega_entry(uint32_t tile, uint32_t row, uint32_t col) {
+  // splitmix64 (Steele, Lea, Flood 2014) on (tile, row, col): a fixed, reproducible test matrix
+  uint64_t x = ((uint64_t)tile << 42) ^ ((uint64_t)row << 21) ^ (uint64_t)col;
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  x ^= x >> 31;
+  return (double)(x >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+// ----------------------------------------------------------------------------------------
+// T[c] = sigma2 * matern32(dist(S_i, S_j)), row-major with leading dimension b.
+__global__ void k_gen_offdiag(const double* TLR_RESTRICT xy, int n, int b, int tile_base,
+                              const int* TLR_RESTRICT ti, const int* TLR_RESTRICT tj, double* TLR_RESTRICT T,
+                              double sigma2, double inv_range, const int* TLR_RESTRICT status) {
+  if (*status != 0) return;
+  const int c = blockIdx.y;
+  const int t = (tile_base + c);
+  const int i = ti[t], j = tj[t];
+  const int i0 = i * b, j0 = j * b;
+  const int bi = min(b, n - i0), bj = min(b, n - j0);
+  double* Tc = T + (size_t)c * b * b;
+  const int total = bi * bj;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    const int a = e / bj, q = e - a * bj;
+    const double2 pa = reinterpret_cast<const double2*>(xy)[i0 + a];
+    const double2 pq = reinterpret_cast<const double2*>(xy)[j0 + q];
+    Tc[(size_t)a * b + q] = matern32_cov(pa.x, pa.y, pq.x, pq.y, sigma2, inv_range);
+  }
+}
+
+// ----------------------------------------------------------------------------------------
+// Strip-wise products with a 16-column block of P held in shared memory.
+//   mode 0: Z[:, g] = T^T (T P[:, g])          (range-finder sketch)
+//   mode 1: C[:, g] = T P[:, g]                 (projection)
+// P is Omega (generated) when omega != 0.  One CTA of 256 threads per (tile, column group).
+template <int H, int ZR>
+__global__ void __launch_bounds__(256) k_sketch(const double* TLR_RESTRICT T, int n, int b, int kcols,
+                                               int tile_base, const int* TLR_RESTRICT ti,
+                                               const int* TLR_RESTRICT tj, const int* TLR_RESTRICT need,
+                                               const double* TLR_RESTRICT P, double* TLR_RESTRICT out,
+                                               int ldp, int omega, int mode, const int* TLR_RESTRICT status) {
+  if (*status != 0) return;
+  const int c = blockIdx.x, g = blockIdx.y;
+  if (!need[c]) return;
+  const int t = (tile_base + c);
+  const int bi = min(b, n - ti[t] * b), bj = min(b, n - tj[t] * b);
+  extern __shared__ double smem[];
+  double* Ps = smem;                       // [bj][16]
+  double* Ts = Ps + (size_t)b * 16;        // [H][b + 1]
+  double* red = Ts + (size_t)H * (b + 1);  // [KS][H][16]
+  double* Ys = red + 256 * 4;              // [H][16]
+  const int ldt = b + 1;
+  const double* Tc = T + (size_t)c * b * b;
+  const size_t pbase = (size_t)c * b * ldp;
+
+  for (int e = threadIdx.x; e < bj * 16; e += 256) {
+    const int row = e >> 4, q = e & 15;
+    Ps[e] = omega ? omega_entry((uint32_t)t, (uint32_t)row, (uint32_t)(g * 16 + q))
+                  : P[pbase + (size_t)(g * 16 + q) * b + row];
+  }
+  constexpr int BLK = (H / 2) * 8;  // 2x2 register blocks per K slice
+  constexpr int KS = 256 / BLK;     // K slices
+  const int ks = threadIdx.x / BLK, loc = threadIdx.x % BLK;
+  const int rp = loc >> 3, cp = loc & 7;
+
+  double zacc[ZR][16];
+#pragma unroll
+  for (int m = 0; m < ZR; ++m)
+#pragma unroll
+    for (int q = 0; q < 16; ++q) zacc[m][q] = 0.0;
+
+  for (int a0 = 0; a0 < bi; a0 += H) {
+    const int hrows = min(H, bi - a0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < H * bj; e += 256) {
+      const int r = e / bj, q = e - r * bj;
+      Ts[r * ldt + q] = (r < hrows) ? Tc[(size_t)(a0 + r) * b + q] : 0.0;
+    }
+    __syncthreads();
+    // phase A: Y = T_s P (H x 16), 2x2 blocks, K split in KS interleaved slices
+    double y00 = 0.0, y01 = 0.0, y10 = 0.0, y11 = 0.0;
+    const double* t0 = Ts + (2 * rp) * ldt;
+    const double* t1 = t0 + ldt;
+    for (int q = ks; q < bj; q += KS) {
+      const double2 pv = *reinterpret_cast<const double2*>(Ps + q * 16 + 2 * cp);
+      const double a = t0[q], bb = t1[q];
+      y00 = fma(a, pv.x, y00); y01 = fma(a, pv.y, y01);
+      y10 = fma(bb, pv.x, y10); y11 = fma(bb, pv.y, y11);
+    }
+    double* rd = red + ks * (H * 16);
+    rd[(2 * rp) * 16 + 2 * cp] = y00; rd[(2 * rp) * 16 + 2 * cp + 1] = y01;
+    rd[(2 * rp + 1) * 16 + 2 * cp] = y10; rd[(2 * rp + 1) * 16 + 2 * cp + 1] = y11;
+    __syncthreads();
+    for (int e = threadIdx.x; e < H * 16; e += 256) {
+      double s = 0.0;
+#pragma unroll
+      for (int k2 = 0; k2 < KS; ++k2) s += red[k2 * (H * 16) + e];
+      Ys[e] = s;
+    }
+    __syncthreads();
+    if (mode == 1) {
+      // C rows a0.., column group g
+      for (int e = threadIdx.x; e < hrows * 16; e += 256) {
+        const int r = e >> 4, q = e & 15;
+        out[pbase + (size_t)(g * 16 + q) * b + a0 + r] = Ys[e];
+      }
+      continue;
+    }
+    // phase B: Z += T_s^T Y
+#pragma unroll
+    for (int m = 0; m < ZR; ++m) {
+      const int z = threadIdx.x + 256 * m;
+      if (z < bj) {
+        for (int r = 0; r < hrows; ++r) {
+          const double a = Ts[r * ldt + z];
+          const double2* yr = reinterpret_cast<const double2*>(Ys + r * 16);
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const double2 yv = yr[q];
+            zacc[m][2 * q] = fma(a, yv.x, zacc[m][2 * q]);
+            zacc[m][2 * q + 1] = fma(a, yv.y, zacc[m][2 * q + 1]);
+          }
+        }
+      }
+    }
+  }
+  if (mode == 0) {
+#pragma unroll
+    for (int m = 0; m < ZR; ++m) {
+      const int z = threadIdx.x + 256 * m;
+      if (z < bj)
+#pragma unroll
+        for (int q = 0; q < 16; ++q) out[pbase + (size_t)(g * 16 + q) * b + z] = zacc[m][q];
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------------------
+// P <- Q of the Householder QR of Z (bj x k); the panel is staged in shared memory.
+__global__ void __launch_bounds__(256) k_orth(double* TLR_RESTRICT Z, int n, int b, int k, int ldp,
+                                             int tile_base, const int* TLR_RESTRICT tj,
+                                             const int* TLR_RESTRICT need, double* TLR_RESTRICT gscratch,
+                                             int in_smem, const int* TLR_RESTRICT status) {
+  if (*status != 0) return;
+  const int c = blockIdx.x;
+  if (!need[c]) return;
+  const int bj = min(b, n - tj[(tile_base + c)] * b);
+  const int ke = min(k, bj);  // a tile narrower than k gets a full basis and zero columns
+  extern __shared__ double smem[];
+  double* red = smem;         // 33
+  double* tau = smem + 40;    // k
+  double* A = tau + 136;      // bj x k (ld bj) when it fits, else global scratch
+  const size_t pbase = (size_t)c * b * ldp;
+  double* W = in_smem ? A : gscratch + pbase;
+  for (int e = threadIdx.x; e < bj * ke; e += blockDim.x) {
+    const int row = e % bj, q = e / bj;
+    W[(size_t)q * bj + row] = Z[pbase + (size_t)q * b + row];
+  }
+  __syncthreads();
+  cta_geqr2(W, bj, bj, ke, tau, red);
+  cta_org2r(W, bj, bj, ke, tau);
+  for (int e = threadIdx.x; e < bj * k; e += blockDim.x) {
+    const int row = e % bj, q = e / bj;
+    Z[pbase + (size_t)q * b + row] = (q < ke) ? W[(size_t)q * bj + row] : 0.0;
+  }
+}
+
+// ----------------------------------------------------------------------------------------
+// Residual of the projection, per column block of 64: parts[c][blk] = sum (T - C P^T)^2 over
+// the block, fparts[c][blk] = sum T^2 over the block.  Element-wise, no cancellation.
+__global__ void __launch_bounds__(256) k_resid(const double* TLR_RESTRICT T, int n, int b, int k, int ldp,
+                                              int tile_base, const int* TLR_RESTRICT ti,
+                                              const int* TLR_RESTRICT tj, const int* TLR_RESTRICT need,
+                                              const double* TLR_RESTRICT P, const double* TLR_RESTRICT C,
+                                              double* TLR_RESTRICT parts, double* TLR_RESTRICT fparts,
+                                              int nblk, const int* TLR_RESTRICT status) {
+  if (*status != 0) return;
+  const int c = blockIdx.x, blk = blockIdx.y;
+  if (!need[c]) return;
+  const int t = (tile_base + c);
+  const int bi = min(b, n - ti[t] * b), bj = min(b, n - tj[t] * b);
+  const int q0 = blk * 64;
+  if (q0 >= bj) {
+    if (threadIdx.x == 0) { parts[c * nblk + blk] = 0.0; fparts[c * nblk + blk] = 0.0; }
+    return;
+  }
+  const int qn = min(64, bj - q0);
+  extern __shared__ double smem[];
+  double* Pb = smem;              // [64][k+1]  P rows q0..q0+63
+  double* Cs = Pb + 64 * (k + 1); // [16][k+1]  C rows of the strip
+  double* red = Cs + 16 * (k + 1);
+  const size_t pbase = (size_t)c * b * ldp;
+  for (int e = threadIdx.x; e < 64 * k; e += 256) {
+    const int r = e % 64, q = e / 64;
+    Pb[r * (k + 1) + q] = (r < qn) ? P[pbase + (size_t)q * b + q0 + r] : 0.0;
+  }
+  const double* Tc = T + (size_t)c * b * b;
+  double acc = 0.0, facc = 0.0;
+  const int col = threadIdx.x & 63, rsub = threadIdx.x >> 6;  // 4 row lanes x 64 columns
+  for (int a0 = 0; a0 < bi; a0 += 16) {
+    const int hrows = min(16, bi - a0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < 16 * k; e += 256) {
+      const int r = e % 16, q = e / 16;
+      Cs[r * (k + 1) + q] = (r < hrows) ? C[pbase + (size_t)q * b + a0 + r] : 0.0;
+    }
+    __syncthreads();
+    if (col < qn) {
+      for (int r = rsub; r < hrows; r += 4) {
+        const double tv = Tc[(size_t)(a0 + r) * b + q0 + col];
+        double s = tv;
+        const double* cr = Cs + r * (k + 1);
+        const double* pr = Pb + col * (k + 1);
+        for (int q = 0; q < k; ++q) s = fma(-cr[q], pr[q], s);
+        acc = fma(s, s, acc);
+        facc = fma(tv, tv, facc);
+      }
+    }
+  }
+  const double tot = block_sum(acc, red);
+  const double ftot = block_sum(facc, red);
+  if (threadIdx.x == 0) { parts[c * nblk + blk] = tot; fparts[c * nblk + blk] = ftot; }
+}
+
+// ----------------------------------------------------------------------------------------
+// Rank decision and output of the truncated pair for every tile still in need.
+__global__ void __launch_bounds__(256) k_finalize(int n, int b, int k, int ldp, int cap, int margin,
+                                                 int rule_fixed, double thr_rel, double thr_abs,
+                                                 int tile_base, const int* TLR_RESTRICT ti,
+                                                 const int* TLR_RESTRICT tj, int* TLR_RESTRICT need,
+                                                 const double* TLR_RESTRICT P, const double* TLR_RESTRICT C,
+                                                 const double* TLR_RESTRICT parts,
+                                                 const double* TLR_RESTRICT fparts, int nblk,
+                                                 double* TLR_RESTRICT gscratch, double* TLR_RESTRICT gsv,
+                                                 double* TLR_RESTRICT Uo,
+                                                 double* TLR_RESTRICT Vo, int* TLR_RESTRICT rank,
+                                                 int last_level, int* TLR_RESTRICT status) {
+  if (*status != 0) return;
+  const int c = blockIdx.x;
+  if (!need[c]) return;
+  const int t = (tile_base + c);
+  const int bi = min(b, n - ti[t] * b), bj = min(b, n - tj[t] * b);
+  extern __shared__ double smem[];
+  double* red = smem;             // 33 (+pad)
+  double* tau = smem + 40;        // k
+  double* sig = tau + 136;        // k
+  int* perm = reinterpret_cast<int*>(sig + 136);  // k
+  int* iflag = perm + 136;
+  int* rsel = iflag + 1;
+  double* M = (k <= 64) ? smem + 40 + 136 * 3 + 8 : gsv + (size_t)c * 2 * k * k;  // k x k
+  double* Vw = M + k * k;                                                             // k x k
+  const size_t pbase = (size_t)c * b * ldp;
+  double* W = gscratch + pbase;  // bi x k copy of C (ld b)
+  for (int e = threadIdx.x; e < bi * k; e += blockDim.x) {
+    const int row = e % bi, q = e / bi;
+    W[(size_t)q * b + row] = C[pbase + (size_t)q * b + row];
+  }
+  __syncthreads();
+  const int kk = min(k, bi);
+  cta_geqr2(W, b, bi, k, tau, red);
+  cta_copy_r(W, b, bi, k, M, k);
+  cta_jacobi_svd(M, k, k, k, Vw, k, sig, perm, iflag);
+  if (threadIdx.x == 0) {
+    double rho2 = 0.0, fro2 = 0.0;
+    for (int q = 0; q < nblk; ++q) { rho2 += parts[c * nblk + q]; fro2 += fparts[c * nblk + q]; }
+    double sorted[128];
+    for (int q = 0; q < k; ++q) sorted[q] = sig[perm[q]];
+    const double thr = rule_fixed ? thr_rel * sqrt(fro2) : thr_abs;
+    const int r = select_rank(sorted, k, rho2, thr, nullptr);
+    const bool exact = (k >= bj) || (k >= bi);
+    int out;
+    if (r >= 0 && (r <= k - margin || exact)) out = r;
+    else if (last_level) out = -2;  // compression limit reached
+    else out = -1;                  // redo with a larger k
+    if (out >= 0 && out > cap) out = -3;
+    *rsel = out;
+  }
+  __syncthreads();
+  const int r = *rsel;
+  (void)kk;
+  if (r == -1) return;
+  if (r < 0) {
+    if (threadIdx.x == 0) atomicCAS(status, 0, r == -2 ? -5 : -2);
+    return;
+  }
+  // U = C W_r, V = P W_r (columns in descending singular-value order)
+  double* Ut = Uo + (size_t)t * b * cap;
+  double* Vt = Vo + (size_t)t * b * cap;
+  for (int e = threadIdx.x; e < bi * r; e += blockDim.x) {
+    const int row = e % bi, q = e / bi;
+    const double* w = Vw + (size_t)perm[q] * k;
+    double s = 0.0;
+    for (int u = 0; u < k; ++u) s = fma(C[pbase + (size_t)u * b + row], w[u], s);
+    Ut[(size_t)q * b + row] = s;
+  }
+  for (int e = threadIdx.x; e < bj * r; e += blockDim.x) {
+    const int row = e % bj, q = e / bj;
+    const double* w = Vw + (size_t)perm[q] * k;
+    double s = 0.0;
+    for (int u = 0; u < k; ++u) s = fma(P[pbase + (size_t)u * b + row], w[u], s);
+    Vt[(size_t)q * b + row] = s;
+  }
+  if (threadIdx.x == 0) { rank[t] = r; need[c] = 0; }
+}
+
+// ----------------------------------------------------------------------------------------
+// launchers
+int launch_gen_offdiag(const double* xy, int n, int b, int tile_base, const int* ti, const int* tj,
+                       double* T, int nchunk, double sigma2, double inv_range, const int* status,
+                       cudaStream_t s) {
+  dim3 grid((unsigned)((b * b + 1023) / 1024), (unsigned)nchunk);
+  k_gen_offdiag<<<grid, 256, 0, s>>>(xy, n, b, tile_base, ti, tj, T, sigma2, inv_range, status);
+  return (int)cudaGetLastError();
+}
+
+static size_t sketch_smem(int b, int H) { return ((size_t)b * 16 + (size_t)H * (b + 1) + 256 * 4 + H * 16) * 8; }
+
+int launch_sketch(const double* T, int n, int b, int k, int tile_base, const int* ti, const int* tj,
+                  const int* need, const double* P, double* out, int ldp, int omega, int mode, int nchunk,
+                  const int* status, cudaStream_t s) {
+  dim3 grid((unsigned)nchunk, (unsigned)(k / 16));
+  if (b <= 512) {
+    const size_t sm = sketch_smem(b, 16);
+    cudaFuncSetAttribute(k_sketch<16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_sketch<16, 2><<<grid, 256, sm, s>>>(T, n, b, k, tile_base, ti, tj, need, P, out, ldp, omega, mode, status);
+  } else {
+    const size_t sm = sketch_smem(b, 8);
+    cudaFuncSetAttribute(k_sketch<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_sketch<8, 4><<<grid, 256, sm, s>>>(T, n, b, k, tile_base, ti, tj, need, P, out, ldp, omega, mode, status);
+  }
+  return (int)cudaGetLastError();
+}
+
+int launch_orth(double* Z, int n, int b, int k, int ldp, int tile_base, const int* tj, const int* need,
+                double* gscratch, int nchunk, const int* status, cudaStream_t s) {
+  size_t sm = (40 + 136) * 8;
+  const int in_smem = (size_t)b * k * 8 <= 160 * 1024;
+  if (in_smem) sm += (size_t)b * k * 8;
+  cudaFuncSetAttribute(k_orth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_orth<<<nchunk, 256, sm, s>>>(Z, n, b, k, ldp, tile_base, tj, need, gscratch, in_smem, status);
+  return (int)cudaGetLastError();
+}
+
+int launch_resid(const double* T, int n, int b, int k, int ldp, int tile_base, const int* ti, const int* tj,
+                 const int* need, const double* P, const double* C, double* parts, double* fparts, int nblk,
+                 int nchunk, const int* status, cudaStream_t s) {
+  const size_t sm = ((size_t)64 * (k + 1) + 16 * (k + 1) + 40) * 8;
+  cudaFuncSetAttribute(k_resid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  dim3 grid((unsigned)nchunk, (unsigned)nblk);
+  k_resid<<<grid, 256, sm, s>>>(T, n, b, k, ldp, tile_base, ti, tj, need, P, C, parts, fparts, nblk, status);
+  return (int)cudaGetLastError();
+}
+
+int launch_finalize(int n, int b, int k, int ldp, int cap, int margin, int rule_fixed, double thr_rel,
+                    double thr_abs, int tile_base, const int* ti, const int* tj, int* need, const double* P,
+                    const double* C, const double* parts, const double* fparts, int nblk, double* gscratch,
+                    double* gsv, double* U, double* V, int* rank, int last_level, int nchunk, int* status,
+                    cudaStream_t s) {
+  const size_t sm = (40 + 136 * 3 + 8 + (k <= 64 ? 2 * (size_t)k * k : 0)) * 8;
+  cudaFuncSetAttribute(k_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_finalize<<<nchunk, 256, sm, s>>>(n, b, k, ldp, cap, margin, rule_fixed, thr_rel, thr_abs, tile_base, ti, tj, need,
+                                     P, C, parts, fparts, nblk, gscratch, gsv, U, V, rank, last_level, status);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace tlr

@@ -1,0 +1,241 @@
+// Device-side building blocks shared by the TLR kernels (sm_100a, FP64).
+//
+// Everything here is cooperative at the CTA level unless named warp_*.  Routines take
+// generic pointers so the same code runs on shared or global (L2-resident) operands.
+// All reductions are deterministic (fixed shuffle/shared-memory order): a log-likelihood
+// evaluated twice on the same inputs is bit-identical.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#ifndef TLR_RESTRICT
+#define TLR_RESTRICT __restrict__
+#endif
+
+namespace tlr {
+
+constexpr double kSqrt3 = 1.7320508075688772935;
+
+// ---------------------------------------------------------------- reductions
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Sum over the CTA; every thread gets the result.  `red` needs 33 doubles of shared memory.
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    double s = lane < nw ? red[lane] : 0.0;
+    s = warp_sum(s);
+    if (lane == 0) red[32] = s;
+  }
+  __syncthreads();
+  return red[32];
+}
+
+// ---------------------------------------------------------------- covariance model
+// Matern nu=3/2 kernel sigma2 (1 + x) e^{-x}, x = sqrt(3) h / range
+// (codes/11_tlr_rank_rules.py:35-37 with the sigma2 scaling of codes/17_tlr_cholesky_pilot.py:161).
+__device__ __forceinline__ double matern32_cov(double ax, double ay, double bx, double by,
+                                               double sigma2, double inv_range) {
+  const double dx = ax - bx, dy = ay - by;
+  const double h = sqrt(fmax(dx * dx + dy * dy, 0.0));
+  const double x = kSqrt3 * h * inv_range;
+  return sigma2 * ((1.0 + x) * exp(-x));
+}
+
+// ---------------------------------------------------------------- rank rule
+// sig[0..m) sorted descending; extra2 = squared norm of what lies outside the represented
+// subspace.  tail[r] = sqrt(extra2 + sum_{t>=r} sig_t^2) accumulated from the smallest
+// value up (codes/17_tlr_cholesky_pilot.py:113).  Returns the smallest r with tail[r] <= thr,
+// or -1 when even tail[m] > thr.  Single thread.
+__device__ __forceinline__ int select_rank(const double* sig, int m, double extra2, double thr,
+                                           double* tail_at_rank) {
+  double acc = extra2;
+  int r = (sqrt(acc) <= thr) ? m : -1;
+  double tr = sqrt(acc);
+  for (int t = m - 1; t >= 0; --t) {
+    acc += sig[t] * sig[t];
+    const double tl = sqrt(acc);
+    if (tl <= thr) { r = t; tr = tl; }
+  }
+  if (tail_at_rank) *tail_at_rank = tr;
+  return r;
+}
+
+// ---------------------------------------------------------------- Householder QR
+// In-place Householder QR of the m x n column-major A (lda): R in the upper triangle,
+// reflector vectors below the diagonal (implicit unit leading entry), tau[0..n).
+// Same reflector convention as LAPACK dgeqr2/dlarfg.  One warp per trailing column.
+__device__ inline void cta_geqr2(double* A, int lda, int m, int n, double* tau, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int kmax = n < m ? n : m;
+  for (int c = 0; c < kmax; ++c) {
+    double* col = A + (size_t)c * lda;
+    double s = 0.0;
+    for (int t = c + 1 + threadIdx.x; t < m; t += blockDim.x) { const double x = col[t]; s += x * x; }
+    const double sig2 = block_sum(s, red);
+    const double alpha = col[c];
+    double beta, tc, scale;
+    if (sig2 == 0.0) { tc = 0.0; beta = alpha; scale = 1.0; }
+    else {
+      beta = -copysign(sqrt(alpha * alpha + sig2), alpha);
+      tc = (beta - alpha) / beta;
+      scale = 1.0 / (alpha - beta);
+    }
+    if (tc != 0.0)
+      for (int t = c + 1 + threadIdx.x; t < m; t += blockDim.x) col[t] *= scale;
+    __syncthreads();
+    for (int j = c + 1 + warp; j < n; j += nwarp) {
+      double* aj = A + (size_t)j * lda;
+      double w = 0.0;
+      for (int t = c + 1 + lane; t < m; t += 32) w += col[t] * aj[t];
+      w = (warp_sum(w) + aj[c]) * tc;
+      for (int t = c + 1 + lane; t < m; t += 32) aj[t] -= w * col[t];
+      __syncwarp();
+      if (lane == 0) aj[c] -= w;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) { col[c] = beta; tau[c] = tc; }
+    __syncthreads();
+  }
+  for (int c = kmax + threadIdx.x; c < n; c += blockDim.x) tau[c] = 0.0;
+  __syncthreads();
+}
+
+// Copy the upper-triangular R (n x n, or kmax rows) out of a factored A into Rout (ldr),
+// zeroing the strictly lower part.
+__device__ inline void cta_copy_r(const double* A, int lda, int m, int n, double* R, int ldr) {
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+    const int i = idx % n, j = idx / n;
+    R[(size_t)j * ldr + i] = (i <= j && i < m) ? A[(size_t)j * lda + i] : 0.0;
+  }
+  __syncthreads();
+}
+
+// Overwrite the factored A (reflectors + tau from cta_geqr2) with the explicit m x n Q
+// (LAPACK dorg2r order: backward accumulation).
+__device__ inline void cta_org2r(double* A, int lda, int m, int n, const double* tau) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int kmax = n < m ? n : m;
+  // columns beyond min(m, n) (only when n > m, not used here) become unit columns
+  for (int c = kmax - 1; c >= 0; --c) {
+    const double* v = A + (size_t)c * lda;
+    const double tc = tau[c];
+    if (c < n - 1 && tc != 0.0) {
+      for (int j = c + 1 + warp; j < n; j += nwarp) {
+        double* aj = A + (size_t)j * lda;
+        double w = 0.0;
+        for (int t = c + 1 + lane; t < m; t += 32) w += v[t] * aj[t];
+        w = (warp_sum(w) + aj[c]) * tc;
+        for (int t = c + 1 + lane; t < m; t += 32) aj[t] -= w * v[t];
+        __syncwarp();
+        if (lane == 0) aj[c] -= w;
+      }
+    }
+    __syncthreads();
+    double* ac = A + (size_t)c * lda;
+    for (int t = threadIdx.x; t < m; t += blockDim.x) {
+      if (t < c) ac[t] = 0.0;
+      else if (t == c) ac[t] = 1.0 - tc;
+      else ac[t] = -tc * ac[t];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- one-sided Jacobi SVD
+// Hestenes one-sided Jacobi on the m x n column-major M (ldm): on return M <- M V has
+// mutually orthogonal columns, V (n x n, ldv) holds the right singular vectors, sig[c] the
+// column norms (singular values, unsorted) and perm[0..n) the column order by descending
+// singular value (ties by index).  Round-robin parallel ordering, one warp per pair.
+// `iflag` needs one int of shared memory.  Returns the number of sweeps.
+__device__ inline int cta_jacobi_svd(double* M, int ldm, int m, int n, double* V, int ldv, double* sig,
+                              int* perm, int* iflag, int max_sweeps = 40) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+    const int i = idx % n, j = idx / n;
+    V[(size_t)j * ldv + i] = (i == j) ? 1.0 : 0.0;
+  }
+  const int np = (n + 1) & ~1;  // even number of players (one dummy when n is odd)
+  int sweep = 0;
+  if (n > 1) {
+    for (sweep = 0; sweep < max_sweeps; ++sweep) {
+      if (threadIdx.x == 0) *iflag = 0;
+      __syncthreads();
+      for (int round = 0; round < np - 1; ++round) {
+        for (int pr = warp; pr < np / 2; pr += nwarp) {
+          // circle method: player 0 fixed, the others rotate
+          int a = (pr == 0) ? 0 : 1 + ((pr - 1 + round) % (np - 1));
+          int b = 1 + ((np - 2 - pr + round) % (np - 1));
+          if (a >= n || b >= n) continue;
+          int p = a < b ? a : b, q = a < b ? b : a;
+          double* mp = M + (size_t)p * ldm;
+          double* mq = M + (size_t)q * ldm;
+          double app = 0.0, aqq = 0.0, apq = 0.0;
+          for (int t = lane; t < m; t += 32) {
+            const double x = mp[t], y = mq[t];
+            app += x * x; aqq += y * y; apq += x * y;
+          }
+          app = warp_sum(app); aqq = warp_sum(aqq); apq = warp_sum(apq);
+          if (apq != 0.0 && fabs(apq) > 1e-15 * sqrt(app) * sqrt(aqq)) {
+            const double zeta = (aqq - app) / (2.0 * apq);
+            const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+            const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
+            for (int r = lane; r < m; r += 32) {
+              const double x = mp[r], y = mq[r];
+              mp[r] = cs * x - sn * y;
+              mq[r] = sn * x + cs * y;
+            }
+            double* vp = V + (size_t)p * ldv;
+            double* vq = V + (size_t)q * ldv;
+            for (int r = lane; r < n; r += 32) {
+              const double x = vp[r], y = vq[r];
+              vp[r] = cs * x - sn * y;
+              vq[r] = sn * x + cs * y;
+            }
+            if (lane == 0) *iflag = 1;
+          }
+        }
+        __syncthreads();
+      }
+      const int any = *iflag;
+      __syncthreads();
+      if (!any) break;
+    }
+  }
+  // singular values = column norms
+  for (int c = warp; c < n; c += nwarp) {
+    const double* mc = M + (size_t)c * ldm;
+    double s = 0.0;
+    for (int t = lane; t < m; t += 32) s += mc[t] * mc[t];
+    s = warp_sum(s);
+    if (lane == 0) sig[c] = sqrt(s);
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < n; c += blockDim.x) {
+    const double sc = sig[c];
+    int pos = 0;
+    for (int d = 0; d < n; ++d) {
+      const double sd = sig[d];
+      pos += (sd > sc) || (sd == sc && d < c);
+    }
+    perm[pos] = c;
+  }
+  __syncthreads();
+  return sweep;
+}
+
+}  // namespace tlr

@@ -1,0 +1,686 @@
+// Right-looking TLR Cholesky, forward solve and log-likelihood (FP64 parity path).
+//
+// Reference: codes/17_tlr_cholesky_pilot.py:168-205 (factorization), 230-240 (forward solve)
+// and 259-266 (log-likelihood).  Per step k, in stream order:
+//   k_diag_build(k)   A_kk = Sigma_kk - sum_{m<k} U_km (V_km^T V_km) U_km^T   (deferred updates,
+//                     same subtraction order m = 0, 1, ... as the reference's step-by-step updates)
+//   k_potrf(k)        blocked Cholesky of A_kk (status k+1 when a pivot is not positive, as LAPACK
+//                     potrf), log det partial, z_k = L_kk^{-1} rhs_k
+//   k_trsm(k)         V_ik <- L_kk^{-1} V_ik for i > k; W_ik = V_ik^T V_ik; rhs_i -= U_ik (V_ik^T z_k)
+//   k_recompress(k)   A_ij <- truncate([U_ij, -U_ik W], [V_ij, U_jk]) for k < j < i, W = V_ik^T V_jk,
+//                     skipped when r_ik = 0 or r_jk = 0 (17:189-194)
+// Layout in HBM: diagonal tiles column-major (ld b); off-diagonal factors U, V column-major
+// (ld b, cap columns per tile); tile (i, j), i > j, has index i (i - 1) / 2 + j.
+#include "tlr_device.cuh"
+#include "tlr_kernels.h"
+
+namespace tlr {
+
+__device__ __forceinline__ int tidx(int i, int j) { return i * (i - 1) / 2 + j; }
+
+// ----------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_diag_build(const double* TLR_RESTRICT xy, int n, int b, int k,
+                                                   double sigma2, double inv_range, double nugget,
+                                                   const double* TLR_RESTRICT U, const double* TLR_RESTRICT Wd,
+                                                   const int* TLR_RESTRICT rank, int cap, double* TLR_RESTRICT D,
+                                                   const int* TLR_RESTRICT status) {
+  if (*status != 0) return;
+  // lower-triangular 32x32 block (rb, cb), rb >= cb
+  int blk = blockIdx.x, rb = 0;
+  while (blk > rb) { blk -= rb + 1; ++rb; }
+  const int cb = blk;
+  const int bk = min(b, n - k * b);
+  const int r0 = rb * 32, c0 = cb * 32;
+  __shared__ double Ua[32][33], Uc[32][33], Xc[32][33];
+  const int cl = threadIdx.x & 31, rl = threadIdx.x >> 5;
+  double acc[4];
+  const double2* p2 = reinterpret_cast<const double2*>(xy);
+  const int cg = c0 + cl;
+  const double2 pc = p2[k * b + min(cg, bk - 1)];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const int ag = r0 + rl + 8 * m;
+    const double2 pa = p2[k * b + min(ag, bk - 1)];
+    acc[m] = matern32_cov(pa.x, pa.y, pc.x, pc.y, sigma2, inv_range) + (ag == cg ? nugget : 0.0);
+  }
+  for (int mt = 0; mt < k; ++mt) {
+    const int t = tidx(k, mt);
+    const int r = rank[t];
+    if (r == 0) continue;
+    const double* Ut = U + (size_t)t * b * cap;
+    for (int q0 = 0; q0 < r; q0 += 32) {  // r <= cap; chunks of 32 columns of the inner dimension
+      const int rq = min(32, r - q0);
+      __syncthreads();
+      for (int e = threadIdx.x; e < 32 * rq; e += 256) {
+        const int rr = e & 31, q = e >> 5;
+        Ua[rr][q] = (r0 + rr < bk) ? Ut[(size_t)(q0 + q) * b + r0 + rr] : 0.0;
+        Uc[rr][q] = (c0 + rr < bk) ? Ut[(size_t)(q0 + q) * b + c0 + rr] : 0.0;
+      }
+      __syncthreads();
+      // Xc[c][p] = sum_q W[p][q] Uc[c][q] over the full inner range of W (needs all of U's columns)
+      for (int e = threadIdx.x; e < 32 * rq; e += 256) {
+        const int cc = e & 31, p = e >> 5;
+        double s = 0.0;
+        for (int q = 0; q < r; ++q) {
+          const double uq = (q >= q0 && q < q0 + rq) ? Uc[cc][q - q0]
+                                                     : ((c0 + cc < bk) ? Ut[(size_t)q * b + c0 + cc] : 0.0);
+          s = fma(Wd[(size_t)t * cap * cap + (size_t)q * cap + (q0 + p)], uq, s);
+        }
+        Xc[cc][p] = s;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const int rr = rl + 8 * m;
+        double s = 0.0;
+        for (int p = 0; p < rq; ++p) s = fma(Ua[rr][p], Xc[cl][p], s);
+        acc[m] -= s;
+      }
+    }
+  }
+  double* A = D + (size_t)k * b * b;
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const int ag = r0 + rl + 8 * m;
+    if (ag < bk && cg < bk && ag >= cg) A[(size_t)cg * b + ag] = acc[m];
+  }
+}
+
+// ----------------------------------------------------------------------------------------
+// Blocked right-looking Cholesky of the lower triangle of A_kk by one CTA, then the forward
+// solve of the diagonal block.  NB = panel width.
+template <int NB>
+__global__ void __launch_bounds__(512) k_potrf(double* TLR_RESTRICT D, int n, int b, int k,
+                                               double* TLR_RESTRICT rhs, double* TLR_RESTRICT z,
+                                               double* TLR_RESTRICT ldpart, double* TLR_RESTRICT qpart,
+                                               int* TLR_RESTRICT status) {
+  if (*status != 0) return;
+  const int bk = min(b, n - k * b);
+  double* A = D + (size_t)k * b * b;
+  extern __shared__ double smem[];
+  double* L11 = smem;                    // [NB][NB+1]
+  double* Pn = L11 + NB * (NB + 1);      // [bk][NB+1] panel below the diagonal block
+  __shared__ int fail;
+  __shared__ double logdet_acc;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int LD = NB + 1;
+  if (tid == 0) { fail = 0; logdet_acc = 0.0; }
+  for (int p0 = 0; p0 < bk; p0 += NB) {
+    const int pw = min(NB, bk - p0);
+    __syncthreads();
+    for (int e = tid; e < NB * NB; e += blockDim.x) {
+      const int i = e % NB, j = e / NB;
+      L11[i * LD + j] = (i < pw && j < pw && i >= j) ? A[(size_t)(p0 + j) * b + p0 + i] : 0.0;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      // unblocked Cholesky of the pw x pw diagonal block, lane = row
+      for (int c = 0; c < pw; ++c) {
+        const double d = L11[c * LD + c];
+        if (!(d > 0.0)) { if (lane == 0) fail = 1; break; }
+        const double sd = sqrt(d);
+        __syncwarp();
+        for (int i = lane; i < pw; i += 32) {
+          if (i > c) L11[i * LD + c] /= sd;
+        }
+        __syncwarp();
+        if (lane == 0) L11[c * LD + c] = sd;
+        for (int i = lane; i < pw; i += 32) {
+          if (i > c) {
+            const double lic = L11[i * LD + c];
+            for (int j = c + 1; j <= i; ++j) L11[i * LD + j] -= lic * L11[j * LD + c];
+          }
+        }
+        __syncwarp();
+      }
+      if (lane == 0 && !fail) {
+        double s = logdet_acc;
+        for (int c = 0; c < pw; ++c) s += log(L11[c * LD + c]);
+        logdet_acc = s;
+      }
+    }
+    __syncthreads();
+    if (fail) {
+      if (tid == 0) atomicCAS(status, 0, k + 1);
+      return;
+    }
+    for (int e = tid; e < pw * pw; e += blockDim.x) {
+      const int i = e % pw, j = e / pw;
+      if (i >= j) A[(size_t)(p0 + j) * b + p0 + i] = L11[i * LD + j];
+    }
+    // panel: rows below, X = A_21 L11^{-T}
+    const int m = bk - p0 - pw;
+    for (int row = tid; row < m; row += blockDim.x) {
+      double x[NB];
+#pragma unroll
+      for (int c = 0; c < NB; ++c) x[c] = (c < pw) ? A[(size_t)(p0 + c) * b + p0 + pw + row] : 0.0;
+#pragma unroll
+      for (int c = 0; c < NB; ++c) {
+        if (c < pw) {
+          double s = x[c];
+#pragma unroll
+          for (int j = 0; j < c; ++j) s -= x[j] * L11[c * LD + j];
+          x[c] = s / L11[c * LD + c];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < NB; ++c) {
+        Pn[row * LD + c] = (c < pw) ? x[c] : 0.0;
+        if (c < pw) A[(size_t)(p0 + c) * b + p0 + pw + row] = x[c];
+      }
+    }
+    __syncthreads();
+    // trailing update of the lower triangle, 4x4 register tiles
+    const int mt = (m + 3) / 4;
+    const int ntiles = mt * (mt + 1) / 2;
+    for (int tt = tid; tt < ntiles; tt += blockDim.x) {
+      int ti2 = 0, rem = tt;
+      // tile row ti2, tile col tj2 <= ti2, enumerated row by row
+      ti2 = (int)((sqrt(8.0 * rem + 1.0) - 1.0) * 0.5);
+      while (ti2 * (ti2 + 1) / 2 > rem) --ti2;
+      while ((ti2 + 1) * (ti2 + 2) / 2 <= rem) ++ti2;
+      const int tj2 = rem - ti2 * (ti2 + 1) / 2;
+      const int a0 = 4 * ti2, c0 = 4 * tj2;
+      double acc[4][4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
+      for (int t = 0; t < pw; ++t) {
+        double pa[4], pc[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          pa[u] = (a0 + u < m) ? Pn[(a0 + u) * LD + t] : 0.0;
+          pc[u] = (c0 + u < m) ? Pn[(c0 + u) * LD + t] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) acc[u][v] = fma(pa[u], pc[v], acc[u][v]);
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int cg = c0 + v;
+        if (cg >= m) continue;
+        double* colp = A + (size_t)(p0 + pw + cg) * b + p0 + pw;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int ag = a0 + u;
+          if (ag < m && ag >= cg) colp[ag] -= acc[u][v];
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // forward solve z_k = L_kk^{-1} rhs_k, blocked by 32 rows
+  double* zk = z + (size_t)k * b;
+  double* rk = rhs + (size_t)k * b;
+  __shared__ double zb[32];
+  __shared__ double red[40];
+  double qacc = 0.0;
+  for (int p0 = 0; p0 < bk; p0 += 32) {
+    const int pw = min(32, bk - p0);
+    if (warp == 0) {
+      double v = (lane < pw) ? rk[p0 + lane] : 0.0;
+      for (int c = 0; c < pw; ++c) {
+        const double xc = __shfl_sync(0xffffffffu, v, c) / A[(size_t)(p0 + c) * b + p0 + c];
+        if (lane == c) v = xc;
+        if (lane > c && lane < pw) v -= A[(size_t)(p0 + c) * b + p0 + lane] * xc;
+      }
+      if (lane < pw) { zb[lane] = v; zk[p0 + lane] = v; }
+    }
+    __syncthreads();
+    for (int row = p0 + pw + tid; row < bk; row += blockDim.x) {
+      double s = rk[row];
+      for (int c = 0; c < pw; ++c) s -= A[(size_t)(p0 + c) * b + row] * zb[c];
+      rk[row] = s;
+    }
+    if (tid < pw) qacc += zb[tid] * zb[tid];
+    __syncthreads();
+  }
+  const double q = block_sum(qacc, red);
+  if (tid == 0) { ldpart[k] = 2.0 * logdet_acc; qpart[k] = q; }
+}
+
+// ----------------------------------------------------------------------------------------
+// Panel solve for column k: one CTA per row tile i > k.
+__global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int n, int b, int k, int nB,
+                                             const double* TLR_RESTRICT U, double* TLR_RESTRICT V,
+                                             double* TLR_RESTRICT Wd, const int* TLR_RESTRICT rank, int cap,
+                                             const double* TLR_RESTRICT z, double* TLR_RESTRICT rhs,
+                                             const int* TLR_RESTRICT status) {
+  if (*status != 0) return;
+  const int i = k + 1 + blockIdx.x;
+  if (i >= nB) return;
+  const int t = tidx(i, k);
+  const int r = rank[t];
+  if (r == 0) return;
+  const int bk = min(b, n - k * b), bi = min(b, n - i * b);
+  const double* L = D + (size_t)k * b * b;
+  double* Vt = V + (size_t)t * b * cap;
+  const double* Ut = U + (size_t)t * b * cap;
+  __shared__ double L11[32][33];
+  __shared__ double Xp[32][65];
+  __shared__ double red[40];
+  __shared__ double zt[64];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int q0 = 0; q0 < r; q0 += 64) {
+    const int rq = min(64, r - q0);
+    for (int p0 = 0; p0 < bk; p0 += 32) {
+      const int pw = min(32, bk - p0);
+      __syncthreads();
+      for (int e = tid; e < 32 * 32; e += 256) {
+        const int a = e & 31, c = e >> 5;
+        L11[a][c] = (a < pw && c < pw && a >= c) ? L[(size_t)(p0 + c) * b + p0 + a] : 0.0;
+      }
+      __syncthreads();
+      // diagonal block solve, one thread per column
+      if (tid < rq) {
+        double* vc = Vt + (size_t)(q0 + tid) * b + p0;
+        double x[32];
+#pragma unroll
+        for (int a = 0; a < 32; ++a) x[a] = (a < pw) ? vc[a] : 0.0;
+#pragma unroll
+        for (int a = 0; a < 32; ++a) {
+          if (a < pw) {
+            double s = x[a];
+#pragma unroll
+            for (int c = 0; c < a; ++c) s -= L11[a][c] * x[c];
+            x[a] = s / L11[a][a];
+          }
+        }
+#pragma unroll
+        for (int a = 0; a < 32; ++a)
+          if (a < pw) { vc[a] = x[a]; Xp[a][tid] = x[a]; }
+      }
+      __syncthreads();
+      // update rows below: V[row, q] -= sum_c L[row, p0 + c] X[c, q]
+      for (int row = p0 + pw + tid; row < bk; row += 256) {
+        double l[32];
+#pragma unroll
+        for (int c = 0; c < 32; ++c) l[c] = (c < pw) ? L[(size_t)(p0 + c) * b + row] : 0.0;
+        for (int q = 0; q < rq; ++q) {
+          double s = 0.0;
+#pragma unroll
+          for (int c = 0; c < 32; ++c) s = fma(l[c], Xp[c][q], s);
+          Vt[(size_t)(q0 + q) * b + row] -= s;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // W = V^T V (r x r) and t = V^T z_k
+  const double* zk = z + (size_t)k * b;
+  double* W = Wd + (size_t)t * cap * cap;
+  for (int e = warp; e < r * r + r; e += 8) {
+    double s = 0.0;
+    if (e < r * r) {
+      const int p = e % r, q = e / r;
+      if (p <= q) {
+        const double* vp = Vt + (size_t)p * b;
+        const double* vq = Vt + (size_t)q * b;
+        for (int a = lane; a < bk; a += 32) s += vp[a] * vq[a];
+        s = warp_sum(s);
+        if (lane == 0) { W[(size_t)q * cap + p] = s; W[(size_t)p * cap + q] = s; }
+      }
+    } else {
+      const int p = e - r * r;
+      const double* vp = Vt + (size_t)p * b;
+      for (int a = lane; a < bk; a += 32) s += vp[a] * zk[a];
+      s = warp_sum(s);
+      if (lane == 0 && p < 64) zt[p] = s;
+    }
+  }
+  __syncthreads();
+  (void)red;
+  double* ri = rhs + (size_t)i * b;
+  if (r <= 64) {
+    for (int a = tid; a < bi; a += 256) {
+      double s = 0.0;
+      for (int q = 0; q < r; ++q) s = fma(Ut[(size_t)q * b + a], zt[q], s);
+      ri[a] -= s;
+    }
+  } else {
+    // wider ranks: recompute the projections column by column (rare)
+    for (int a = tid; a < bi; a += 256) {
+      double s = 0.0;
+      for (int q = 0; q < r; ++q) {
+        double tq = 0.0;
+        const double* vq = Vt + (size_t)q * b;
+        for (int u = 0; u < bk; ++u) tq += vq[u] * zk[u];
+        s = fma(Ut[(size_t)q * b + a], tq, s);
+      }
+      ri[a] -= s;
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------------------
+// Recompression of the trailing tiles at step k.  Persistent grid; each CTA owns one slot of
+// global scratch (L2-resident working arrays).
+struct RcScratch {
+  double *W, *Cc, *Dd, *X, *Y, *Ru, *Rv, *M, *Vs, *G, *Hh, *Uo, *Vo;
+};
+
+__device__ RcScratch rc_slot(double* base, int b, int cap) {
+  const size_t c2 = (size_t)cap * cap, s2 = (size_t)4 * cap * cap, bc = (size_t)b * cap;
+  RcScratch s;
+  double* p = base;
+  s.W = p; p += c2;
+  s.Cc = p; p += c2;
+  s.Dd = p; p += c2;
+  s.X = p; p += bc;
+  s.Y = p; p += bc;
+  s.Ru = p; p += s2;
+  s.Rv = p; p += s2;
+  s.M = p; p += s2;
+  s.Vs = p; p += s2;
+  s.G = p; p += 2 * c2;
+  s.Hh = p; p += c2;
+  s.Uo = p; p += bc;
+  s.Vo = p; p += bc;
+  return s;
+}
+
+size_t rc_slot_doubles(int b, int cap) {
+  const size_t c2 = (size_t)cap * cap, bc = (size_t)b * cap;
+  return 3 * c2 + 2 * bc + 4 * 4 * c2 + 2 * c2 + c2 + 2 * bc;
+}
+
+// C (p x q, ld p) = A^T B with A (m x p, lda), B (m x q, ldb): one warp per entry.
+__device__ void cta_atb(const double* A, int lda, const double* B, int ldb, int m, int p, int q, double* C,
+                        int ldc, double scale_a_inv_by_norm /*unused*/) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  for (int e = warp; e < p * q; e += nwarp) {
+    const int u = e % p, v = e / p;
+    const double* a = A + (size_t)u * lda;
+    const double* bb = B + (size_t)v * ldb;
+    double s = 0.0;
+    for (int t = lane; t < m; t += 32) s += a[t] * bb[t];
+    s = warp_sum(s);
+    if (lane == 0) C[(size_t)v * ldc + u] = s;
+  }
+  (void)scale_a_inv_by_norm;
+}
+
+__global__ void __launch_bounds__(256) k_recompress(int n, int b, int k, int nB, double* TLR_RESTRICT U,
+                                                   double* TLR_RESTRICT V, int* TLR_RESTRICT rank, int cap,
+                                                   int rule_fixed, double thr_rel, double thr_abs,
+                                                   double* TLR_RESTRICT scratch, size_t slot_doubles,
+                                                   int* TLR_RESTRICT status) {
+  if (*status != 0) return;
+  const int mB = nB - k - 1;  // trailing tiles
+  const long npairs = (long)mB * (mB - 1) / 2;
+  RcScratch S = rc_slot(scratch + (size_t)blockIdx.x * slot_doubles, b, cap);
+  __shared__ double red[40];
+  __shared__ double n1[128];
+  __shared__ double ninv[128];
+  __shared__ double sig[256];
+  __shared__ int perm[256];
+  __shared__ int iflag;
+  __shared__ int rsel;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (long pp = blockIdx.x; pp < npairs; pp += gridDim.x) {
+    // decode pp -> (ii, jj), ii > jj >= 0 within the trailing block
+    int ii = (int)((1.0 + sqrt(1.0 + 8.0 * (double)pp)) * 0.5);
+    while ((long)ii * (ii - 1) / 2 > pp) --ii;
+    while ((long)(ii + 1) * ii / 2 <= pp) ++ii;
+    const int jj = (int)(pp - (long)ii * (ii - 1) / 2);
+    const int i = k + 1 + ii, j = k + 1 + jj;
+    const int tij = tidx(i, j), tik = tidx(i, k), tjk = tidx(j, k);
+    const int r1 = rank[tij], ri = rank[tik], rj = rank[tjk];
+    if (ri == 0 || rj == 0) continue;
+    const int bi = min(b, n - i * b), bj = min(b, n - j * b), bk = min(b, n - k * b);
+    const double* Uij = U + (size_t)tij * b * cap;
+    const double* Vij = V + (size_t)tij * b * cap;
+    const double* Uik = U + (size_t)tik * b * cap;
+    const double* Vik = V + (size_t)tik * b * cap;
+    const double* Ujk = U + (size_t)tjk * b * cap;
+    const double* Vjk = V + (size_t)tjk * b * cap;
+    const int s = r1 + rj;
+    __syncthreads();
+    // W = V_ik^T V_jk (ri x rj)
+    cta_atb(Vik, b, Vjk, b, bk, ri, rj, S.W, cap, 0.0);
+    // column norms of U_ij
+    for (int c = warp; c < r1; c += 8) {
+      const double* u = Uij + (size_t)c * b;
+      double a = 0.0;
+      for (int t = lane; t < bi; t += 32) a += u[t] * u[t];
+      a = warp_sum(a);
+      if (lane == 0) { n1[c] = sqrt(a); ninv[c] = a > 0.0 ? 1.0 / sqrt(a) : 0.0; }
+    }
+    __syncthreads();
+    // X = -U_ik W (bi x rj)
+    for (int e = tid; e < bi * rj; e += 256) {
+      const int a = e % bi, q = e / bi;
+      double acc = 0.0;
+      for (int p = 0; p < ri; ++p) acc = fma(Uik[(size_t)p * b + a], S.W[(size_t)q * cap + p], acc);
+      S.X[(size_t)q * b + a] = -acc;
+    }
+    __syncthreads();
+    // block Gram-Schmidt twice against Q1 = U_ij diag(1/n1): C = Q1^T X, X -= Q1 C
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int e = warp; e < r1 * rj; e += 8) {
+        const int u = e % r1, v = e / r1;
+        const double* a = Uij + (size_t)u * b;
+        const double* x = S.X + (size_t)v * b;
+        double acc = 0.0;
+        for (int t = lane; t < bi; t += 32) acc += a[t] * x[t];
+        acc = warp_sum(acc);
+        if (lane == 0) S.G[(size_t)v * cap + u] = acc * ninv[u];  // temporary C increment
+      }
+      __syncthreads();
+      for (int e = tid; e < bi * rj; e += 256) {
+        const int a = e % bi, v = e / bi;
+        double acc = 0.0;
+        for (int u = 0; u < r1; ++u) acc = fma(Uij[(size_t)u * b + a] * ninv[u], S.G[(size_t)v * cap + u], acc);
+        S.X[(size_t)v * b + a] -= acc;
+      }
+      for (int e = tid; e < r1 * rj; e += 256) {
+        const int u = e % r1, v = e / r1;
+        const double inc = S.G[(size_t)v * cap + u];
+        S.Cc[(size_t)v * cap + u] = pass == 0 ? inc : S.Cc[(size_t)v * cap + u] + inc;
+      }
+      __syncthreads();
+    }
+    // R2 from Householder QR of the projected X (bi x rj); reflectors are not needed
+    cta_geqr2(S.X, b, bi, rj, sig, red);
+    // V side: D = V_ij^T U_jk, Y = U_jk - V_ij D (twice)
+    for (int e = tid; e < bj * rj; e += 256) {
+      const int a = e % bj, v = e / bj;
+      S.Y[(size_t)v * b + a] = Ujk[(size_t)v * b + a];
+    }
+    __syncthreads();
+    for (int pass = 0; pass < 3; ++pass) {
+      // pass 0, 1: D; pass 2: re-orthogonalisation of the explicit Q3 (after the QR below)
+      if (pass == 2) break;
+      cta_atb(Vij, b, S.Y, b, bj, r1, rj, S.G, cap, 0.0);
+      __syncthreads();
+      for (int e = tid; e < bj * rj; e += 256) {
+        const int a = e % bj, v = e / bj;
+        double acc = 0.0;
+        for (int u = 0; u < r1; ++u) acc = fma(Vij[(size_t)u * b + a], S.G[(size_t)v * cap + u], acc);
+        S.Y[(size_t)v * b + a] -= acc;
+      }
+      for (int e = tid; e < r1 * rj; e += 256) {
+        const int u = e % r1, v = e / r1;
+        const double inc = S.G[(size_t)v * cap + u];
+        S.Dd[(size_t)v * cap + u] = pass == 0 ? inc : S.Dd[(size_t)v * cap + u] + inc;
+      }
+      __syncthreads();
+    }
+    // R_u = [[diag(n1), C], [0, R2]] and the R3 part of R_v, both s x s (ld 2cap)
+    const int ls = 2 * cap;
+    for (int e = tid; e < s * s; e += 256) {
+      const int a = e % s, c = e / s;
+      double vu = 0.0;
+      if (a < r1) vu = (c < r1) ? (a == c ? n1[a] : 0.0) : S.Cc[(size_t)(c - r1) * cap + a];
+      else if (c >= r1 && a <= c && a - r1 < bi) vu = S.X[(size_t)(c - r1) * b + (a - r1)];
+      S.Ru[(size_t)c * ls + a] = vu;
+    }
+    __syncthreads();
+    double* tau3 = sig + 128;
+    cta_geqr2(S.Y, b, bj, rj, tau3, red);
+    for (int e = tid; e < s * s; e += 256) {
+      const int a = e % s, c = e / s;
+      double vv = 0.0;
+      if (a < r1) vv = (c < r1) ? (a == c ? 1.0 : 0.0) : S.Dd[(size_t)(c - r1) * cap + a];
+      else if (c >= r1 && a <= c && a - r1 < bj) vv = S.Y[(size_t)(c - r1) * b + (a - r1)];
+      S.Rv[(size_t)c * ls + a] = vv;
+    }
+    __syncthreads();
+    cta_org2r(S.Y, b, bj, rj, tau3);
+    if (rj > bj) {  // a ragged tile shorter than the rank: the extra basis columns are zero
+      for (int e = tid; e < bj * (rj - bj); e += 256) {
+        const int a = e % bj, v = bj + e / bj;
+        S.Y[(size_t)v * b + a] = 0.0;
+      }
+      __syncthreads();
+    }
+    // re-orthogonalise Q3 against V_ij once
+    if (r1 > 0) {
+      cta_atb(Vij, b, S.Y, b, bj, r1, rj, S.G, cap, 0.0);
+      __syncthreads();
+      for (int e = tid; e < bj * rj; e += 256) {
+        const int a = e % bj, v = e / bj;
+        double acc = 0.0;
+        for (int u = 0; u < r1; ++u) acc = fma(Vij[(size_t)u * b + a], S.G[(size_t)v * cap + u], acc);
+        S.Y[(size_t)v * b + a] -= acc;
+      }
+      __syncthreads();
+    }
+    // core M = R_u R_v^T (s x s)
+    for (int e = tid; e < s * s; e += 256) {
+      const int a = e % s, c = e / s;
+      double acc = 0.0;
+      for (int t = 0; t < s; ++t) acc = fma(S.Ru[(size_t)t * ls + a], S.Rv[(size_t)t * ls + c], acc);
+      S.M[(size_t)c * ls + a] = acc;
+    }
+    __syncthreads();
+    cta_jacobi_svd(S.M, ls, s, s, S.Vs, ls, sig, perm, &iflag);
+    if (tid == 0) {
+      double srt[256];
+      double fro2 = 0.0;
+      for (int q = 0; q < s; ++q) { srt[q] = sig[perm[q]]; }
+      for (int q = s - 1; q >= 0; --q) fro2 += srt[q] * srt[q];
+      const double thr = rule_fixed ? thr_rel * sqrt(fro2) : thr_abs;
+      int r = select_rank(srt, s, 0.0, thr, nullptr);
+      if (r < 0) r = s;
+      if (r > cap) { atomicCAS(status, 0, -2); r = -1; }
+      rsel = r;
+    }
+    __syncthreads();
+    const int rn = rsel;
+    if (rn < 0) return;
+    // G = R_v^T Vs_r (s x rn), H = W G_bottom (ri x rn)
+    for (int e = tid; e < s * rn; e += 256) {
+      const int t = e % s, c = e / s;
+      const double* vc = S.Vs + (size_t)perm[c] * ls;
+      double acc = 0.0;
+      for (int a = 0; a < s; ++a) acc = fma(S.Rv[(size_t)t * ls + a], vc[a], acc);
+      S.G[(size_t)c * ls + t] = acc;
+    }
+    __syncthreads();
+    for (int e = tid; e < ri * rn; e += 256) {
+      const int p = e % ri, c = e / ri;
+      double acc = 0.0;
+      for (int q = 0; q < rj; ++q) acc = fma(S.W[(size_t)q * cap + p], S.G[(size_t)c * ls + r1 + q], acc);
+      S.Hh[(size_t)c * cap + p] = acc;
+    }
+    __syncthreads();
+    // U' = U_ij G_top - U_ik H ; V' = V_ij Vs_top + Q3 Vs_bottom
+    for (int e = tid; e < bi * rn; e += 256) {
+      const int a = e % bi, c = e / bi;
+      double acc = 0.0;
+      for (int t = 0; t < r1; ++t) acc = fma(Uij[(size_t)t * b + a], S.G[(size_t)c * ls + t], acc);
+      for (int p = 0; p < ri; ++p) acc = fma(-Uik[(size_t)p * b + a], S.Hh[(size_t)c * cap + p], acc);
+      S.Uo[(size_t)c * b + a] = acc;
+    }
+    for (int e = tid; e < bj * rn; e += 256) {
+      const int a = e % bj, c = e / bj;
+      const double* vc = S.Vs + (size_t)perm[c] * ls;
+      double acc = 0.0;
+      for (int t = 0; t < r1; ++t) acc = fma(Vij[(size_t)t * b + a], vc[t], acc);
+      for (int t = 0; t < rj; ++t) acc = fma(S.Y[(size_t)t * b + a], vc[r1 + t], acc);
+      S.Vo[(size_t)c * b + a] = acc;
+    }
+    __syncthreads();
+    double* Uw = U + (size_t)tij * b * cap;
+    double* Vw = V + (size_t)tij * b * cap;
+    for (int e = tid; e < bi * rn; e += 256) {
+      const int a = e % bi, c = e / bi;
+      Uw[(size_t)c * b + a] = S.Uo[(size_t)c * b + a];
+    }
+    for (int e = tid; e < bj * rn; e += 256) {
+      const int a = e % bj, c = e / bj;
+      Vw[(size_t)c * b + a] = S.Vo[(size_t)c * b + a];
+    }
+    if (tid == 0) rank[tij] = rn;
+    __syncthreads();
+  }
+}
+
+// ----------------------------------------------------------------------------------------
+__global__ void k_finish(int nB, int n, const double* ldpart, const double* qpart, double* out,
+                         const int* status) {
+  if (threadIdx.x != 0) return;
+  if (*status != 0) { out[0] = 0.0; out[1] = 0.0; out[2] = 0.0; return; }
+  double ld = 0.0, q = 0.0;
+  for (int k = 0; k < nB; ++k) { ld += ldpart[k]; q += qpart[k]; }
+  const double log2pi = 1.8378770664093454836;
+  out[0] = -0.5 * (q + ld + (double)n * log2pi);
+  out[1] = ld;
+  out[2] = q;
+}
+
+// ----------------------------------------------------------------------------------------
+int launch_diag_build(const double* xy, int n, int b, int k, double sigma2, double inv_range, double nugget,
+                      const double* U, const double* Wd, const int* rank, int cap, double* D, const int* status,
+                      cudaStream_t s) {
+  const int bk = std::min(b, n - k * b);
+  const int nb = (bk + 31) / 32;
+  k_diag_build<<<nb * (nb + 1) / 2, 256, 0, s>>>(xy, n, b, k, sigma2, inv_range, nugget, U, Wd, rank, cap, D,
+                                                 status);
+  return (int)cudaGetLastError();
+}
+
+int launch_potrf(double* D, int n, int b, int k, double* rhs, double* z, double* ldpart, double* qpart,
+                 int* status, cudaStream_t s) {
+  if (b <= 640) {
+    const size_t sm = ((size_t)32 * 33 + (size_t)b * 33) * 8;
+    cudaFuncSetAttribute(k_potrf<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_potrf<32><<<1, 512, sm, s>>>(D, n, b, k, rhs, z, ldpart, qpart, status);
+  } else {
+    const size_t sm = ((size_t)16 * 17 + (size_t)b * 17) * 8;
+    cudaFuncSetAttribute(k_potrf<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_potrf<16><<<1, 512, sm, s>>>(D, n, b, k, rhs, z, ldpart, qpart, status);
+  }
+  return (int)cudaGetLastError();
+}
+
+int launch_trsm(const double* D, int n, int b, int k, int nB, const double* U, double* V, double* Wd,
+                const int* rank, int cap, const double* z, double* rhs, const int* status, cudaStream_t s) {
+  if (nB - k - 1 <= 0) return 0;
+  k_trsm<<<nB - k - 1, 256, 0, s>>>(D, n, b, k, nB, U, V, Wd, rank, cap, z, rhs, status);
+  return (int)cudaGetLastError();
+}
+
+int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, int rule_fixed,
+                      double thr_rel, double thr_abs, double* scratch, size_t slot_doubles, int nslots,
+                      int* status, cudaStream_t s) {
+  const long mB = nB - k - 1;
+  const long npairs = mB * (mB - 1) / 2;
+  if (npairs <= 0) return 0;
+  const int grid = (int)std::min<long>(npairs, nslots);
+  k_recompress<<<grid, 256, 0, s>>>(n, b, k, nB, U, V, rank, cap, rule_fixed, thr_rel, thr_abs, scratch,
+                                    slot_doubles, status);
+  return (int)cudaGetLastError();
+}
+
+int launch_finish(int nB, int n, const double* ldpart, const double* qpart, double* out, const int* status,
+                  cudaStream_t s) {
+  k_finish<<<1, 32, 0, s>>>(nB, n, ldpart, qpart, out, status);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace tlr

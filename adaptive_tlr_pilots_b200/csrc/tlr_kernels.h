@@ -1,0 +1,50 @@
+// Host-side launchers of the TLR kernels (internal to the library).
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <algorithm>
+
+namespace tlr {
+
+// Morton order (codes/11_tlr_rank_rules.py:40-53)
+int launch_morton(const double* xy, int n, int order, unsigned* keys, unsigned* cnt, unsigned* off,
+                  unsigned* cursor, long long* perm, cudaStream_t s);
+int launch_gather_sites(const double* xy_in, const double* y_in, const long long* perm, int n, double* xy_out,
+                        double* y_out, cudaStream_t s);
+
+// initial compression
+int launch_gen_offdiag(const double* xy, int n, int b, int tile_base, const int* ti, const int* tj, double* T,
+                       int nchunk, double sigma2, double inv_range, const int* status, cudaStream_t s);
+int launch_sketch(const double* T, int n, int b, int k, int tile_base, const int* ti, const int* tj, const int* need,
+                  const double* P, double* out, int ldp, int omega, int mode, int nchunk, const int* status,
+                  cudaStream_t s);
+int launch_orth(double* Z, int n, int b, int k, int ldp, int tile_base, const int* tj, const int* need,
+                double* gscratch, int nchunk, const int* status, cudaStream_t s);
+int launch_resid(const double* T, int n, int b, int k, int ldp, int tile_base, const int* ti, const int* tj,
+                 const int* need, const double* P, const double* C, double* parts, double* fparts, int nblk,
+                 int nchunk, const int* status, cudaStream_t s);
+int launch_finalize(int n, int b, int k, int ldp, int cap, int margin, int rule_fixed, double thr_rel,
+                    double thr_abs, int tile_base, const int* ti, const int* tj, int* need, const double* P,
+                    const double* C, const double* parts, const double* fparts, int nblk, double* gscratch,
+                    double* gsv, double* U, double* V, int* rank, int last_level, int nchunk, int* status,
+                    cudaStream_t s);
+
+// factorization
+int launch_diag_build(const double* xy, int n, int b, int k, double sigma2, double inv_range, double nugget,
+                      const double* U, const double* Wd, const int* rank, int cap, double* D, const int* status,
+                      cudaStream_t s);
+int launch_potrf(double* D, int n, int b, int k, double* rhs, double* z, double* ldpart, double* qpart,
+                 int* status, cudaStream_t s);
+int launch_trsm(const double* D, int n, int b, int k, int nB, const double* U, double* V, double* Wd,
+                const int* rank, int cap, const double* z, double* rhs, const int* status, cudaStream_t s);
+size_t rc_slot_doubles(int b, int cap);
+int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, int rule_fixed,
+                      double thr_rel, double thr_abs, double* scratch, size_t slot_doubles, int nslots,
+                      int* status, cudaStream_t s);
+int launch_finish(int nB, int n, const double* ldpart, const double* qpart, double* out, const int* status,
+                  cudaStream_t s);
+
+// small utilities
+int launch_fill_int(int* p, int v, int count, cudaStream_t s);
+
+}  // namespace tlr

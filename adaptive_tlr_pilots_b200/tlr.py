@@ -1,0 +1,313 @@
+"""Reference-facing Python surface of the B200 TLR log-likelihood.
+
+Mirrors the functions the pilot scripts call (marysalvana/adaptive-tlr-pilots):
+
+  tile_bounds(n, b)                         codes/11_tlr_rank_rules.py:69-71
+  morton_order(xy, order=10)                codes/11_tlr_rank_rules.py:40-53   (on the GPU)
+  tlr_loglik(S, y, theta, bounds, rule, v)  codes/17_tlr_cholesky_pilot.py:259-266
+  neg_loglik_tlr(logth, S, y, bounds, ...)  codes/17_tlr_cholesky_pilot.py:279-290
+  Likelihood(S, y, b, device)(theta, ...)   codes/19_tlr_mcmc_gpu.py:27-138 (call surface)
+  loglik(theta, locs, y, b, rule, tau|eps)  the (loglik, per-tile ranks, PD) form
+
+Every evaluation runs on the GPU through libtlr_b200.so (include/tlr_b200.h).  There is no CPU
+path: without the library or a CUDA device these functions raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+
+RULES = {"fixed": _lib.TLR_RULE_FIXED, "adaptive": _lib.TLR_RULE_ADAPTIVE}
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("adaptive_tlr_pilots_b200 needs a CUDA device (no CPU fallback)")
+    return torch
+
+
+def tile_bounds(n, b):
+    """[(0, b), (b, 2b), ..., (., n)]; the last tile may be short (codes/11_tlr_rank_rules.py:69-71)."""
+    edges = list(range(0, n, b)) + [n]
+    return [(edges[t], edges[t + 1]) for t in range(len(edges) - 1)]
+
+
+def _tile_size(bounds, n):
+    """The uniform tile size of a bounds list made by tile_bounds; ValueError otherwise."""
+    if not bounds:
+        raise ValueError("bounds is empty")
+    b = bounds[0][1] - bounds[0][0]
+    if b <= 0 or list(map(tuple, bounds)) != tile_bounds(n, b):
+        raise ValueError("bounds must be tile_bounds(n, b) for one tile size b")
+    return b
+
+
+def morton_order(xy, order=10, device=0):
+    """Stable Z-order permutation of points (N x 2), computed on the GPU.
+
+    Same quantisation, bit interleave and stable tie order as codes/11_tlr_rank_rules.py:40-53."""
+    torch = _torch()
+    xy = np.ascontiguousarray(np.asarray(xy, dtype=np.float64))
+    if xy.ndim != 2 or xy.shape[1] != 2:
+        raise ValueError("xy must be N x 2")
+    n = xy.shape[0]
+    lib = _lib.load()
+    dev = torch.device("cuda", device)
+    with torch.cuda.device(dev):
+        t = torch.from_numpy(xy).to(dev)
+        perm = torch.empty(n, dtype=torch.int64, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(lib.tlr_morton_order(ctypes.c_void_p(t.data_ptr()), n, order, ctypes.c_void_p(perm.data_ptr()),
+                                        ctypes.c_void_p(stream)))
+        return perm.cpu().numpy()
+
+
+@dataclass
+class Evaluation:
+    status: int                 # 0 ok, k + 1 not PD at diagonal tile k
+    loglik: float | None
+    info: dict
+    factor_ranks: np.ndarray    # reference L_off order (for k, for i > k)
+    sigma_ranks: np.ndarray     # initial ranks (for i, for j < i)
+
+
+class Plan:
+    """Device workspace for one (N, b) problem: owns a tlr_plan of the C ABI."""
+
+    def __init__(self, n, b, cap=64, device=0):
+        torch = _torch()
+        self.lib = _lib.load()
+        self.n, self.b, self.cap, self.device = int(n), int(b), int(cap), int(device)
+        self.nB = (self.n + self.b - 1) // self.b
+        self.ntiles = self.nB * (self.nB - 1) // 2
+        self.dev = torch.device("cuda", self.device)
+        self.stream = torch.cuda.current_stream(self.dev)
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.tlr_plan_create(ctypes.byref(h), self.n, self.b, self.cap, self.device,
+                                            ctypes.c_void_p(self.stream.cuda_stream)))
+        self.handle = h
+        self.generation = 0
+        self._data = None
+
+    def close(self):
+        if self.handle is not None and self.handle.value:
+            self.lib.tlr_plan_destroy(self.handle)
+        self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_data(self, S, y):
+        """Load Morton-ordered sites and observations (numpy or torch) onto the device."""
+        torch = _torch()
+        S_t = torch.as_tensor(S, dtype=torch.float64).to(self.dev).contiguous()
+        y_t = torch.as_tensor(y, dtype=torch.float64).to(self.dev).contiguous()
+        if S_t.shape != (self.n, 2) or y_t.shape != (self.n,):
+            raise ValueError(f"expected S of shape ({self.n}, 2) and y of shape ({self.n},)")
+        self._data = (S_t, y_t)
+        _lib.check(self.lib.tlr_set_data(self.handle, ctypes.c_void_p(S_t.data_ptr()),
+                                         ctypes.c_void_p(y_t.data_ptr())))
+
+    def evaluate(self, theta, rule, value, host_S=None, host_y=None) -> Evaluation:
+        if rule not in RULES:
+            raise ValueError(f"rule must be one of {sorted(RULES)}, got {rule!r}")
+        th = (ctypes.c_double * 3)(*[float(v) for v in theta])
+        ll = ctypes.c_double(0.0)
+        info = _lib.TlrInfo()
+        fr = np.zeros(max(self.ntiles, 1), dtype=np.int32)
+        sr = np.zeros(max(self.ntiles, 1), dtype=np.int32)
+        ip = ctypes.POINTER(ctypes.c_int)
+        if host_S is not None:
+            S = np.ascontiguousarray(host_S, dtype=np.float64)
+            y = np.ascontiguousarray(host_y, dtype=np.float64)
+            if S.shape != (self.n, 2) or y.shape != (self.n,):
+                raise ValueError(f"expected S of shape ({self.n}, 2) and y of shape ({self.n},)")
+            rc = self.lib.tlr_loglik_host(self.handle, S.ctypes.data_as(ctypes.c_void_p),
+                                          y.ctypes.data_as(ctypes.c_void_p), th, RULES[rule], float(value),
+                                          ctypes.byref(ll), ctypes.byref(info), fr.ctypes.data_as(ip),
+                                          sr.ctypes.data_as(ip))
+        else:
+            rc = self.lib.tlr_loglik(self.handle, th, RULES[rule], float(value), ctypes.byref(ll), ctypes.byref(info),
+                                     fr.ctypes.data_as(ip), sr.ctypes.data_as(ip))
+        rc = _lib.check(rc)
+        self.generation += 1
+        d = dict(completed=bool(info.completed), stored_sigma=int(info.stored_sigma),
+                 max_rank_sigma=int(info.max_rank_sigma))
+        if rc == 0:
+            d.update(stored_factor=int(info.stored_factor), mean_rank_factor=float(info.mean_rank_factor),
+                     max_rank_factor=int(info.max_rank_factor), logdet=float(info.logdet), quad=float(info.quad))
+        else:
+            d.update(failed_at=int(info.failed_at))
+        return Evaluation(rc, float(ll.value) if rc == 0 else None, d, fr[: self.ntiles], sr[: self.ntiles])
+
+    # factor access (checking / prediction)
+    def diag_tile(self, k):
+        bk = min(self.b, self.n - k * self.b)
+        out = np.zeros((bk, bk), order="F")
+        _lib.check(self.lib.tlr_get_diag_tile(self.handle, k, out.ctypes.data_as(ctypes.c_void_p)))
+        return np.ascontiguousarray(out)
+
+    def offdiag_tile(self, i, j):
+        bi = min(self.b, self.n - i * self.b)
+        bj = min(self.b, self.n - j * self.b)
+        u = np.zeros((self.cap, bi))
+        v = np.zeros((self.cap, bj))
+        r = ctypes.c_int(0)
+        _lib.check(self.lib.tlr_get_offdiag_tile(self.handle, i, j, u.ctypes.data_as(ctypes.c_void_p),
+                                                 v.ctypes.data_as(ctypes.c_void_p), ctypes.byref(r)))
+        r = r.value
+        return np.ascontiguousarray(u[:r].T), np.ascontiguousarray(v[:r].T)
+
+
+class TLRFactor:
+    """Lazy view of the factor left in a plan by the last evaluation (L_diag, L_off as in
+    codes/17_tlr_cholesky_pilot.py:215).  Invalidated by the plan's next evaluation."""
+
+    def __init__(self, plan: Plan):
+        self.plan = plan
+        self.generation = plan.generation
+
+    def _check(self):
+        if self.plan.generation != self.generation:
+            raise RuntimeError("this factor was overwritten by a later evaluation on the same plan")
+
+    @property
+    def L_diag(self):
+        self._check()
+        return [self.plan.diag_tile(k) for k in range(self.plan.nB)]
+
+    @property
+    def L_off(self):
+        self._check()
+        out = {}
+        for k in range(self.plan.nB):
+            for i in range(k + 1, self.plan.nB):
+                out[(i, k)] = self.plan.offdiag_tile(i, k)
+        return out
+
+
+_PLANS: dict = {}
+
+
+def get_plan(n, b, cap=64, device=0) -> Plan:
+    key = (int(n), int(b), int(cap), int(device))
+    p = _PLANS.get(key)
+    if p is None:
+        p = Plan(n, b, cap, device)
+        _PLANS[key] = p
+    return p
+
+
+def release_plans():
+    for p in _PLANS.values():
+        p.close()
+    _PLANS.clear()
+
+
+def tlr_loglik(S, y, theta, bounds, rule, value, cap=64, device=0):
+    """Drop-in for codes/17_tlr_cholesky_pilot.py:259 tlr_loglik.
+
+    Returns (loglik, factor, info) or (None, None, info) when a diagonal tile is not positive
+    definite (info['completed'] False, info['failed_at'] = k), like 17:172-176.  `factor` is a
+    lazy TLRFactor on the device."""
+    S = np.asarray(S, dtype=np.float64)
+    n = S.shape[0]
+    b = _tile_size(bounds, n)
+    plan = get_plan(n, b, cap, device)
+    ev = plan.evaluate(theta, rule, value, host_S=S, host_y=np.asarray(y, dtype=np.float64))
+    if ev.status != 0:
+        return None, None, ev.info
+    return ev.loglik, TLRFactor(plan), ev.info
+
+
+def neg_loglik_tlr(logth, S, y, bounds, rule, value, trace):
+    """Optimizer objective, codes/17_tlr_cholesky_pilot.py:279-290: 1e12 on a failed
+    factorization, evaluations and failures counted in `trace`."""
+    theta = np.exp(logth)
+    trace["evals"] += 1
+    if rule == "dense":
+        ll = dense_loglik(S, y, theta)
+    else:
+        ll, _, _ = tlr_loglik(S, y, theta, bounds, rule, value)
+    if ll is None:
+        trace["failures"] += 1
+        return 1e12
+    return -ll
+
+
+def dense_loglik(S, y, theta, device=0):
+    """Dense FP64 log-likelihood on the GPU (cuSOLVER Cholesky through torch); None if not PD.
+
+    The 'dense' rule of codes/17_tlr_cholesky_pilot.py:282-284 (rules.loglik_dense, 11:112-120)."""
+    torch = _torch()
+    dev = torch.device("cuda", device)
+    St = torch.as_tensor(np.asarray(S, dtype=np.float64), device=dev)
+    yt = torch.as_tensor(np.asarray(y, dtype=np.float64), device=dev)
+    sigma2, rng, eta = [float(v) for v in theta]
+    x = (3.0 ** 0.5) * torch.cdist(St, St) / rng
+    K = sigma2 * (1.0 + x) * torch.exp(-x)
+    K.diagonal().add_(sigma2 * eta)
+    L, info = torch.linalg.cholesky_ex(K)
+    if int(info.item()) != 0:
+        return None
+    z = torch.linalg.solve_triangular(L, yt[:, None], upper=False)[:, 0]
+    ld = 2.0 * torch.log(torch.diagonal(L)).sum()
+    return float(-0.5 * (z @ z + ld + len(yt) * np.log(2 * np.pi)))
+
+
+def loglik(theta, locs, y, b, rule, tau=None, eps=None, ordered=False, cap=64, device=0):
+    """(loglik | None, per-tile factor ranks, PD flag) for sites `locs` and observations `y`.
+
+    rule 'adaptive' takes tau, rule 'fixed' takes eps.  Unless ordered=True the sites are first
+    put into Morton order on the GPU (the reference orders them before every fit, 17:324)."""
+    if rule == "adaptive":
+        if tau is None:
+            raise ValueError("rule 'adaptive' needs tau")
+        value = tau
+    elif rule == "fixed":
+        if eps is None:
+            raise ValueError("rule 'fixed' needs eps")
+        value = eps
+    else:
+        raise ValueError(f"rule must be 'adaptive' or 'fixed', got {rule!r}")
+    locs = np.asarray(locs, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    if not ordered:
+        perm = morton_order(locs, device=device)
+        locs, y = locs[perm], y[perm]
+    n = locs.shape[0]
+    plan = get_plan(n, b, cap, device)
+    ev = plan.evaluate(theta, rule, value, host_S=locs, host_y=y)
+    return ev.loglik, ev.factor_ranks.copy(), ev.status == 0
+
+
+class Likelihood:
+    """Call surface of codes/19_tlr_mcmc_gpu.py:27-138: Likelihood(S, y, b, device)(theta, rule,
+    value) -> log-likelihood, or -inf when the factorization fails; self.last records
+    ok / stored values / time.  Here the likelihood is the TLR Cholesky one (never assembled)."""
+
+    def __init__(self, S, y, b, device=0, cap=64):
+        self.n = int(np.asarray(S).shape[0])
+        self.b = int(b)
+        dev = device.index if hasattr(device, "index") and device.index is not None else (
+            0 if not isinstance(device, int) else device)
+        self.plan = Plan(self.n, self.b, cap, dev)
+        self.plan.set_data(S, y)
+        self.last = {}
+
+    def __call__(self, theta, rule, value):
+        t0 = time.time()
+        ev = self.plan.evaluate(theta, rule, value)
+        ok = ev.status == 0
+        self.last = dict(ok=ok, stored=ev.info.get("stored_factor", ev.info["stored_sigma"]), time=time.time() - t0,
+                         info=ev.info)
+        return ev.loglik if ok else -float("inf")

@@ -1,0 +1,98 @@
+/*
+ * C ABI of the B200 adaptive tile-low-rank (TLR) Gaussian-process log-likelihood.
+ *
+ * The reference (marysalvana/adaptive-tlr-pilots) has no FFI: its scripts load
+ * codes/11_tlr_rank_rules.py and codes/17_tlr_cholesky_pilot.py by file path and call Python
+ * functions.  Each entry point below replaces one of those calls; the comment on each names
+ * the reference interface (path:line) it stands in for.  The Python package
+ * adaptive_tlr_pilots_b200 binds these symbols with ctypes and presents the reference's call
+ * surface on top of them.
+ *
+ * Conventions
+ *   - plain C types only; device pointers are CUDA device addresses, host pointers are host
+ *     addresses; sizes are element counts;
+ *   - every function returns a status: 0 on success, > 0 only where documented (a factorization
+ *     that is not positive definite), < 0 on error, with a message in tlr_last_error();
+ *   - nothing aborts, nothing throws; no call prints;
+ *   - a plan owns all of its device memory (allocated once, at creation); a plan is used by one
+ *     host thread at a time; work is issued on the plan's stream.
+ */
+#ifndef TLR_B200_H
+#define TLR_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* rank rules: codes/17_tlr_cholesky_pilot.py:149-150 */
+#define TLR_RULE_FIXED 0    /* relative Frobenius tolerance eps per tile */
+#define TLR_RULE_ADAPTIVE 1 /* absolute budget tau * b * sigma2 * eta / N */
+
+/* status codes */
+#define TLR_OK 0
+#define TLR_ERR_ARG (-1)          /* invalid argument */
+#define TLR_ERR_RANK_CAP (-2)     /* a tile rank exceeded the plan's rank capacity */
+#define TLR_ERR_CUDA (-3)         /* CUDA runtime error */
+#define TLR_ERR_NOMEM (-4)        /* device allocation failed */
+#define TLR_ERR_COMPRESS (-5)     /* a tile needed more than the largest sketch width */
+#define TLR_ERR_NOT_READY (-6)    /* tlr_set_data has not been called */
+
+typedef struct tlr_plan tlr_plan;
+
+/* Per-evaluation statistics, the `info` dict of codes/17_tlr_cholesky_pilot.py:167, 175, 206-209. */
+typedef struct {
+  int completed;            /* 1 when every diagonal tile factorized */
+  int failed_at;            /* first diagonal tile that is not positive definite, or -1 */
+  long long stored_sigma;   /* stored values of the compressed covariance (17:154-167) */
+  int max_rank_sigma;
+  long long stored_factor;  /* stored values of the factor (17:206) */
+  double mean_rank_factor;
+  int max_rank_factor;
+  double logdet;            /* 2 sum log diag L_kk */
+  double quad;              /* z^T z, z = L^{-1} y */
+} tlr_info;
+
+/* Create a plan for N sites in tiles of b (the last tile may be short, as
+ * codes/11_tlr_rank_rules.py:69-71 tile_bounds), with room for `cap` columns per off-diagonal
+ * factor.  stream may be NULL (the legacy default stream).  Allocates all device memory. */
+int tlr_plan_create(tlr_plan** plan, int n, int b, int cap, int device, void* stream);
+void tlr_plan_destroy(tlr_plan* plan);
+
+/* Morton (Z-order) permutation of n points (device xy, n x 2, row-major) into device perm
+ * (n int64): replaces morton_order, codes/11_tlr_rank_rules.py:40-53 (order = bits per axis). */
+int tlr_morton_order(const double* xy_dev, int n, int order, long long* perm_dev, void* stream);
+
+/* Load Morton-ordered sites (device, n x 2 row-major) and observations (device, n) into the
+ * plan (copied; the caller keeps ownership).  The reference passes S and y to every call of
+ * tlr_loglik (codes/17_tlr_cholesky_pilot.py:259); here they are loaded once. */
+int tlr_set_data(tlr_plan* plan, const double* xy_dev, const double* y_dev);
+
+/* Log-likelihood at theta = (sigma2, range, eta) with rule TLR_RULE_FIXED (value = eps) or
+ * TLR_RULE_ADAPTIVE (value = tau): replaces tlr_loglik, codes/17_tlr_cholesky_pilot.py:259-266
+ * (tlr_cholesky 137-215 and tlr_forward 230-240 inside).
+ * Returns 0 on success, k + 1 when diagonal tile k is not positive definite (the reference's
+ * (None, None, {completed: False, failed_at: k}), 17:172-176), < 0 on error.
+ * loglik, info, factor_ranks and sigma_ranks are host pointers and may be NULL.
+ * factor_ranks receives nB (nB - 1) / 2 ranks in the reference's L_off order (for k, for i > k,
+ * 17:207); sigma_ranks the initial ranks in the order (for i, for j < i) (17:155-166). */
+int tlr_loglik(tlr_plan* plan, const double theta[3], int rule, double value, double* loglik, tlr_info* info,
+               int* factor_ranks, int* sigma_ranks);
+
+/* The same evaluation with HOST sites and observations (Morton-ordered), copied to the device
+ * inside the call: the end-to-end form of tlr_loglik for callers that hold numpy arrays. */
+int tlr_loglik_host(tlr_plan* plan, const double* xy_host, const double* y_host, const double theta[3], int rule,
+                    double value, double* loglik, tlr_info* info, int* factor_ranks, int* sigma_ranks);
+
+/* Copy factor pieces to the host for checking: the dense lower factor of diagonal tile k
+ * (bk x bk, column-major) or the (U, V) pair of off-diagonal tile (i, j), i > j (b_i x r and
+ * b_j x r, column-major, r = *rank).  Valid after a successful tlr_loglik. */
+int tlr_get_diag_tile(tlr_plan* plan, int k, double* out_host);
+int tlr_get_offdiag_tile(tlr_plan* plan, int i, int j, double* u_host, double* v_host, int* rank);
+
+/* Message of the last error on this thread. */
+const char* tlr_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TLR_B200_H */

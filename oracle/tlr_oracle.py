@@ -1,0 +1,397 @@
+"""CPU oracle for the adaptive tile-low-rank (TLR) Gaussian-process log-likelihood.
+
+TEST INFRASTRUCTURE ONLY.  This module is a plain NumPy/SciPy restatement of the
+reference pipeline (marysalvana/adaptive-tlr-pilots, ``codes/11_tlr_rank_rules.py``
+and ``codes/17_tlr_cholesky_pilot.py``).  It exists so that ``tests/``, the smoke check
+and the CPU-baseline leg of ``bench.py`` have something independent to compare the
+CUDA path with.  The product path (``adaptive_tlr_pilots_b200``) never imports it.
+
+Every function cites the reference lines it follows.  Parity of this restatement with
+the reference itself is pinned by ``tests/golden/`` (fixtures generated by importing the
+reference, plus the committed result values the reference ships) and checked in
+``tests/test_oracle.py``.
+
+Additions that the reference does not have (needed to check the CUDA path):
+  * frozen ranks: ``tlr_cholesky(..., rank_log=..., frozen=...)`` records every rank the
+    rule picks (initial compression and each recompression) and can replay them at
+    another theta, so finite differences see a smooth function;
+  * ``singular_tail``: the shared tail/threshold logic, written once.
+"""
+from __future__ import annotations
+
+import numpy as np
+from scipy.linalg import LinAlgError, cholesky, solve_triangular
+from scipy.linalg import svd as scipy_svd
+
+SQRT3 = np.sqrt(3.0)
+LOG2PI = np.log(2.0 * np.pi)
+
+
+# ----------------------------------------------------------------------------- model
+def matern32(h, rng):
+    """Matern nu=3/2 correlation (1 + x) exp(-x), x = sqrt(3) h / range.
+
+    Follows codes/11_tlr_rank_rules.py:35-37."""
+    x = SQRT3 * h / rng
+    return (1.0 + x) * np.exp(-x)
+
+
+def morton_order(xy, order=10):
+    """Z-order permutation of points in the unit square.
+
+    Coordinates are quantised to ``order`` bits per axis (clip(floor(2^order * c))),
+    the x bits go to even and the y bits to odd positions of the key, and the
+    permutation is a stable argsort of the key (ties keep input order).
+    Follows codes/11_tlr_rank_rules.py:40-53."""
+    n = 1 << order
+    q = np.clip((xy * n).astype(np.int64), 0, n - 1).astype(np.uint64)
+
+    def interleave_zeros(v):
+        out = np.zeros_like(v)
+        for bit in range(order):
+            out |= ((v >> np.uint64(bit)) & np.uint64(1)) << np.uint64(2 * bit)
+        return out
+
+    key = interleave_zeros(q[:, 0]) | (interleave_zeros(q[:, 1]) << np.uint64(1))
+    return np.argsort(key, kind="stable")
+
+
+def pairwise_dist(A, B):
+    """Euclidean distances sqrt(max(dx^2 + dy^2, 0)).  codes/11_tlr_rank_rules.py:56-58."""
+    d2 = (A[:, None, 0] - B[None, :, 0]) ** 2 + (A[:, None, 1] - B[None, :, 1]) ** 2
+    return np.sqrt(np.maximum(d2, 0.0))
+
+
+def cov_dense(S, theta):
+    """Dense covariance sigma2 * M + sigma2 * eta * I.  codes/11_tlr_rank_rules.py:61-65."""
+    sigma2, rng, eta = theta
+    K = sigma2 * matern32(pairwise_dist(S, S), rng)
+    K[np.diag_indices_from(K)] += sigma2 * eta
+    return K
+
+
+def tile_bounds(n, b):
+    """[(0,b), (b,2b), ..., (.., n)]; the last tile may be short.  codes/11_tlr_rank_rules.py:69-71."""
+    edges = list(range(0, n, b)) + [n]
+    return [(edges[t], edges[t + 1]) for t in range(len(edges) - 1)]
+
+
+# ------------------------------------------------------------------------ rank rule
+def singular_tail(s):
+    """tail[r] = ||T - T_r||_F for r = 0..len(s), with tail[len(s)] = 0.
+
+    Summed from the smallest singular value up, as codes/17_tlr_cholesky_pilot.py:113."""
+    return np.append(np.sqrt(np.cumsum(s[::-1] ** 2)[::-1]), 0.0)
+
+
+def choose_rank(s, rule, thr_rel, thr_abs):
+    """Smallest r with tail[r] <= threshold; threshold is thr_rel*||s||_2 for 'fixed' and
+    thr_abs for 'adaptive'.  codes/17_tlr_cholesky_pilot.py:113-115 (same rule at 130-132,
+    codes/11_tlr_rank_rules.py:92-98)."""
+    tail = singular_tail(s)
+    thr = thr_rel * np.sqrt((s ** 2).sum()) if rule == "fixed" else thr_abs
+    return int(np.argmax(tail <= thr)), tail
+
+
+def _svd(T, full_matrices=False):
+    # gesdd first, gesvd when it does not converge: codes/17_tlr_cholesky_pilot.py:109-112
+    try:
+        return np.linalg.svd(T, full_matrices=full_matrices)
+    except np.linalg.LinAlgError:
+        return scipy_svd(T, full_matrices=full_matrices, lapack_driver="gesvd")
+
+
+def truncate_svd(T, rule, thr_rel, thr_abs, rank=None):
+    """Rank-r truncation of a dense tile: returns (U*s, V, tail[r], r).
+
+    codes/17_tlr_cholesky_pilot.py:107-116.  ``rank`` overrides the rule (frozen ranks)."""
+    U, s, Vt = _svd(T)
+    r, tail = choose_rank(s, rule, thr_rel, thr_abs)
+    if rank is not None:
+        r = int(rank)
+    return U[:, :r] * s[:r], Vt[:r].T, float(tail[r]), r
+
+
+def recompress(U, V, rule, thr_rel, thr_abs, rank=None):
+    """Recompress U V^T: QR(U), QR(V), SVD of the k x k core R_u R_v^T, same rule.
+
+    codes/17_tlr_cholesky_pilot.py:119-133.  ``rank`` overrides the rule."""
+    if U.shape[1] == 0:
+        return U, V, 0.0, 0
+    Qu, Ru = np.linalg.qr(U)
+    Qv, Rv = np.linalg.qr(V)
+    Uw, s, Vwt = _svd(Ru @ Rv.T, full_matrices=True)
+    r, tail = choose_rank(s, rule, thr_rel, thr_abs)
+    if rank is not None:
+        r = int(rank)
+    return Qu @ (Uw[:, :r] * s[:r]), Qv @ Vwt[:r].T, float(tail[r]), r
+
+
+def thresholds(n, b, theta, rule, value):
+    """(thr_rel, thr_abs): fixed -> eps; adaptive -> tau * b * sigma2 * eta / N.
+
+    codes/17_tlr_cholesky_pilot.py:143-150 (b is the largest tile size)."""
+    sigma2, _, eta = theta
+    thr_rel = value if rule == "fixed" else None
+    thr_abs = value * b * sigma2 * eta / n if rule == "adaptive" else None
+    return thr_rel, thr_abs
+
+
+# ------------------------------------------------------------------ TLR Cholesky
+def tlr_cholesky(S, theta, bounds, rule, value, rank_log=None, frozen=None):
+    """Right-looking TLR Cholesky of Sigma(theta) without forming Sigma.
+
+    Returns (L_diag, L_off, info) or (None, None, info) when a diagonal tile is not
+    positive definite.  L_off[(i, j)] = (U, V), L_ij ~ U V^T, i > j, in the insertion
+    order of the reference (for k, for i > k).  codes/17_tlr_cholesky_pilot.py:137-215
+    for rules 'fixed' and 'adaptive'.
+
+    rank_log: optional dict, filled with {('init', i, j): r, ('rc', k, i, j): r}.
+    frozen:   optional dict of the same form; its ranks replace the rule's choice.
+    """
+    if rule not in ("fixed", "adaptive"):
+        raise ValueError(f"rule must be 'fixed' or 'adaptive', got {rule!r}")
+    n = S.shape[0]
+    nB = len(bounds)
+    b = max(e - s for s, e in bounds)
+    sigma2, rng, eta = theta
+    nugget = sigma2 * eta
+    thr_rel, thr_abs = thresholds(n, b, theta, rule, value)
+
+    def pick(key):
+        return None if frozen is None else frozen[key]
+
+    # tile generation + initial compression: 17:151-167
+    A_diag = []
+    A_off = {}
+    stored0 = 0
+    for i, (i0, i1) in enumerate(bounds):
+        D = sigma2 * matern32(pairwise_dist(S[i0:i1], S[i0:i1]), rng)
+        D[np.diag_indices_from(D)] += nugget
+        A_diag.append(D)
+        stored0 += (i1 - i0) ** 2
+        for j, (j0, j1) in enumerate(bounds[:i]):
+            T = sigma2 * matern32(pairwise_dist(S[i0:i1], S[j0:j1]), rng)
+            U, V, _, r = truncate_svd(T, rule, thr_rel, thr_abs, pick(("init", i, j)))
+            if rank_log is not None:
+                rank_log[("init", i, j)] = r
+            A_off[(i, j)] = (U, V)
+            stored0 += 2 * r * max(i1 - i0, j1 - j0)
+    sigma_ranks = [u.shape[1] for u, _ in A_off.values()]
+    info = dict(stored_sigma=int(stored0), max_rank_sigma=max(sigma_ranks) if sigma_ranks else 0,
+                sigma_ranks=sigma_ranks)
+
+    L_diag = [None] * nB
+    L_off = {}
+    for k in range(nB):
+        # diagonal POTRF: 17:171-177
+        try:
+            Lkk = cholesky(A_diag[k], lower=True, check_finite=False)
+        except LinAlgError:
+            info.update(completed=False, failed_at=k)
+            return None, None, info
+        L_diag[k] = Lkk
+        # panel TRSM, V <- L_kk^{-1} V: 17:178-185
+        for i in range(k + 1, nB):
+            U, V = A_off.pop((i, k))
+            if U.shape[1]:
+                V = solve_triangular(Lkk, V, lower=True, check_finite=False)
+            L_off[(i, k)] = (U, V)
+        # trailing update A_ij -= L_ik L_jk^T with recompression: 17:186-205
+        for i in range(k + 1, nB):
+            Ui, Vi = L_off[(i, k)]
+            if Ui.shape[1] == 0:
+                continue
+            for j in range(k + 1, i + 1):
+                Uj, Vj = L_off[(j, k)]
+                if Uj.shape[1] == 0:
+                    continue
+                W = Vi.T @ Vj
+                if i == j:
+                    A_diag[i] -= (Ui @ W) @ Ui.T
+                else:
+                    Uij, Vij = A_off[(i, j)]
+                    Ur, Vr, _, r = recompress(np.hstack([Uij, -(Ui @ W)]), np.hstack([Vij, Uj]),
+                                              rule, thr_rel, thr_abs, pick(("rc", k, i, j)))
+                    if rank_log is not None:
+                        rank_log[("rc", k, i, j)] = r
+                    A_off[(i, j)] = (Ur, Vr)
+    # storage statistics: 17:206-209
+    ranks = [u.shape[1] for u, _ in L_off.values()]
+    stored = sum(d.shape[0] ** 2 for d in L_diag) + sum(2 * u.shape[1] * u.shape[0] for u, _ in L_off.values())
+    info.update(completed=True, stored_factor=int(stored),
+                mean_rank_factor=float(np.mean(ranks)) if ranks else 0.0,
+                max_rank_factor=int(max(ranks)) if ranks else 0, factor_ranks=ranks)
+    return L_diag, L_off, info
+
+
+def tlr_matvec_L(L_diag, L_off, bounds, Z):
+    """Y = L Z for the tile factor.  codes/17_tlr_cholesky_pilot.py:218-227."""
+    Y = np.zeros_like(Z)
+    for k, (k0, k1) in enumerate(bounds):
+        Y[k0:k1] = L_diag[k] @ Z[k0:k1]
+        for j, (j0, j1) in enumerate(bounds[:k]):
+            U, V = L_off[(k, j)]
+            if U.shape[1]:
+                Y[k0:k1] += U @ (V.T @ Z[j0:j1])
+    return Y
+
+
+def tlr_forward(L_diag, L_off, bounds, B):
+    """Solve L Z = B tile by tile.  codes/17_tlr_cholesky_pilot.py:230-240."""
+    Z = np.zeros_like(B)
+    for k, (k0, k1) in enumerate(bounds):
+        rhs = B[k0:k1].copy()
+        for j, (j0, j1) in enumerate(bounds[:k]):
+            U, V = L_off[(k, j)]
+            if U.shape[1]:
+                rhs -= U @ (V.T @ Z[j0:j1])
+        Z[k0:k1] = solve_triangular(L_diag[k], rhs, lower=True, check_finite=False)
+    return Z
+
+
+def tlr_backward(L_diag, L_off, bounds, Z):
+    """Solve L^T X = Z tile by tile.  codes/17_tlr_cholesky_pilot.py:243-256."""
+    nB = len(bounds)
+    X = np.zeros_like(Z)
+    for k in range(nB - 1, -1, -1):
+        k0, k1 = bounds[k]
+        rhs = Z[k0:k1].copy()
+        for i in range(k + 1, nB):
+            i0, i1 = bounds[i]
+            U, V = L_off[(i, k)]
+            if U.shape[1]:
+                rhs -= V @ (U.T @ X[i0:i1])
+        X[k0:k1] = solve_triangular(L_diag[k], rhs, lower=True, trans="T", check_finite=False)
+    return X
+
+
+def tlr_loglik(S, y, theta, bounds, rule, value, rank_log=None, frozen=None):
+    """(loglik | None, (L_diag, L_off) | None, info).
+
+    l = -1/2 (z^T z + 2 sum log diag L_kk + N log 2 pi), z = L^{-1} y.
+    codes/17_tlr_cholesky_pilot.py:259-266."""
+    L_diag, L_off, info = tlr_cholesky(S, theta, bounds, rule, value, rank_log=rank_log, frozen=frozen)
+    if L_diag is None:
+        return None, None, info
+    z = tlr_forward(L_diag, L_off, bounds, y[:, None])[:, 0]
+    logdet = 2.0 * sum(np.log(np.diag(d)).sum() for d in L_diag)
+    ll = -0.5 * (z @ z + logdet + len(y) * LOG2PI)
+    info.update(logdet=float(logdet), quad=float(z @ z))
+    return float(ll), (L_diag, L_off), info
+
+
+def neg_loglik_tlr(logth, S, y, bounds, rule, value, trace):
+    """Optimizer wrapper: 1e12 on a failed factorization.  codes/17_tlr_cholesky_pilot.py:279-290."""
+    theta = np.exp(logth)
+    trace["evals"] += 1
+    if rule == "dense":
+        ll, _ = loglik_dense(cov_dense(S, theta), y)
+    else:
+        ll, _, _ = tlr_loglik(S, y, theta, bounds, rule, value)
+    if ll is None:
+        trace["failures"] += 1
+        return 1e12
+    return -ll
+
+
+# -------------------------------------------------------------------------- dense oracle
+def loglik_dense(K, y):
+    """Dense FP64 log-likelihood by Cholesky; (None, None) when K is not PD.
+
+    codes/11_tlr_rank_rules.py:112-120."""
+    try:
+        c = cholesky(K, lower=True, check_finite=False)
+    except LinAlgError:
+        return None, None
+    z = solve_triangular(c, y, lower=True, check_finite=False)
+    logdet = 2.0 * np.log(np.diag(c)).sum()
+    return float(-0.5 * (z @ z + logdet + len(y) * LOG2PI)), c
+
+
+def dense_loglik_and_grad(S, y, theta):
+    """Dense FP64 log-likelihood and its gradient in (sigma2, range, eta).
+
+    dl/dtheta = 1/2 alpha^T dK alpha - 1/2 tr(K^{-1} dK), alpha = K^{-1} y, with
+    dK/dsigma2 = K/sigma2, dK/drange = sigma2 x^2 e^{-x} / range (x = sqrt3 h/range),
+    dK/deta = sigma2 I.  No counterpart in the reference (it has no gradient code)."""
+    sigma2, rng, eta = theta
+    H = pairwise_dist(S, S)
+    x = SQRT3 * H / rng
+    M = (1.0 + x) * np.exp(-x)
+    K = sigma2 * M
+    K[np.diag_indices_from(K)] += sigma2 * eta
+    c = cholesky(K, lower=True, check_finite=False)
+    z = solve_triangular(c, y, lower=True, check_finite=False)
+    alpha = solve_triangular(c, z, lower=True, trans="T", check_finite=False)
+    Ci = solve_triangular(c, np.eye(len(y)), lower=True, check_finite=False)
+    Kinv = Ci.T @ Ci
+    ll = -0.5 * (z @ z + 2.0 * np.log(np.diag(c)).sum() + len(y) * LOG2PI)
+    dKs = M + eta * np.eye(len(y))
+    dKr = sigma2 * x * x * np.exp(-x) / rng
+    grads = []
+    for dK in (dKs, dKr, None):
+        if dK is None:
+            grads.append(0.5 * sigma2 * (alpha @ alpha) - 0.5 * sigma2 * np.trace(Kinv))
+        else:
+            grads.append(0.5 * alpha @ dK @ alpha - 0.5 * np.sum(Kinv * dK))
+    return float(ll), np.array(grads)
+
+
+# ---------------------------------------------------------- assembled-matrix rank rule
+def truncate_tiles(K, bounds, rule, value, m_theta):
+    """Truncate every off-diagonal tile of an assembled K in place.
+
+    Returns (stored, max_rel, max_abs, ||Delta||_F, ranks).  codes/11_tlr_rank_rules.py:74-108."""
+    n = K.shape[0]
+    b = max(e - s for s, e in bounds)
+    stored = sum((e - s) ** 2 for s, e in bounds)
+    emax = value * b * m_theta / n
+    ranks, max_rel, max_abs, fro2 = [], 0.0, 0.0, 0.0
+    for i, (i0, i1) in enumerate(bounds):
+        for j, (j0, j1) in enumerate(bounds[:i]):
+            T = K[i0:i1, j0:j1]
+            U, s, Vt = _svd(T)
+            r, tail = choose_rank(s, rule, value, emax)
+            Tr = (U[:, :r] * s[:r]) @ Vt[:r] if r > 0 else np.zeros_like(T)
+            err = tail[r]
+            K[i0:i1, j0:j1] = Tr
+            K[j0:j1, i0:i1] = Tr.T
+            stored += 2 * r * max(i1 - i0, j1 - j0)
+            ranks.append(r)
+            fro2 += 2 * err ** 2
+            max_abs = max(max_abs, err)
+            max_rel = max(max_rel, err / max(np.sqrt((s ** 2).sum()), 1e-300))
+    return stored, max_rel, max_abs, float(np.sqrt(fro2)), ranks
+
+
+# ------------------------------------------------------------------ data protocol
+def simulate_field(n, theta=(1.0, 0.3, 0.05), n_pred=300, seed=20261020):
+    """Seeded synthetic field: uniform sites, y = L z with L the dense FP64 Cholesky of
+    Sigma(S_all), a random split into n observed / n_pred held out, Morton order of the
+    observed sites.  codes/17_tlr_cholesky_pilot.py:313-325.
+
+    Returns (S, y, Sp, yp) with S, y Morton-ordered."""
+    rng = np.random.default_rng(seed)
+    theta = np.asarray(theta, float)
+    n_tot = n + n_pred
+    S_all = rng.random((n_tot, 2))
+    L = np.linalg.cholesky(cov_dense(S_all, theta))
+    y_all = L @ rng.standard_normal(n_tot)
+    del L
+    perm = rng.permutation(n_tot)
+    obs, hold = perm[:n], perm[n:]
+    S, y, Sp, yp = S_all[obs], y_all[obs], S_all[hold], y_all[hold]
+    order = morton_order(S)
+    return S[order], y[order], Sp, yp
+
+
+def simulate_sites(n, n_pred=300, seed=20261020):
+    """Sites only (no field), Morton-ordered, drawn in the same order as simulate_field
+    (S_all first, then the permutation is drawn after the field's normals)."""
+    rng = np.random.default_rng(seed)
+    S_all = rng.random((n + n_pred, 2))
+    rng.standard_normal(n + n_pred)
+    perm = rng.permutation(n + n_pred)
+    S = S_all[perm[:n]]
+    return S[morton_order(S)]

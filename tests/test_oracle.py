@@ -1,0 +1,95 @@
+"""The CPU oracle against the reference's own outputs (tests/golden, made by make_golden.py)
+and against the values the reference committed for N = 10,000."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import tlr_oracle as O
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def load_gold():
+    return json.load(open(os.path.join(GOLD, "golden.json")))
+
+
+def test_tile_bounds():
+    assert O.tile_bounds(10, 4) == [(0, 4), (4, 8), (8, 10)]
+    assert O.tile_bounds(8, 4) == [(0, 4), (4, 8)]
+    assert O.tile_bounds(3, 5) == [(0, 3)]
+
+
+def test_morton_matches_reference():
+    d = np.load(os.path.join(GOLD, "morton_case.npz"))
+    np.testing.assert_array_equal(O.morton_order(d["xy"]), d["perm"])
+
+
+@pytest.mark.parametrize("case", [c["name"] for c in load_gold()["cases"]])
+def test_oracle_matches_reference(case):
+    gold = {c["name"]: c for c in load_gold()["cases"]}[case]
+    d = np.load(os.path.join(GOLD, gold["data"]))
+    S, y = d["S"], d["y"]
+    bounds = O.tile_bounds(gold["n"], gold["b"])
+    ll_dense, _ = O.loglik_dense(O.cov_dense(S, gold["theta"]), y)
+    assert abs(ll_dense - gold["dense_loglik"]) <= 1e-10 * abs(gold["dense_loglik"])
+    for rec in gold["rules"]:
+        ll, fac, info = O.tlr_loglik(S, y, gold["theta"], bounds, rec["rule"], rec["value"])
+        assert info["sigma_ranks"] == rec["sigma_ranks"]
+        assert info["stored_sigma"] == rec["stored_sigma"]
+        assert info["completed"] == rec["completed"]
+        if rec["completed"]:
+            assert info["factor_ranks"] == rec["factor_ranks"]
+            assert info["stored_factor"] == rec["stored_factor"]
+            assert abs(ll - rec["loglik"]) <= 1e-10 * abs(rec["loglik"])
+        else:
+            assert info["failed_at"] == rec["failed_at"]
+
+
+@pytest.mark.slow
+def test_oracle_reproduces_committed_n10000():
+    """results/tlr_cholesky/tlr_cholesky_n10000.json: dense and TLR log-likelihoods on the
+    reference's own simulated field (regenerated here by the same seeded protocol)."""
+    com = load_gold()["committed_n10000"]
+    S, y, _, _ = O.simulate_field(10000)
+    bounds = O.tile_bounds(10000, 250)
+    ll_dense, _ = O.loglik_dense(O.cov_dense(S, (1.0, 0.3, 0.05)), y)
+    assert abs(ll_dense - com["dense_loglik"]) <= 1e-9 * abs(com["dense_loglik"])
+    for rec in com["rules"]:
+        if rec["rule"] != "adaptive" and rec["value"] not in (1e-3, 1e-4):
+            continue
+        ll, _, info = O.tlr_loglik(S, y, (1.0, 0.3, 0.05), bounds, rec["rule"], rec["value"])
+        assert info["stored_sigma"] == rec["stored_sigma"]
+        assert info["completed"] == rec["completed"]
+        if rec["completed"]:
+            assert info["stored_factor"] == rec["stored_factor"]
+            assert info["max_rank_factor"] == rec["max_rank_factor"]
+            assert abs(info["mean_rank_factor"] - rec["mean_rank_factor"]) < 1e-12
+            assert abs((ll - ll_dense) - rec["loglik_err"]) <= 1e-7
+        else:
+            assert info["failed_at"] == rec["failed_at_tile"]
+
+
+def test_frozen_ranks_replay():
+    """Replaying the recorded ranks at the same theta gives the same log-likelihood."""
+    d = np.load(os.path.join(GOLD, "n1030_b100_data.npz"))
+    S, y = d["S"], d["y"]
+    bounds = O.tile_bounds(1030, 100)
+    log = {}
+    ll, _, _ = O.tlr_loglik(S, y, (1.0, 0.3, 0.05), bounds, "adaptive", 0.9, rank_log=log)
+    ll2, _, _ = O.tlr_loglik(S, y, (1.0, 0.3, 0.05), bounds, "adaptive", 0.9, frozen=log)
+    assert ll == ll2
+
+
+def test_dense_gradient_matches_finite_differences():
+    d = np.load(os.path.join(GOLD, "n1030_b100_data.npz"))
+    S, y = d["S"][:300], d["y"][:300]
+    th = np.array([1.0, 0.3, 0.05])
+    _, g = O.dense_loglik_and_grad(S, y, th)
+    for a in range(3):
+        h = 1e-5 * th[a]
+        tp, tm = th.copy(), th.copy()
+        tp[a] += h; tm[a] -= h
+        fd = (O.loglik_dense(O.cov_dense(S, tp), y)[0] - O.loglik_dense(O.cov_dense(S, tm), y)[0]) / (2 * h)
+        assert abs(fd - g[a]) <= 1e-5 * max(1.0, abs(g[a]))
