@@ -17,6 +17,9 @@ TLR_RULE_ADAPTIVE = 1
 
 _lib = None
 
+KERNEL_KINDS = ["fill", "gen_offdiag", "sketch", "orth", "project", "resid", "finalize", "diag_build", "potrf",
+                "trsm", "recompress", "finish"]
+
 
 class TlrInfo(ctypes.Structure):
     _fields_ = [
@@ -50,6 +53,10 @@ SIGNATURES = {
     "tlr_get_diag_tile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "tlr_get_offdiag_tile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                             ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    "tlr_plan_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tlr_plan_kernel_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                             ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double),
+                                             ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int]),
     "tlr_last_error": (ctypes.c_char_p, []),
 }
 

@@ -58,6 +58,15 @@ struct tlr_plan {
   // host copies
   std::vector<int> h_rank, h_rank0, h_ti, h_tj;
   std::vector<void*> allocs;
+  // launch accounting and optional per-kernel event timing
+  bool prof = false;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  std::vector<int> ev_kind;
+  double kms[TLR_NKINDS] = {0};
+  long long klaunch[TLR_NKINDS] = {0};
+  double kflops[TLR_NKINDS] = {0};
+  double kbytes[TLR_NKINDS] = {0};
 };
 
 namespace {
@@ -87,9 +96,25 @@ void free_all(tlr_plan* p) {
     if (_rc != 0) return _rc;       \
   } while (0)
 
-#define TRYK(x)                                                                   \
-  do {                                                                            \
-    const int _rc = (x);                                                          \
+cudaEvent_t next_event(tlr_plan* p) {
+  if (p->ev_used == p->ev_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    p->ev_pool.push_back(e);
+  }
+  return p->ev_pool[p->ev_used++];
+}
+
+// launch one kernel of kind `kind`; with profiling on, bracket it by two events
+#define LAUNCH(kind, x)                                                             \
+  do {                                                                              \
+    if (p->prof) {                                                                  \
+      cudaEventRecord(next_event(p), p->stream);                                    \
+      p->ev_kind.push_back(kind);                                                   \
+    }                                                                               \
+    const int _rc = (x);                                                            \
+    if (p->prof) cudaEventRecord(next_event(p), p->stream);                         \
+    p->klaunch[kind] += 1;                                                          \
     if (_rc != 0) return fail(TLR_ERR_CUDA, std::string("kernel launch failed: ") + \
                                                 cudaGetErrorString((cudaError_t)_rc)); \
   } while (0)
@@ -100,23 +125,23 @@ int run_compression(tlr_plan* p, double sigma2, double inv_range, int rule_fixed
   const int ldp = kMaxK;
   for (int base = 0; base < p->ntiles; base += p->chunk) {
     const int nc = std::min(p->chunk, p->ntiles - base);
-    TRYK(tlr::launch_fill_int(p->need, 1, nc, s));
-    TRYK(tlr::launch_gen_offdiag(p->xy, p->n, p->b, base, p->ti, p->tj, p->T, nc, sigma2, inv_range, p->status, s));
+    LAUNCH(TLR_K_FILL, tlr::launch_fill_int(p->need, 1, nc, s));
+    LAUNCH(TLR_K_GEN, tlr::launch_gen_offdiag(p->xy, p->n, p->b, base, p->ti, p->tj, p->T, nc, sigma2, inv_range, p->status, s));
     for (int lev = 0; lev < kLevels; ++lev) {
       const int k = 16 << lev;
       double* Pp = p->P;
       double* Zp = p->Z;
       for (int it = 0; it < kPowerPasses; ++it) {
-        TRYK(tlr::launch_sketch(p->T, p->n, p->b, k, base, p->ti, p->tj, p->need, Pp, Zp, ldp, it == 0 ? 1 : 0, 0,
+        LAUNCH(TLR_K_SKETCH, tlr::launch_sketch(p->T, p->n, p->b, k, base, p->ti, p->tj, p->need, Pp, Zp, ldp, it == 0 ? 1 : 0, 0,
                                 nc, p->status, s));
-        TRYK(tlr::launch_orth(Zp, p->n, p->b, k, ldp, base, p->tj, p->need, p->gscr, nc, p->status, s));
+        LAUNCH(TLR_K_ORTH, tlr::launch_orth(Zp, p->n, p->b, k, ldp, base, p->tj, p->need, p->gscr, nc, p->status, s));
         std::swap(Pp, Zp);
       }
-      TRYK(tlr::launch_sketch(p->T, p->n, p->b, k, base, p->ti, p->tj, p->need, Pp, p->C, ldp, 0, 1, nc, p->status,
+      LAUNCH(TLR_K_PROJECT, tlr::launch_sketch(p->T, p->n, p->b, k, base, p->ti, p->tj, p->need, Pp, p->C, ldp, 0, 1, nc, p->status,
                               s));
-      TRYK(tlr::launch_resid(p->T, p->n, p->b, k, ldp, base, p->ti, p->tj, p->need, Pp, p->C, p->parts, p->fparts,
+      LAUNCH(TLR_K_RESID, tlr::launch_resid(p->T, p->n, p->b, k, ldp, base, p->ti, p->tj, p->need, Pp, p->C, p->parts, p->fparts,
                              p->nblk, nc, p->status, s));
-      TRYK(tlr::launch_finalize(p->n, p->b, k, ldp, p->cap, kMargin, rule_fixed, thr_rel, thr_abs, base, p->ti,
+      LAUNCH(TLR_K_FINALIZE, tlr::launch_finalize(p->n, p->b, k, ldp, p->cap, kMargin, rule_fixed, thr_rel, thr_abs, base, p->ti,
                                 p->tj, p->need, Pp, p->C, p->parts, p->fparts, p->nblk, p->gscr, p->gsv, p->U, p->V,
                                 p->rank, lev == kLevels - 1 ? 1 : 0, nc, p->status, s));
     }
@@ -128,14 +153,14 @@ int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugge
                       double thr_abs) {
   cudaStream_t s = p->stream;
   for (int k = 0; k < p->nB; ++k) {
-    TRYK(tlr::launch_diag_build(p->xy, p->n, p->b, k, sigma2, inv_range, nugget, p->U, p->Wd, p->rank, p->cap, p->D,
+    LAUNCH(TLR_K_DIAG, tlr::launch_diag_build(p->xy, p->n, p->b, k, sigma2, inv_range, nugget, p->U, p->Wd, p->rank, p->cap, p->D,
                                 p->status, s));
-    TRYK(tlr::launch_potrf(p->D, p->n, p->b, k, p->rhs, p->z, p->ldpart, p->qpart, p->status, s));
-    TRYK(tlr::launch_trsm(p->D, p->n, p->b, k, p->nB, p->U, p->V, p->Wd, p->rank, p->cap, p->z, p->rhs, p->status, s));
-    TRYK(tlr::launch_recompress(p->n, p->b, k, p->nB, p->U, p->V, p->rank, p->cap, rule_fixed, thr_rel, thr_abs,
+    LAUNCH(TLR_K_POTRF, tlr::launch_potrf(p->D, p->n, p->b, k, p->rhs, p->z, p->ldpart, p->qpart, p->status, s));
+    LAUNCH(TLR_K_TRSM, tlr::launch_trsm(p->D, p->n, p->b, k, p->nB, p->U, p->V, p->Wd, p->rank, p->cap, p->z, p->rhs, p->status, s));
+    LAUNCH(TLR_K_RECOMPRESS, tlr::launch_recompress(p->n, p->b, k, p->nB, p->U, p->V, p->rank, p->cap, rule_fixed, thr_rel, thr_abs,
                                 p->rcs, p->slot_doubles, p->nslots, p->status, s));
   }
-  TRYK(tlr::launch_finish(p->nB, p->n, p->ldpart, p->qpart, p->out, p->status, s));
+  LAUNCH(TLR_K_FINISH, tlr::launch_finish(p->nB, p->n, p->ldpart, p->qpart, p->out, p->status, s));
   return 0;
 }
 
@@ -200,7 +225,8 @@ int tlr_plan_create(tlr_plan** plan, int n, int b, int cap, int device, void* st
   A(dalloc(p, &p->ldpart, (size_t)p->nB));
   A(dalloc(p, &p->qpart, (size_t)p->nB));
   A(dalloc(p, &p->out, 4));
-  A(dalloc(p, &p->status, 1));
+  // control block: status, padding, [flops, bytes] per kernel kind
+  A(dalloc(p, &p->status, 4 + 4 * TLR_NKINDS));
   if (rc != 0) {
     free_all(p);
     delete p;
@@ -234,6 +260,7 @@ void tlr_plan_destroy(tlr_plan* plan) {
   if (!plan) return;
   cudaSetDevice(plan->device);
   if (plan->stream) cudaStreamSynchronize(plan->stream);
+  for (cudaEvent_t e : plan->ev_pool) cudaEventDestroy(e);
   free_all(plan);
   delete plan;
 }
@@ -336,7 +363,7 @@ int tlr_loglik(tlr_plan* p, const double theta[3], int rule, double value, doubl
   const int rule_fixed = rule == TLR_RULE_FIXED;
   const double thr_rel = rule_fixed ? value : 0.0;
   const double thr_abs = rule_fixed ? 0.0 : value * (double)std::min(p->b, p->n) * sigma2 * eta / (double)p->n;
-  TRY(cuda_check(cudaMemsetAsync(p->status, 0, sizeof(int), s), "reset status"));
+  TRY(cuda_check(cudaMemsetAsync(p->status, 0, sizeof(int) * (4 + 4 * TLR_NKINDS), s), "reset status"));
   TRY(cuda_check(cudaMemsetAsync(p->rank, 0, sizeof(int) * std::max(p->ntiles, 1), s), "reset ranks"));
   TRY(cuda_check(cudaMemcpyAsync(p->rhs, p->y, sizeof(double) * p->n, cudaMemcpyDeviceToDevice, s), "rhs"));
   TRY(run_compression(p, sigma2, 1.0 / range, rule_fixed, thr_rel, thr_abs));
@@ -348,6 +375,9 @@ int tlr_loglik(tlr_plan* p, const double theta[3], int rule, double value, doubl
   double out[4] = {0, 0, 0, 0};
   TRY(cuda_check(cudaMemcpyAsync(&status, p->status, sizeof(int), cudaMemcpyDeviceToHost, s), "status"));
   TRY(cuda_check(cudaMemcpyAsync(out, p->out, sizeof(double) * 3, cudaMemcpyDeviceToHost, s), "out"));
+  double work[2 * TLR_NKINDS];
+  TRY(cuda_check(cudaMemcpyAsync(work, p->status + 4, sizeof(double) * 2 * TLR_NKINDS, cudaMemcpyDeviceToHost, s),
+                 "work"));
   if (p->ntiles > 0) {
     TRY(cuda_check(cudaMemcpyAsync(p->h_rank.data(), p->rank, sizeof(int) * p->ntiles, cudaMemcpyDeviceToHost, s),
                    "ranks"));
@@ -355,6 +385,19 @@ int tlr_loglik(tlr_plan* p, const double theta[3], int rule, double value, doubl
                    "ranks0"));
   }
   TRY(cuda_check(cudaStreamSynchronize(s), "evaluation"));
+  if (p->prof) {
+    for (size_t q = 0; q < p->ev_kind.size(); ++q) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, p->ev_pool[2 * q], p->ev_pool[2 * q + 1]);
+      p->kms[p->ev_kind[q]] += ms;
+    }
+  }
+  p->ev_used = 0;
+  p->ev_kind.clear();
+  for (int q = 0; q < TLR_NKINDS; ++q) {
+    p->kflops[q] += work[2 * q];
+    p->kbytes[q] += work[2 * q + 1];
+  }
   if (status < 0) {
     const char* why = status == TLR_ERR_RANK_CAP ? "a tile rank exceeded the plan's rank capacity"
                       : status == TLR_ERR_COMPRESS ? "a tile needed more than 120 singular directions"
@@ -376,6 +419,31 @@ int tlr_loglik_host(tlr_plan* p, const double* xy_host, const double* y_host, co
                  "copy observations"));
   p->has_data = true;
   return tlr_loglik(p, theta, rule, value, loglik, info, factor_ranks, sigma_ranks);
+}
+
+int tlr_plan_set_profiling(tlr_plan* p, int on) {
+  if (!p) return fail(TLR_ERR_ARG, "plan is NULL");
+  p->prof = on != 0;
+  return 0;
+}
+
+int tlr_plan_kernel_stats(tlr_plan* p, double* ms, long long* launches, double* flops, double* bytes, int nkinds,
+                          int reset) {
+  if (!p) return fail(TLR_ERR_ARG, "plan is NULL");
+  for (int q = 0; q < nkinds && q < TLR_NKINDS; ++q) {
+    if (ms) ms[q] = p->kms[q];
+    if (launches) launches[q] = p->klaunch[q];
+    if (flops) flops[q] = p->kflops[q];
+    if (bytes) bytes[q] = p->kbytes[q];
+  }
+  if (reset)
+    for (int q = 0; q < TLR_NKINDS; ++q) {
+      p->kms[q] = 0.0;
+      p->klaunch[q] = 0;
+      p->kflops[q] = 0.0;
+      p->kbytes[q] = 0.0;
+    }
+  return 0;
 }
 
 int tlr_get_diag_tile(tlr_plan* p, int k, double* out_host) {

@@ -43,6 +43,7 @@ __global__ void k_gen_offdiag(const double* TLR_RESTRICT xy, int n, int b, int t
   const int bi = min(b, n - i0), bj = min(b, n - j0);
   double* Tc = T + (size_t)c * b * b;
   const int total = bi * bj;
+  if (blockIdx.x == 0 && threadIdx.x == 0) add_work(status, 1, 0.0, 8.0 * total);
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
     const int a = e / bj, q = e - a * bj;
     const double2 pa = reinterpret_cast<const double2*>(xy)[i0 + a];
@@ -67,6 +68,9 @@ __global__ void __launch_bounds__(256) k_sketch(const double* TLR_RESTRICT T, in
   if (!need[c]) return;
   const int t = (tile_base + c);
   const int bi = min(b, n - ti[t] * b), bj = min(b, n - tj[t] * b);
+  if (threadIdx.x == 0)
+    add_work(status, mode == 0 ? 2 : 4, (mode == 0 ? 4.0 : 2.0) * bi * bj * 16,
+             8.0 * ((double)bi * bj + (omega ? 0.0 : bj * 16.0) + (mode == 0 ? bj : bi) * 16.0));
   extern __shared__ double smem[];
   double* Ps = smem;                       // [bj][16]
   double* Ts = Ps + (size_t)b * 16;        // [H][b + 1]
@@ -169,6 +173,7 @@ __global__ void __launch_bounds__(256) k_orth(double* TLR_RESTRICT Z, int n, int
   if (!need[c]) return;
   const int bj = min(b, n - tj[(tile_base + c)] * b);
   const int ke = min(k, bj);  // a tile narrower than k gets a full basis and zero columns
+  if (threadIdx.x == 0) add_work(status, 3, 4.0 * bj * ke * ke, 16.0 * bj * k);
   extern __shared__ double smem[];
   double* red = smem;         // 33
   double* tau = smem + 40;    // k
@@ -208,6 +213,7 @@ __global__ void __launch_bounds__(256) k_resid(const double* TLR_RESTRICT T, int
     return;
   }
   const int qn = min(64, bj - q0);
+  if (threadIdx.x == 0) add_work(status, 5, 2.0 * bi * qn * (k + 1), 8.0 * ((double)bi * qn + (bi + qn) * k));
   extern __shared__ double smem[];
   double* Pb = smem;              // [64][k+1]  P rows q0..q0+63
   double* Cs = Pb + 64 * (k + 1); // [16][k+1]  C rows of the strip
@@ -263,6 +269,7 @@ __global__ void __launch_bounds__(256) k_finalize(int n, int b, int k, int ldp, 
   if (!need[c]) return;
   const int t = (tile_base + c);
   const int bi = min(b, n - ti[t] * b), bj = min(b, n - tj[t] * b);
+  if (threadIdx.x == 0) add_work(status, 6, 4.0 * bi * k * k + 6.0 * 8.0 * k * k * k, 8.0 * (bi + bj) * k);
   extern __shared__ double smem[];
   double* red = smem;             // 33 (+pad)
   double* tau = smem + 40;        // k

@@ -45,6 +45,15 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return red[32];
 }
 
+// ---------------------------------------------------------------- work counters
+// The plan's control block: int status, three ints of padding, then [flops, bytes] doubles per
+// kernel kind (algorithmic counts, accumulated by the kernels for the roofline report).
+__device__ __forceinline__ void add_work(const int* status, int kind, double flops, double bytes) {
+  double* w = reinterpret_cast<double*>(const_cast<int*>(status) + 4);
+  atomicAdd(w + 2 * kind, flops);
+  atomicAdd(w + 2 * kind + 1, bytes);
+}
+
 // ---------------------------------------------------------------- covariance model
 // Matern nu=3/2 kernel sigma2 (1 + x) e^{-x}, x = sqrt(3) h / range
 // (codes/11_tlr_rank_rules.py:35-37 with the sigma2 scaling of codes/17_tlr_cholesky_pilot.py:161).

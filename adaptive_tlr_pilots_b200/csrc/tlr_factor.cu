@@ -31,6 +31,11 @@ __global__ void __launch_bounds__(256) k_diag_build(const double* TLR_RESTRICT x
   const int cb = blk;
   const int bk = min(b, n - k * b);
   const int r0 = rb * 32, c0 = cb * 32;
+  if (threadIdx.x == 0 && rb == cb && rb == 0) {
+    double fl = 0.0;
+    for (int mt = 0; mt < k; ++mt) fl += 2.0 * bk * bk * rank[tidx(k, mt)];
+    add_work(status, 7, 0.5 * fl, 4.0 * bk * bk);
+  }
   __shared__ double Ua[32][33], Uc[32][33], Xc[32][33];
   const int cl = threadIdx.x & 31, rl = threadIdx.x >> 5;
   double acc[4];
@@ -104,7 +109,11 @@ __global__ void __launch_bounds__(512) k_potrf(double* TLR_RESTRICT D, int n, in
   __shared__ double logdet_acc;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int LD = NB + 1;
-  if (tid == 0) { fail = 0; logdet_acc = 0.0; }
+  if (tid == 0) {
+    fail = 0;
+    logdet_acc = 0.0;
+    add_work(status, 8, (double)bk * bk * bk / 3.0 + (double)bk * bk, 8.0 * bk * bk);
+  }
   for (int p0 = 0; p0 < bk; p0 += NB) {
     const int pw = min(NB, bk - p0);
     __syncthreads();
@@ -259,6 +268,8 @@ __global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int 
   const double* L = D + (size_t)k * b * b;
   double* Vt = V + (size_t)t * b * cap;
   const double* Ut = U + (size_t)t * b * cap;
+  if (threadIdx.x == 0) add_work(status, 9, (double)bk * bk * r + 2.0 * bk * r * r + 4.0 * bk * r,
+                                 8.0 * ((double)bk * bk * 0.5 + 2.0 * bk * r + bi * r));
   __shared__ double L11[32][33];
   __shared__ double Xp[32][65];
   __shared__ double red[40];
@@ -420,6 +431,11 @@ __global__ void __launch_bounds__(256) k_recompress(int n, int b, int k, int nB,
   __shared__ int iflag;
   __shared__ int rsel;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (blockIdx.x == 0 && tid == 0) {  // the panel column k is read once per step
+    double by = 0.0;
+    for (int i = k + 1; i < nB; ++i) by += 8.0 * 2.0 * b * rank[tidx(i, k)];
+    add_work(status, 10, 0.0, by);
+  }
   for (long pp = blockIdx.x; pp < npairs; pp += gridDim.x) {
     // decode pp -> (ii, jj), ii > jj >= 0 within the trailing block
     int ii = (int)((1.0 + sqrt(1.0 + 8.0 * (double)pp)) * 0.5);
@@ -572,6 +588,9 @@ __global__ void __launch_bounds__(256) k_recompress(int n, int b, int k, int nB,
     __syncthreads();
     const int rn = rsel;
     if (rn < 0) return;
+    if (tid == 0)  // 4 b r_ik r_jk + 8 b s^2 + 4 b s r' flops; old and new pair read / written
+      add_work(status, 10, 4.0 * b * ri * rj + 8.0 * b * s * s + 4.0 * b * s * rn,
+               8.0 * ((double)(bi + bj) * r1 + (double)(bi + bj) * rn));
     // G = R_v^T Vs_r (s x rn), H = W G_bottom (ri x rn)
     for (int e = tid; e < s * rn; e += 256) {
       const int t = e % s, c = e / s;

@@ -149,6 +149,21 @@ class Plan:
             d.update(failed_at=int(info.failed_at))
         return Evaluation(rc, float(ll.value) if rc == 0 else None, d, fr[: self.ntiles], sr[: self.ntiles])
 
+    def set_profiling(self, on=True):
+        """Bracket every launch with CUDA events (per-kernel device time; results unchanged)."""
+        _lib.check(self.lib.tlr_plan_set_profiling(self.handle, 1 if on else 0))
+
+    def kernel_stats(self, reset=False):
+        """{kernel kind: dict(ms, launches, flops, bytes)} accumulated since the last reset
+        (ms needs profiling on; flops/bytes are the kernels' own algorithmic counts)."""
+        nk = len(_lib.KERNEL_KINDS)
+        ms = (ctypes.c_double * nk)()
+        cnt = (ctypes.c_longlong * nk)()
+        fl = (ctypes.c_double * nk)()
+        by = (ctypes.c_double * nk)()
+        _lib.check(self.lib.tlr_plan_kernel_stats(self.handle, ms, cnt, fl, by, nk, 1 if reset else 0))
+        return {k: dict(ms=ms[q], launches=cnt[q], flops=fl[q], bytes=by[q]) for q, k in enumerate(_lib.KERNEL_KINDS)}
+
     # factor access (checking / prediction)
     def diag_tile(self, k):
         bk = min(self.b, self.n - k * self.b)
@@ -253,15 +268,22 @@ def dense_loglik(S, y, theta, device=0):
     St = torch.as_tensor(np.asarray(S, dtype=np.float64), device=dev)
     yt = torch.as_tensor(np.asarray(y, dtype=np.float64), device=dev)
     sigma2, rng, eta = [float(v) for v in theta]
-    x = (3.0 ** 0.5) * torch.cdist(St, St) / rng
-    K = sigma2 * (1.0 + x) * torch.exp(-x)
-    K.diagonal().add_(sigma2 * eta)
-    L, info = torch.linalg.cholesky_ex(K)
-    if int(info.item()) != 0:
-        return None
-    z = torch.linalg.solve_triangular(L, yt[:, None], upper=False)[:, 0]
-    ld = 2.0 * torch.log(torch.diagonal(L)).sum()
-    return float(-0.5 * (z @ z + ld + len(yt) * np.log(2 * np.pi)))
+    with torch.no_grad():
+        K = torch.cdist(St, St)
+        K.mul_((3.0 ** 0.5) / rng)
+        E = torch.exp(-K)
+        K.add_(1.0).mul_(E).mul_(sigma2)
+        del E
+        K.diagonal().add_(sigma2 * eta)
+        L, info = torch.linalg.cholesky_ex(K)
+        del K
+        if int(info.item()) != 0:
+            return None
+        z = torch.linalg.solve_triangular(L, yt[:, None], upper=False)[:, 0]
+        ld = 2.0 * torch.log(torch.diagonal(L)).sum()
+        out = float(-0.5 * (z @ z + ld + len(yt) * np.log(2 * np.pi)))
+        del L
+    return out
 
 
 def loglik(theta, locs, y, b, rule, tau=None, eps=None, ordered=False, cap=64, device=0):

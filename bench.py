@@ -1,0 +1,264 @@
+#!/usr/bin/env python
+"""Benchmark of the TLR Gaussian-process log-likelihood on B200.
+
+Workload: N = 50,000 seeded sites (the reference's data protocol, codes/17_tlr_cholesky_pilot.py:
+313-325), Morton-ordered, tiles b = 500, Matern-3/2 at theta = (1, 0.3, 0.05), adaptive rule
+tau = 0.9; one step = one full log-likelihood evaluation (tile generation, compression, TLR
+Cholesky, solve) on the plain FP64 path.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With --gpus N > 1 (launched by torch.distributed.run) every rank evaluates its own replica of the
+workload (independent evaluations, no collective on the data path: weak scaling); the device time
+is the max over ranks.  --impl reference times the reference pipeline on the host's cores
+(the CPU oracle, a restatement of codes/17_tlr_cholesky_pilot.py) on a bounded sample.
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+THETA = (1.0, 0.3, 0.05)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=50000)
+    ap.add_argument("--b", type=int, default=500)
+    ap.add_argument("--tau", type=float, default=0.9)
+    ap.add_argument("--cpu-sample", type=int, default=1, help="0: skip the CPU baseline leg")
+    return ap.parse_args()
+
+
+METRIC = "TLR loglik evals/s at N=50k, b=500, adaptive tau=0.9 (plain FP64 path)"
+
+
+def workload(a):
+    return {"workload": f"TLR log-likelihood, N={a.n}, b={a.b}, Matern-3/2 theta=(1,0.3,0.05), adaptive tau={a.tau}",
+            "n": a.n, "b": a.b, "rule": "adaptive", "tau": a.tau, "precision": "fp64 plain",
+            "l2": "inputs larger than L2 (per-evaluation working set several GB)"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        mx = max((float(r[2]) for r in rows if r[2].replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if r[5 + q].lower().startswith("active")})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def cpu_baseline(S, y, a):
+    from oracle.cpu_sample import SampledPipeline, blas_threads
+    t0 = time.perf_counter()
+    sp = SampledPipeline(S, y, THETA, a.b, "adaptive", a.tau, n_pairs=48)
+    setup = time.perf_counter() - t0
+    est, wall = sp.step(n_compress=12, n_trsm=16, n_recompress=48)
+    return {"value": 1.0 / est, "unit": "evals/s", "cores": blas_threads(), "kind": "port",
+            "sample": (f"oracle (NumPy/SciPy restatement of codes/17_tlr_cholesky_pilot.py) per-tile operations at "
+                       f"N={a.n}, b={a.b}: 12 tile compressions, 1 POTRF, 16 panel solves/diag updates, 48 step-0 "
+                       f"recompressions timed ({wall:.1f} s, setup {setup:.1f} s) and scaled by their counts in one "
+                       f"evaluation; estimated {est:.1f} s per evaluation")}
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import numpy as np  # noqa: F401
+
+    from adaptive_tlr_pilots_b200 import synth
+    from oracle import tlr_oracle as O
+    from oracle.cpu_sample import SampledPipeline, blas_threads
+    S, y, _, _ = synth.simulate_field(a.n, THETA, order_fn=O.morton_order)
+    sp = SampledPipeline(S, y, THETA, a.b, "adaptive", a.tau, n_pairs=48)
+    for w in range(a.warmup):
+        sp.step(n_compress=4, n_trsm=4, n_recompress=8, seed=100 + w)
+    ests, walls = [], []
+    for s in range(a.steps):
+        est, wall = sp.step(n_compress=6, n_trsm=8, n_recompress=24, seed=s)
+        ests.append(est)
+        walls.append(wall)
+    est = sum(ests) / len(ests)
+    value = 1.0 / est
+    sample = (f"oracle port of codes/17_tlr_cholesky_pilot.py per-tile operations at N={a.n}, b={a.b}: per step 6 "
+              f"compressions, 1 POTRF, 8 panel solves/diag updates, 24 step-0 recompressions, scaled by their counts "
+              f"in one evaluation ({est:.1f} s per evaluation estimated)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 * est, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded reference protocol)",
+            "config": workload(a),
+            "cpu_baseline": {"value": value, "unit": "evals/s", "cores": blas_threads(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+        return
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import adaptive_tlr_pilots_b200 as tlr
+    from adaptive_tlr_pilots_b200 import synth
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    S, y, _, _ = synth.simulate_field(a.n, THETA, device=local)
+    plan = tlr.Plan(a.n, a.b, cap=64, device=local)
+    plan.set_data(S, y)
+    for _ in range(a.warmup):
+        ev = plan.evaluate(THETA, "adaptive", a.tau)
+    plan.set_profiling(True)
+    plan.kernel_stats(reset=True)
+    sampler = ClockSampler(local)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(a.steps):
+        ev = plan.evaluate(THETA, "adaptive", a.tau)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    stats = plan.kernel_stats(reset=True)
+    plan.set_profiling(False)
+    t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+
+    # end to end through the public drop-in (host buffers in pinned memory, copies inside)
+    S_pin = torch.from_numpy(np.ascontiguousarray(S)).pin_memory().numpy()
+    y_pin = torch.from_numpy(np.ascontiguousarray(y)).pin_memory().numpy()
+    bounds = tlr.tile_bounds(a.n, a.b)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(a.steps):
+        ll_e2e, _, info_e2e = tlr.tlr_loglik(S_pin, y_pin, THETA, bounds, "adaptive", a.tau, device=local)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1)
+    t = torch.tensor([ms_e2e], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_e2e = float(t.item())
+    ntiles = plan.ntiles
+    h2d = S_pin.nbytes + y_pin.nbytes
+    d2h = 4 + 8 * 3 + 8 * 2 * 12 + 2 * 4 * ntiles
+
+    if rank == 0:
+        dense = synth.dense_loglik_gpu(S, y, THETA, device=local)
+        pk, pk_kind = peaks()
+        launches = int(sum(v["launches"] for v in stats.values()))
+        top = max(stats, key=lambda k: stats[k]["ms"])
+        st = stats[top]
+        per_launch_ms = st["ms"] / max(st["launches"], 1)
+        achieved_gbs = st["bytes"] / max(st["launches"], 1) / (per_launch_ms * 1e-3) / 1e9
+        roof = {"kernel": top, "bound": "hbm", "achieved": achieved_gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved_gbs / pk["hbm_gbs"], "traffic": None, "peak_kind": pk_kind,
+                "fp64_tflops": st["flops"] / max(st["launches"], 1) / (per_launch_ms * 1e-3) / 1e12,
+                "fp64_peak_nominal_tflops": 37.0,
+                "share": st["ms"] / sum(v["ms"] for v in stats.values()),
+                "per_launch_ms": per_launch_ms, "launches_per_step": st["launches"] / a.steps}
+        kern = {k: {"ms_per_step": v["ms"] / a.steps, "launches_per_step": v["launches"] / a.steps,
+                    "gflop_per_step": v["flops"] / a.steps / 1e9, "gb_per_step": v["bytes"] / a.steps / 1e9}
+                for k, v in stats.items() if v["launches"]}
+        line = {"metric": METRIC, "value": world * a.steps / (ms_max / 1e3), "unit": "evals/s", "n_gpus": world,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded reference protocol, y = L z with the dense FP64 Cholesky)",
+                "config": dict(workload(a), parallelism=f"replicas x{world}"),
+                "loglik": ev.loglik, "dense_loglik": dense,
+                "abs_dloglik_vs_dense": None if dense is None else abs(ev.loglik - dense),
+                "mean_rank_factor": ev.info["mean_rank_factor"], "max_rank_factor": ev.info["max_rank_factor"],
+                "e2e": {"value": world * a.steps / (ms_e2e / 1e3), "unit": "evals/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h},
+                "gpu_launches": launches, "roofline": roof, "kernels": kern, "clocks": clocks}
+        if world == 1 and a.cpu_sample:
+            line["cpu_baseline"] = cpu_baseline(S, y, a)
+        print(json.dumps(line), flush=True)
+    plan.close()
+    tlr.release_plans()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

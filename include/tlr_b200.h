@@ -89,6 +89,30 @@ int tlr_loglik_host(tlr_plan* plan, const double* xy_host, const double* y_host,
 int tlr_get_diag_tile(tlr_plan* plan, int k, double* out_host);
 int tlr_get_offdiag_tile(tlr_plan* plan, int i, int j, double* u_host, double* v_host, int* rank);
 
+/* Kernel kinds counted by tlr_plan_kernel_stats (launches issued by the plan's evaluations). */
+#define TLR_K_FILL 0
+#define TLR_K_GEN 1        /* off-diagonal tile generation */
+#define TLR_K_SKETCH 2     /* Z = T^T (T P) */
+#define TLR_K_ORTH 3       /* Householder orthonormalisation of the sketch */
+#define TLR_K_PROJECT 4    /* C = T P */
+#define TLR_K_RESID 5      /* ||T - C P^T||_F^2 */
+#define TLR_K_FINALIZE 6   /* rank decision + truncated pair */
+#define TLR_K_DIAG 7       /* diagonal tile generation + deferred updates */
+#define TLR_K_POTRF 8      /* diagonal Cholesky + forward-solve block */
+#define TLR_K_TRSM 9       /* panel solve */
+#define TLR_K_RECOMPRESS 10 /* Schur update + recompression */
+#define TLR_K_FINISH 11
+#define TLR_NKINDS 12
+
+/* Profiling: when on, every launch is bracketed by CUDA events on the plan's stream and the
+ * per-kind device time is accumulated (no effect on results).  No reference counterpart. */
+int tlr_plan_set_profiling(tlr_plan* plan, int on);
+/* Per-kind accumulated device milliseconds (profiling on), launch counts and algorithmic work
+ * (FP64 flops and HBM bytes the kernels count for themselves) since the last reset.  Any output
+ * pointer may be NULL.  No reference counterpart. */
+int tlr_plan_kernel_stats(tlr_plan* plan, double* ms, long long* launches, double* flops, double* bytes, int nkinds,
+                          int reset);
+
 /* Message of the last error on this thread. */
 const char* tlr_last_error(void);
 
