@@ -42,6 +42,8 @@ SIGNATURES = {
     "tlr_plan_destroy": (None, [ctypes.c_void_p]),
     "tlr_morton_order": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                         ctypes.c_void_p]),
+    "tlr_morton_order_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                                ctypes.c_void_p]),
     "tlr_set_data": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "tlr_loglik": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_double,
                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(TlrInfo),

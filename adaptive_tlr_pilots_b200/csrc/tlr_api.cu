@@ -34,6 +34,11 @@ constexpr int kMargin = 8;       // accepted rank must leave k - margin unresolv
 
 }  // namespace
 
+namespace tlr {
+// lets other translation units of the library report through tlr_last_error()
+int set_error(int code, const char* msg) { return fail(code, msg); }
+}  // namespace tlr
+
 struct tlr_plan {
   int n = 0, b = 0, nB = 0, ntiles = 0, cap = 0, device = 0;
   cudaStream_t stream = nullptr;

@@ -44,6 +44,9 @@ int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* ra
 int launch_finish(int nB, int n, const double* ldpart, const double* qpart, double* out, const int* status,
                   cudaStream_t s);
 
+// error reporting shared by the library's translation units (message for tlr_last_error)
+int set_error(int code, const char* msg);
+
 // small utilities
 int launch_fill_int(int* p, int v, int count, cudaStream_t s);
 

@@ -62,6 +62,18 @@ void tlr_plan_destroy(tlr_plan* plan);
  * (n int64): replaces morton_order, codes/11_tlr_rank_rules.py:40-53 (order = bits per axis). */
 int tlr_morton_order(const double* xy_dev, int n, int order, long long* perm_dev, void* stream);
 
+/* Allocation-free form of tlr_morton_order for callers that may not allocate device memory
+ * during the call (a framework's caching allocator owns the device memory, a service loop that
+ * must not allocate after start-up, ...).  No counterpart in the reference.  Same inputs,
+ * outputs and result as tlr_morton_order; the working memory is a 16 MiB array inside the
+ * library's device image (held by every GPU that loads the library until the process exits),
+ * so n <= 1,048,576 and order <= 10, otherwise TLR_ERR_ARG.  The first call on a device looks
+ * up the array's address (make that first call before any stream capture).  The work is queued
+ * on `stream` and the call returns without waiting.  All calls share the one array: calls
+ * whose work can overlap on the GPU (different streams, or different host threads) race, so
+ * serialise them, for example on one stream. */
+int tlr_morton_order_noalloc(const double* xy_dev, int n, int order, long long* perm_dev, void* stream);
+
 /* Load Morton-ordered sites (device, n x 2 row-major) and observations (device, n) into the
  * plan (copied; the caller keeps ownership).  The reference passes S and y to every call of
  * tlr_loglik (codes/17_tlr_cholesky_pilot.py:259); here they are loaded once. */
