@@ -57,6 +57,9 @@ struct tlr_plan {
   int nslots = 0;
   size_t slot_doubles = 0;
   double* rcs = nullptr;
+  // look-ahead: POTRF(k+1) runs on a second stream while step k's recompression runs
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_panel = nullptr, ev_diag = nullptr;
   // results
   double *ldpart = nullptr, *qpart = nullptr, *out = nullptr;
   int* status = nullptr;
@@ -110,19 +113,20 @@ cudaEvent_t next_event(tlr_plan* p) {
   return p->ev_pool[p->ev_used++];
 }
 
-// launch one kernel of kind `kind`; with profiling on, bracket it by two events
-#define LAUNCH(kind, x)                                                             \
+// launch one kernel of kind `kind` on stream `st`; with profiling on, bracket it by two events
+#define LAUNCH_ON(st, kind, x)                                                      \
   do {                                                                              \
     if (p->prof) {                                                                  \
-      cudaEventRecord(next_event(p), p->stream);                                    \
+      cudaEventRecord(next_event(p), st);                                           \
       p->ev_kind.push_back(kind);                                                   \
     }                                                                               \
     const int _rc = (x);                                                            \
-    if (p->prof) cudaEventRecord(next_event(p), p->stream);                         \
+    if (p->prof) cudaEventRecord(next_event(p), st);                                \
     p->klaunch[kind] += 1;                                                          \
     if (_rc != 0) return fail(TLR_ERR_CUDA, std::string("kernel launch failed: ") + \
                                                 cudaGetErrorString((cudaError_t)_rc)); \
   } while (0)
+#define LAUNCH(kind, x) LAUNCH_ON(p->stream, kind, x)
 
 int run_compression(tlr_plan* p, double sigma2, double inv_range, int rule_fixed, double thr_rel,
                     double thr_abs) {
@@ -156,14 +160,29 @@ int run_compression(tlr_plan* p, double sigma2, double inv_range, int rule_fixed
 
 int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugget, int rule_fixed, double thr_rel,
                       double thr_abs) {
-  cudaStream_t s = p->stream;
+  cudaStream_t s = p->stream, sd = p->side;
+  LAUNCH(TLR_K_DIAG, tlr::launch_diag_build(p->xy, p->n, p->b, 0, sigma2, inv_range, nugget, p->U, p->Wd, p->rank,
+                                            p->cap, p->D, p->status, s));
+  LAUNCH(TLR_K_POTRF, tlr::launch_potrf(p->D, p->n, p->b, 0, p->rhs, p->z, p->ldpart, p->qpart, p->status, s));
   for (int k = 0; k < p->nB; ++k) {
-    LAUNCH(TLR_K_DIAG, tlr::launch_diag_build(p->xy, p->n, p->b, k, sigma2, inv_range, nugget, p->U, p->Wd, p->rank, p->cap, p->D,
-                                p->status, s));
-    LAUNCH(TLR_K_POTRF, tlr::launch_potrf(p->D, p->n, p->b, k, p->rhs, p->z, p->ldpart, p->qpart, p->status, s));
-    LAUNCH(TLR_K_TRSM, tlr::launch_trsm(p->D, p->n, p->b, k, p->nB, p->U, p->V, p->Wd, p->rank, p->cap, p->z, p->rhs, p->status, s));
-    LAUNCH(TLR_K_RECOMPRESS, tlr::launch_recompress(p->n, p->b, k, p->nB, p->U, p->V, p->rank, p->cap, rule_fixed, thr_rel, thr_abs,
-                                p->rcs, p->slot_doubles, p->nslots, p->status, s));
+    LAUNCH(TLR_K_TRSM, tlr::launch_trsm(p->D, p->n, p->b, k, p->nB, p->U, p->V, p->Wd, p->rank, p->cap, p->z, p->rhs,
+                                        p->status, s));
+    const bool ahead = k + 1 < p->nB;
+    if (ahead) {
+      // A_{k+1,k+1} needs only the panels m <= k, all final once the panel solve of step k is
+      // done; step k's recompression touches tiles (i, j) with j > k + 1 only.
+      TRY(cuda_check(cudaEventRecord(p->ev_panel, s), "event"));
+      TRY(cuda_check(cudaStreamWaitEvent(sd, p->ev_panel, 0), "wait"));
+      LAUNCH_ON(sd, TLR_K_DIAG, tlr::launch_diag_build(p->xy, p->n, p->b, k + 1, sigma2, inv_range, nugget, p->U,
+                                                       p->Wd, p->rank, p->cap, p->D, p->status, sd));
+      LAUNCH_ON(sd, TLR_K_POTRF, tlr::launch_potrf(p->D, p->n, p->b, k + 1, p->rhs, p->z, p->ldpart, p->qpart,
+                                                   p->status, sd));
+      TRY(cuda_check(cudaEventRecord(p->ev_diag, sd), "event"));
+    }
+    LAUNCH(TLR_K_RECOMPRESS, tlr::launch_recompress(p->n, p->b, k, p->nB, p->U, p->V, p->rank, p->cap, rule_fixed,
+                                                    thr_rel, thr_abs, p->rcs, p->slot_doubles, p->nslots, p->status,
+                                                    s));
+    if (ahead) TRY(cuda_check(cudaStreamWaitEvent(s, p->ev_diag, 0), "wait"));
   }
   LAUNCH(TLR_K_FINISH, tlr::launch_finish(p->nB, p->n, p->ldpart, p->qpart, p->out, p->status, s));
   return 0;
@@ -227,6 +246,11 @@ int tlr_plan_create(tlr_plan** plan, int n, int b, int cap, int device, void* st
   p->nslots = nsm * 4;
   p->slot_doubles = tlr::rc_slot_doubles(b, cap);
   A(dalloc(p, &p->rcs, (size_t)p->nslots * p->slot_doubles));
+  if (rc == 0) {
+    rc = cuda_check(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking), "side stream");
+    if (!rc) rc = cuda_check(cudaEventCreateWithFlags(&p->ev_panel, cudaEventDisableTiming), "event");
+    if (!rc) rc = cuda_check(cudaEventCreateWithFlags(&p->ev_diag, cudaEventDisableTiming), "event");
+  }
   A(dalloc(p, &p->ldpart, (size_t)p->nB));
   A(dalloc(p, &p->qpart, (size_t)p->nB));
   A(dalloc(p, &p->out, 4));
@@ -266,6 +290,9 @@ void tlr_plan_destroy(tlr_plan* plan) {
   cudaSetDevice(plan->device);
   if (plan->stream) cudaStreamSynchronize(plan->stream);
   for (cudaEvent_t e : plan->ev_pool) cudaEventDestroy(e);
+  if (plan->ev_panel) cudaEventDestroy(plan->ev_panel);
+  if (plan->ev_diag) cudaEventDestroy(plan->ev_diag);
+  if (plan->side) cudaStreamDestroy(plan->side);
   free_all(plan);
   delete plan;
 }

@@ -169,40 +169,56 @@ __device__ inline void cta_org2r(double* A, int lda, int m, int n, const double*
 // Hestenes one-sided Jacobi on the m x n column-major M (ldm): on return M <- M V has
 // mutually orthogonal columns, V (n x n, ldv) holds the right singular vectors, sig[c] the
 // column norms (singular values, unsorted) and perm[0..n) the column order by descending
-// singular value (ties by index).  Round-robin parallel ordering, one warp per pair.
-// `iflag` needs one int of shared memory.  Returns the number of sweeps.
+// singular value (ties by index).  Round-robin parallel ordering, one warp per pair; squared
+// column norms are computed afresh at the start of every sweep and updated by the rotation
+// formulas within it (a_pp' = a_pp - t a_pq, a_qq' = a_qq + t a_pq), so a pair costs one inner
+// product.  `sig` needs n doubles, `iflag` one int of shared memory.  Returns the sweeps used.
 __device__ inline int cta_jacobi_svd(double* M, int ldm, int m, int n, double* V, int ldv, double* sig,
-                              int* perm, int* iflag, int max_sweeps = 40) {
+                                     int* perm, int* iflag, int max_sweeps = 40) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
-    const int i = idx % n, j = idx / n;
-    V[(size_t)j * ldv + i] = (i == j) ? 1.0 : 0.0;
-  }
+  for (int j = warp; j < n; j += nwarp)
+    for (int i = lane; i < n; i += 32) V[(size_t)j * ldv + i] = (i == j) ? 1.0 : 0.0;
   const int np = (n + 1) & ~1;  // even number of players (one dummy when n is odd)
+  // rotate unless the pair is orthogonal to working precision, |cos| <= m eps (the singular
+  // values then carry a relative error of order cos^2)
+  const double tol = (double)(m > 4 ? m : 4) * 2.220446049250313e-16;
+  const double tol2 = tol * tol;
   int sweep = 0;
   if (n > 1) {
     for (sweep = 0; sweep < max_sweeps; ++sweep) {
+      for (int c = warp; c < n; c += nwarp) {
+        const double* mc = M + (size_t)c * ldm;
+        double a = 0.0;
+        for (int t = lane; t < m; t += 32) a += mc[t] * mc[t];
+        a = warp_sum(a);
+        if (lane == 0) sig[c] = a;
+      }
       if (threadIdx.x == 0) *iflag = 0;
       __syncthreads();
       for (int round = 0; round < np - 1; ++round) {
         for (int pr = warp; pr < np / 2; pr += nwarp) {
           // circle method: player 0 fixed, the others rotate
-          int a = (pr == 0) ? 0 : 1 + ((pr - 1 + round) % (np - 1));
-          int b = 1 + ((np - 2 - pr + round) % (np - 1));
+          const int a = (pr == 0) ? 0 : 1 + ((pr - 1 + round) % (np - 1));
+          const int b = 1 + ((np - 2 - pr + round) % (np - 1));
           if (a >= n || b >= n) continue;
-          int p = a < b ? a : b, q = a < b ? b : a;
+          const int p = a < b ? a : b, q = a < b ? b : a;
           double* mp = M + (size_t)p * ldm;
           double* mq = M + (size_t)q * ldm;
-          double app = 0.0, aqq = 0.0, apq = 0.0;
-          for (int t = lane; t < m; t += 32) {
-            const double x = mp[t], y = mq[t];
-            app += x * x; aqq += y * y; apq += x * y;
-          }
-          app = warp_sum(app); aqq = warp_sum(aqq); apq = warp_sum(apq);
-          if (apq != 0.0 && fabs(apq) > 1e-15 * sqrt(app) * sqrt(aqq)) {
-            const double zeta = (aqq - app) / (2.0 * apq);
-            const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-            const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
+          double apq = 0.0;
+          for (int t = lane; t < m; t += 32) apq += mp[t] * mq[t];
+          apq = warp_sum(apq);
+          const double app = sig[p], aqq = sig[q];
+          if (apq != 0.0 && apq * apq > tol2 * app * aqq) {
+            // t = tan of the rotation angle, the smaller root of t^2 + 2 zeta t - 1 = 0 with
+            // zeta = (a_qq - a_pp) / (2 a_pq); for |zeta| > 1e7, t = 1 / (2 zeta) to full precision
+            const double d = aqq - app;
+            double t;
+            if (fabs(d) > 2.0e7 * fabs(apq)) t = apq / d;
+            else {
+              const double zeta = 0.5 * d / apq;
+              t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+            }
+            const double cs = rsqrt(1.0 + t * t), sn = cs * t;
             for (int r = lane; r < m; r += 32) {
               const double x = mp[r], y = mq[r];
               mp[r] = cs * x - sn * y;
@@ -215,7 +231,12 @@ __device__ inline int cta_jacobi_svd(double* M, int ldm, int m, int n, double* V
               vp[r] = cs * x - sn * y;
               vq[r] = sn * x + cs * y;
             }
-            if (lane == 0) *iflag = 1;
+            __syncwarp();
+            if (lane == 0) {
+              sig[p] = app - t * apq;
+              sig[q] = aqq + t * apq;
+              *iflag = 1;
+            }
           }
         }
         __syncthreads();

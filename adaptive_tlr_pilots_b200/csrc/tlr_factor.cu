@@ -92,166 +92,6 @@ __global__ void __launch_bounds__(256) k_diag_build(const double* TLR_RESTRICT x
 }
 
 // ----------------------------------------------------------------------------------------
-// Blocked right-looking Cholesky of the lower triangle of A_kk by one CTA, then the forward
-// solve of the diagonal block.  NB = panel width.
-template <int NB>
-__global__ void __launch_bounds__(512) k_potrf(double* TLR_RESTRICT D, int n, int b, int k,
-                                               double* TLR_RESTRICT rhs, double* TLR_RESTRICT z,
-                                               double* TLR_RESTRICT ldpart, double* TLR_RESTRICT qpart,
-                                               int* TLR_RESTRICT status) {
-  if (*status != 0) return;
-  const int bk = min(b, n - k * b);
-  double* A = D + (size_t)k * b * b;
-  extern __shared__ double smem[];
-  double* L11 = smem;                    // [NB][NB+1]
-  double* Pn = L11 + NB * (NB + 1);      // [bk][NB+1] panel below the diagonal block
-  __shared__ int fail;
-  __shared__ double logdet_acc;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  constexpr int LD = NB + 1;
-  if (tid == 0) {
-    fail = 0;
-    logdet_acc = 0.0;
-    add_work(status, 8, (double)bk * bk * bk / 3.0 + (double)bk * bk, 8.0 * bk * bk);
-  }
-  for (int p0 = 0; p0 < bk; p0 += NB) {
-    const int pw = min(NB, bk - p0);
-    __syncthreads();
-    for (int e = tid; e < NB * NB; e += blockDim.x) {
-      const int i = e % NB, j = e / NB;
-      L11[i * LD + j] = (i < pw && j < pw && i >= j) ? A[(size_t)(p0 + j) * b + p0 + i] : 0.0;
-    }
-    __syncthreads();
-    if (warp == 0) {
-      // unblocked Cholesky of the pw x pw diagonal block, lane = row
-      for (int c = 0; c < pw; ++c) {
-        const double d = L11[c * LD + c];
-        if (!(d > 0.0)) { if (lane == 0) fail = 1; break; }
-        const double sd = sqrt(d);
-        __syncwarp();
-        for (int i = lane; i < pw; i += 32) {
-          if (i > c) L11[i * LD + c] /= sd;
-        }
-        __syncwarp();
-        if (lane == 0) L11[c * LD + c] = sd;
-        for (int i = lane; i < pw; i += 32) {
-          if (i > c) {
-            const double lic = L11[i * LD + c];
-            for (int j = c + 1; j <= i; ++j) L11[i * LD + j] -= lic * L11[j * LD + c];
-          }
-        }
-        __syncwarp();
-      }
-      if (lane == 0 && !fail) {
-        double s = logdet_acc;
-        for (int c = 0; c < pw; ++c) s += log(L11[c * LD + c]);
-        logdet_acc = s;
-      }
-    }
-    __syncthreads();
-    if (fail) {
-      if (tid == 0) atomicCAS(status, 0, k + 1);
-      return;
-    }
-    for (int e = tid; e < pw * pw; e += blockDim.x) {
-      const int i = e % pw, j = e / pw;
-      if (i >= j) A[(size_t)(p0 + j) * b + p0 + i] = L11[i * LD + j];
-    }
-    // panel: rows below, X = A_21 L11^{-T}
-    const int m = bk - p0 - pw;
-    for (int row = tid; row < m; row += blockDim.x) {
-      double x[NB];
-#pragma unroll
-      for (int c = 0; c < NB; ++c) x[c] = (c < pw) ? A[(size_t)(p0 + c) * b + p0 + pw + row] : 0.0;
-#pragma unroll
-      for (int c = 0; c < NB; ++c) {
-        if (c < pw) {
-          double s = x[c];
-#pragma unroll
-          for (int j = 0; j < c; ++j) s -= x[j] * L11[c * LD + j];
-          x[c] = s / L11[c * LD + c];
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < NB; ++c) {
-        Pn[row * LD + c] = (c < pw) ? x[c] : 0.0;
-        if (c < pw) A[(size_t)(p0 + c) * b + p0 + pw + row] = x[c];
-      }
-    }
-    __syncthreads();
-    // trailing update of the lower triangle, 4x4 register tiles
-    const int mt = (m + 3) / 4;
-    const int ntiles = mt * (mt + 1) / 2;
-    for (int tt = tid; tt < ntiles; tt += blockDim.x) {
-      int ti2 = 0, rem = tt;
-      // tile row ti2, tile col tj2 <= ti2, enumerated row by row
-      ti2 = (int)((sqrt(8.0 * rem + 1.0) - 1.0) * 0.5);
-      while (ti2 * (ti2 + 1) / 2 > rem) --ti2;
-      while ((ti2 + 1) * (ti2 + 2) / 2 <= rem) ++ti2;
-      const int tj2 = rem - ti2 * (ti2 + 1) / 2;
-      const int a0 = 4 * ti2, c0 = 4 * tj2;
-      double acc[4][4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
-      for (int t = 0; t < pw; ++t) {
-        double pa[4], pc[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          pa[u] = (a0 + u < m) ? Pn[(a0 + u) * LD + t] : 0.0;
-          pc[u] = (c0 + u < m) ? Pn[(c0 + u) * LD + t] : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-#pragma unroll
-          for (int v = 0; v < 4; ++v) acc[u][v] = fma(pa[u], pc[v], acc[u][v]);
-      }
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        const int cg = c0 + v;
-        if (cg >= m) continue;
-        double* colp = A + (size_t)(p0 + pw + cg) * b + p0 + pw;
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int ag = a0 + u;
-          if (ag < m && ag >= cg) colp[ag] -= acc[u][v];
-        }
-      }
-    }
-  }
-  __syncthreads();
-  // forward solve z_k = L_kk^{-1} rhs_k, blocked by 32 rows
-  double* zk = z + (size_t)k * b;
-  double* rk = rhs + (size_t)k * b;
-  __shared__ double zb[32];
-  __shared__ double red[40];
-  double qacc = 0.0;
-  for (int p0 = 0; p0 < bk; p0 += 32) {
-    const int pw = min(32, bk - p0);
-    if (warp == 0) {
-      double v = (lane < pw) ? rk[p0 + lane] : 0.0;
-      for (int c = 0; c < pw; ++c) {
-        const double xc = __shfl_sync(0xffffffffu, v, c) / A[(size_t)(p0 + c) * b + p0 + c];
-        if (lane == c) v = xc;
-        if (lane > c && lane < pw) v -= A[(size_t)(p0 + c) * b + p0 + lane] * xc;
-      }
-      if (lane < pw) { zb[lane] = v; zk[p0 + lane] = v; }
-    }
-    __syncthreads();
-    for (int row = p0 + pw + tid; row < bk; row += blockDim.x) {
-      double s = rk[row];
-      for (int c = 0; c < pw; ++c) s -= A[(size_t)(p0 + c) * b + row] * zb[c];
-      rk[row] = s;
-    }
-    if (tid < pw) qacc += zb[tid] * zb[tid];
-    __syncthreads();
-  }
-  const double q = block_sum(qacc, red);
-  if (tid == 0) { ldpart[k] = 2.0 * logdet_acc; qpart[k] = q; }
-}
-
-// ----------------------------------------------------------------------------------------
 // Panel solve for column k: one CTA per row tile i > k.
 __global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int n, int b, int k, int nB,
                                              const double* TLR_RESTRICT U, double* TLR_RESTRICT V,
@@ -414,6 +254,8 @@ __device__ void cta_atb(const double* A, int lda, const double* B, int ldb, int 
   (void)scale_a_inv_by_norm;
 }
 
+constexpr int kRcSmemS = 64;  // cores with s <= 64 are solved in shared memory
+
 __global__ void __launch_bounds__(256) k_recompress(int n, int b, int k, int nB, double* TLR_RESTRICT U,
                                                    double* TLR_RESTRICT V, int* TLR_RESTRICT rank, int cap,
                                                    int rule_fixed, double thr_rel, double thr_abs,
@@ -423,14 +265,21 @@ __global__ void __launch_bounds__(256) k_recompress(int n, int b, int k, int nB,
   const int mB = nB - k - 1;  // trailing tiles
   const long npairs = (long)mB * (mB - 1) / 2;
   RcScratch S = rc_slot(scratch + (size_t)blockIdx.x * slot_doubles, b, cap);
+  extern __shared__ double rc_smem[];
+  double* Msm = rc_smem;                            // kRcSmemS^2
+  double* Vsm = rc_smem + kRcSmemS * kRcSmemS;      // kRcSmemS^2
+  double* Zsm = rc_smem + 2 * kRcSmemS * kRcSmemS;  // kRcSmemS^2
   __shared__ double red[40];
   __shared__ double n1[128];
   __shared__ double ninv[128];
+  __shared__ double nvv[128];
+  __shared__ double nvinv[128];
   __shared__ double sig[256];
   __shared__ int perm[256];
   __shared__ int iflag;
   __shared__ int rsel;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ls = 2 * cap;
   if (blockIdx.x == 0 && tid == 0) {  // the panel column k is read once per step
     double by = 0.0;
     for (int i = k + 1; i < nB; ++i) by += 8.0 * 2.0 * b * rank[tidx(i, k)];
@@ -454,135 +303,166 @@ __global__ void __launch_bounds__(256) k_recompress(int n, int b, int k, int nB,
     const double* Ujk = U + (size_t)tjk * b * cap;
     const double* Vjk = V + (size_t)tjk * b * cap;
     const int s = r1 + rj;
+    const bool core_in_smem = s <= kRcSmemS;
+    double* Mc = core_in_smem ? Msm : S.M;
+    double* Vc = core_in_smem ? Vsm : S.Vs;
+    double* Zc = core_in_smem ? Zsm : S.Ru;  // R_u is no longer needed once M is formed
+    const int lc = core_in_smem ? kRcSmemS : ls;
     __syncthreads();
-    // W = V_ik^T V_jk (ri x rj)
+    // W = V_ik^T V_jk (ri x rj); column norms of U_ij
     cta_atb(Vik, b, Vjk, b, bk, ri, rj, S.W, cap, 0.0);
-    // column norms of U_ij
     for (int c = warp; c < r1; c += 8) {
       const double* u = Uij + (size_t)c * b;
-      double a = 0.0;
+      const double* v = Vij + (size_t)c * b;
+      double a = 0.0, av = 0.0;
       for (int t = lane; t < bi; t += 32) a += u[t] * u[t];
+      for (int t = lane; t < bj; t += 32) av += v[t] * v[t];
       a = warp_sum(a);
-      if (lane == 0) { n1[c] = sqrt(a); ninv[c] = a > 0.0 ? 1.0 / sqrt(a) : 0.0; }
+      av = warp_sum(av);
+      if (lane == 0) {
+        n1[c] = sqrt(a);
+        ninv[c] = a > 0.0 ? 1.0 / sqrt(a) : 0.0;
+        nvv[c] = sqrt(av);
+        nvinv[c] = av > 0.0 ? 1.0 / sqrt(av) : 0.0;
+      }
     }
     __syncthreads();
     // X = -U_ik W (bi x rj)
-    for (int e = tid; e < bi * rj; e += 256) {
-      const int a = e % bi, q = e / bi;
-      double acc = 0.0;
-      for (int p = 0; p < ri; ++p) acc = fma(Uik[(size_t)p * b + a], S.W[(size_t)q * cap + p], acc);
-      S.X[(size_t)q * b + a] = -acc;
-    }
+    for (int q = 0; q < rj; ++q)
+      for (int a = tid; a < bi; a += 256) {
+        double acc = 0.0;
+        for (int p = 0; p < ri; ++p) acc = fma(Uik[(size_t)p * b + a], S.W[(size_t)q * cap + p], acc);
+        S.X[(size_t)q * b + a] = -acc;
+      }
     __syncthreads();
     // block Gram-Schmidt twice against Q1 = U_ij diag(1/n1): C = Q1^T X, X -= Q1 C
     for (int pass = 0; pass < 2; ++pass) {
-      for (int e = warp; e < r1 * rj; e += 8) {
-        const int u = e % r1, v = e / r1;
-        const double* a = Uij + (size_t)u * b;
-        const double* x = S.X + (size_t)v * b;
-        double acc = 0.0;
-        for (int t = lane; t < bi; t += 32) acc += a[t] * x[t];
-        acc = warp_sum(acc);
-        if (lane == 0) S.G[(size_t)v * cap + u] = acc * ninv[u];  // temporary C increment
-      }
-      __syncthreads();
-      for (int e = tid; e < bi * rj; e += 256) {
-        const int a = e % bi, v = e / bi;
-        double acc = 0.0;
-        for (int u = 0; u < r1; ++u) acc = fma(Uij[(size_t)u * b + a] * ninv[u], S.G[(size_t)v * cap + u], acc);
-        S.X[(size_t)v * b + a] -= acc;
-      }
-      for (int e = tid; e < r1 * rj; e += 256) {
-        const int u = e % r1, v = e / r1;
-        const double inc = S.G[(size_t)v * cap + u];
-        S.Cc[(size_t)v * cap + u] = pass == 0 ? inc : S.Cc[(size_t)v * cap + u] + inc;
+      if (r1 > 0) {
+        for (int e = warp; e < r1 * rj; e += 8) {
+          const int u = e % r1, v = e / r1;
+          const double* a = Uij + (size_t)u * b;
+          const double* x = S.X + (size_t)v * b;
+          double acc = 0.0;
+          for (int t = lane; t < bi; t += 32) acc += a[t] * x[t];
+          acc = warp_sum(acc);
+          if (lane == 0) S.G[(size_t)v * cap + u] = acc * ninv[u];  // C increment
+        }
+        __syncthreads();
+        for (int v = 0; v < rj; ++v)
+          for (int a = tid; a < bi; a += 256) {
+            double acc = 0.0;
+            for (int u = 0; u < r1; ++u) acc = fma(Uij[(size_t)u * b + a] * ninv[u], S.G[(size_t)v * cap + u], acc);
+            S.X[(size_t)v * b + a] -= acc;
+          }
+        for (int e = tid; e < r1 * rj; e += 256) {
+          const int u = e % r1, v = e / r1;
+          const double inc = S.G[(size_t)v * cap + u];
+          S.Cc[(size_t)v * cap + u] = pass == 0 ? inc : S.Cc[(size_t)v * cap + u] + inc;
+        }
       }
       __syncthreads();
     }
-    // R2 from Householder QR of the projected X (bi x rj); reflectors are not needed
+    // R2 from Householder QR of the projected X (bi x rj); its reflectors are not needed
     cta_geqr2(S.X, b, bi, rj, sig, red);
     // V side: D = V_ij^T U_jk, Y = U_jk - V_ij D (twice)
-    for (int e = tid; e < bj * rj; e += 256) {
-      const int a = e % bj, v = e / bj;
-      S.Y[(size_t)v * b + a] = Ujk[(size_t)v * b + a];
-    }
+    for (int v = 0; v < rj; ++v)
+      for (int a = tid; a < bj; a += 256) S.Y[(size_t)v * b + a] = Ujk[(size_t)v * b + a];
     __syncthreads();
-    for (int pass = 0; pass < 3; ++pass) {
-      // pass 0, 1: D; pass 2: re-orthogonalisation of the explicit Q3 (after the QR below)
-      if (pass == 2) break;
-      cta_atb(Vij, b, S.Y, b, bj, r1, rj, S.G, cap, 0.0);
-      __syncthreads();
-      for (int e = tid; e < bj * rj; e += 256) {
-        const int a = e % bj, v = e / bj;
-        double acc = 0.0;
-        for (int u = 0; u < r1; ++u) acc = fma(Vij[(size_t)u * b + a], S.G[(size_t)v * cap + u], acc);
-        S.Y[(size_t)v * b + a] -= acc;
-      }
-      for (int e = tid; e < r1 * rj; e += 256) {
-        const int u = e % r1, v = e / r1;
-        const double inc = S.G[(size_t)v * cap + u];
-        S.Dd[(size_t)v * cap + u] = pass == 0 ? inc : S.Dd[(size_t)v * cap + u] + inc;
+    for (int pass = 0; pass < 2; ++pass) {
+      if (r1 > 0) {
+        cta_atb(Vij, b, S.Y, b, bj, r1, rj, S.G, cap, 0.0);
+        __syncthreads();
+        for (int e = tid; e < r1 * rj; e += 256) S.G[(size_t)(e / r1) * cap + (e % r1)] *= nvinv[e % r1];
+        __syncthreads();
+        for (int v = 0; v < rj; ++v)
+          for (int a = tid; a < bj; a += 256) {
+            double acc = 0.0;
+            for (int u = 0; u < r1; ++u) acc = fma(Vij[(size_t)u * b + a] * nvinv[u], S.G[(size_t)v * cap + u], acc);
+            S.Y[(size_t)v * b + a] -= acc;
+          }
+        for (int e = tid; e < r1 * rj; e += 256) {
+          const int u = e % r1, v = e / r1;
+          const double inc = S.G[(size_t)v * cap + u];
+          S.Dd[(size_t)v * cap + u] = pass == 0 ? inc : S.Dd[(size_t)v * cap + u] + inc;
+        }
       }
       __syncthreads();
     }
-    // R_u = [[diag(n1), C], [0, R2]] and the R3 part of R_v, both s x s (ld 2cap)
-    const int ls = 2 * cap;
-    for (int e = tid; e < s * s; e += 256) {
-      const int a = e % s, c = e / s;
-      double vu = 0.0;
-      if (a < r1) vu = (c < r1) ? (a == c ? n1[a] : 0.0) : S.Cc[(size_t)(c - r1) * cap + a];
-      else if (c >= r1 && a <= c && a - r1 < bi) vu = S.X[(size_t)(c - r1) * b + (a - r1)];
-      S.Ru[(size_t)c * ls + a] = vu;
-    }
+    // R_u = [[diag(n1), C], [0, R2]] (s x s, ld ls)
+    for (int c = 0; c < s; ++c)
+      for (int a = tid; a < s; a += 256) {
+        double vu = 0.0;
+        if (a < r1) vu = (c < r1) ? (a == c ? n1[a] : 0.0) : S.Cc[(size_t)(c - r1) * cap + a];
+        else if (c >= r1 && a <= c && a - r1 < bi) vu = S.X[(size_t)(c - r1) * b + (a - r1)];
+        S.Ru[(size_t)c * ls + a] = vu;
+      }
     __syncthreads();
     double* tau3 = sig + 128;
     cta_geqr2(S.Y, b, bj, rj, tau3, red);
-    for (int e = tid; e < s * s; e += 256) {
-      const int a = e % s, c = e / s;
-      double vv = 0.0;
-      if (a < r1) vv = (c < r1) ? (a == c ? 1.0 : 0.0) : S.Dd[(size_t)(c - r1) * cap + a];
-      else if (c >= r1 && a <= c && a - r1 < bj) vv = S.Y[(size_t)(c - r1) * b + (a - r1)];
-      S.Rv[(size_t)c * ls + a] = vv;
-    }
+    // R_v = [[I, D], [0, R3]]
+    for (int c = 0; c < s; ++c)
+      for (int a = tid; a < s; a += 256) {
+        double vv = 0.0;
+        if (a < r1) vv = (c < r1) ? (a == c ? nvv[a] : 0.0) : S.Dd[(size_t)(c - r1) * cap + a];
+        else if (c >= r1 && a <= c && a - r1 < bj) vv = S.Y[(size_t)(c - r1) * b + (a - r1)];
+        S.Rv[(size_t)c * ls + a] = vv;
+      }
     __syncthreads();
     cta_org2r(S.Y, b, bj, rj, tau3);
     if (rj > bj) {  // a ragged tile shorter than the rank: the extra basis columns are zero
-      for (int e = tid; e < bj * (rj - bj); e += 256) {
-        const int a = e % bj, v = bj + e / bj;
-        S.Y[(size_t)v * b + a] = 0.0;
-      }
+      for (int v = bj; v < rj; ++v)
+        for (int a = tid; a < bj; a += 256) S.Y[(size_t)v * b + a] = 0.0;
       __syncthreads();
     }
-    // re-orthogonalise Q3 against V_ij once
+    // re-orthogonalise Q3 against the normalised V_ij once
     if (r1 > 0) {
       cta_atb(Vij, b, S.Y, b, bj, r1, rj, S.G, cap, 0.0);
       __syncthreads();
-      for (int e = tid; e < bj * rj; e += 256) {
-        const int a = e % bj, v = e / bj;
-        double acc = 0.0;
-        for (int u = 0; u < r1; ++u) acc = fma(Vij[(size_t)u * b + a], S.G[(size_t)v * cap + u], acc);
-        S.Y[(size_t)v * b + a] -= acc;
-      }
+      for (int v = 0; v < rj; ++v)
+        for (int a = tid; a < bj; a += 256) {
+          double acc = 0.0;
+          for (int u = 0; u < r1; ++u)
+            acc = fma(Vij[(size_t)u * b + a] * nvinv[u], S.G[(size_t)v * cap + u] * nvinv[u], acc);
+          S.Y[(size_t)v * b + a] -= acc;
+        }
       __syncthreads();
     }
-    // core M = R_u R_v^T (s x s)
-    for (int e = tid; e < s * s; e += 256) {
-      const int a = e % s, c = e / s;
-      double acc = 0.0;
-      for (int t = 0; t < s; ++t) acc = fma(S.Ru[(size_t)t * ls + a], S.Rv[(size_t)t * ls + c], acc);
-      S.M[(size_t)c * ls + a] = acc;
+    // core M = R_u R_v^T (s x s); both factors are upper triangular
+    for (int c = 0; c < s; ++c)
+      for (int a = tid; a < s; a += 256) {
+        double acc = 0.0;
+        const int t0 = a > c ? a : c;
+        for (int t = t0; t < s; ++t) acc = fma(S.Ru[(size_t)t * ls + a], S.Rv[(size_t)t * ls + c], acc);
+        Mc[(size_t)c * lc + a] = acc;
+      }
+    __syncthreads();
+    // SVD of the core: Householder QR M = Q_M R_M, then one-sided Jacobi on R_M^T (R_M^T W = Z,
+    // orthogonal columns, sigma = column norms), so M = Q_M W Z^T and the right singular vectors
+    // are the normalised columns of Z.  The QR grades the columns, so the Jacobi needs 3-5 sweeps
+    // instead of 6-16 on M itself.
+    cta_geqr2(Mc, lc, s, s, sig, red);
+    for (int c = 0; c < s; ++c)
+      for (int a = tid; a < s; a += 256) Zc[(size_t)c * lc + a] = (a >= c) ? Mc[(size_t)a * lc + c] : 0.0;
+    __syncthreads();
+    cta_jacobi_svd(Zc, lc, s, s, Vc, lc, sig, perm, &iflag);
+    // Vc <- normalised Z (right singular vectors of M), in place of the rotation matrix
+    for (int c = warp; c < s; c += 8) {
+      const double inv = sig[c] > 0.0 ? 1.0 / sig[c] : 0.0;
+      for (int a = lane; a < s; a += 32) Vc[(size_t)c * lc + a] = Zc[(size_t)c * lc + a] * inv;
     }
     __syncthreads();
-    cta_jacobi_svd(S.M, ls, s, s, S.Vs, ls, sig, perm, &iflag);
     if (tid == 0) {
       double srt[256];
       double fro2 = 0.0;
-      for (int q = 0; q < s; ++q) { srt[q] = sig[perm[q]]; }
+      for (int q = 0; q < s; ++q) srt[q] = sig[perm[q]];
       for (int q = s - 1; q >= 0; --q) fro2 += srt[q] * srt[q];
       const double thr = rule_fixed ? thr_rel * sqrt(fro2) : thr_abs;
       int r = select_rank(srt, s, 0.0, thr, nullptr);
       if (r < 0) r = s;
-      if (r > cap) { atomicCAS(status, 0, -2); r = -1; }
+      if (r > cap) {
+        atomicCAS(status, 0, -2);
+        r = -1;
+      }
       rsel = r;
     }
     __syncthreads();
@@ -592,13 +472,13 @@ __global__ void __launch_bounds__(256) k_recompress(int n, int b, int k, int nB,
       add_work(status, 10, 4.0 * b * ri * rj + 8.0 * b * s * s + 4.0 * b * s * rn,
                8.0 * ((double)(bi + bj) * r1 + (double)(bi + bj) * rn));
     // G = R_v^T Vs_r (s x rn), H = W G_bottom (ri x rn)
-    for (int e = tid; e < s * rn; e += 256) {
-      const int t = e % s, c = e / s;
-      const double* vc = S.Vs + (size_t)perm[c] * ls;
-      double acc = 0.0;
-      for (int a = 0; a < s; ++a) acc = fma(S.Rv[(size_t)t * ls + a], vc[a], acc);
-      S.G[(size_t)c * ls + t] = acc;
-    }
+    for (int c = 0; c < rn; ++c)
+      for (int t = tid; t < s; t += 256) {
+        const double* vc = Vc + (size_t)perm[c] * lc;
+        double acc = 0.0;
+        for (int a = 0; a <= t; ++a) acc = fma(S.Rv[(size_t)t * ls + a], vc[a], acc);
+        S.G[(size_t)c * ls + t] = acc;
+      }
     __syncthreads();
     for (int e = tid; e < ri * rn; e += 256) {
       const int p = e % ri, c = e / ri;
@@ -608,31 +488,29 @@ __global__ void __launch_bounds__(256) k_recompress(int n, int b, int k, int nB,
     }
     __syncthreads();
     // U' = U_ij G_top - U_ik H ; V' = V_ij Vs_top + Q3 Vs_bottom
-    for (int e = tid; e < bi * rn; e += 256) {
-      const int a = e % bi, c = e / bi;
-      double acc = 0.0;
-      for (int t = 0; t < r1; ++t) acc = fma(Uij[(size_t)t * b + a], S.G[(size_t)c * ls + t], acc);
-      for (int p = 0; p < ri; ++p) acc = fma(-Uik[(size_t)p * b + a], S.Hh[(size_t)c * cap + p], acc);
-      S.Uo[(size_t)c * b + a] = acc;
-    }
-    for (int e = tid; e < bj * rn; e += 256) {
-      const int a = e % bj, c = e / bj;
-      const double* vc = S.Vs + (size_t)perm[c] * ls;
-      double acc = 0.0;
-      for (int t = 0; t < r1; ++t) acc = fma(Vij[(size_t)t * b + a], vc[t], acc);
-      for (int t = 0; t < rj; ++t) acc = fma(S.Y[(size_t)t * b + a], vc[r1 + t], acc);
-      S.Vo[(size_t)c * b + a] = acc;
+    for (int c = 0; c < rn; ++c) {
+      const double* gc = S.G + (size_t)c * ls;
+      const double* hc = S.Hh + (size_t)c * cap;
+      const double* vc = Vc + (size_t)perm[c] * lc;
+      for (int a = tid; a < bi; a += 256) {
+        double acc = 0.0;
+        for (int t = 0; t < r1; ++t) acc = fma(Uij[(size_t)t * b + a], gc[t], acc);
+        for (int p = 0; p < ri; ++p) acc = fma(-Uik[(size_t)p * b + a], hc[p], acc);
+        S.Uo[(size_t)c * b + a] = acc;
+      }
+      for (int a = tid; a < bj; a += 256) {
+        double acc = 0.0;
+        for (int t = 0; t < r1; ++t) acc = fma(Vij[(size_t)t * b + a] * nvinv[t], vc[t], acc);
+        for (int t = 0; t < rj; ++t) acc = fma(S.Y[(size_t)t * b + a], vc[r1 + t], acc);
+        S.Vo[(size_t)c * b + a] = acc;
+      }
     }
     __syncthreads();
     double* Uw = U + (size_t)tij * b * cap;
     double* Vw = V + (size_t)tij * b * cap;
-    for (int e = tid; e < bi * rn; e += 256) {
-      const int a = e % bi, c = e / bi;
-      Uw[(size_t)c * b + a] = S.Uo[(size_t)c * b + a];
-    }
-    for (int e = tid; e < bj * rn; e += 256) {
-      const int a = e % bj, c = e / bj;
-      Vw[(size_t)c * b + a] = S.Vo[(size_t)c * b + a];
+    for (int c = 0; c < rn; ++c) {
+      for (int a = tid; a < bi; a += 256) Uw[(size_t)c * b + a] = S.Uo[(size_t)c * b + a];
+      for (int a = tid; a < bj; a += 256) Vw[(size_t)c * b + a] = S.Vo[(size_t)c * b + a];
     }
     if (tid == 0) rank[tij] = rn;
     __syncthreads();
@@ -663,20 +541,6 @@ int launch_diag_build(const double* xy, int n, int b, int k, double sigma2, doub
   return (int)cudaGetLastError();
 }
 
-int launch_potrf(double* D, int n, int b, int k, double* rhs, double* z, double* ldpart, double* qpart,
-                 int* status, cudaStream_t s) {
-  if (b <= 640) {
-    const size_t sm = ((size_t)32 * 33 + (size_t)b * 33) * 8;
-    cudaFuncSetAttribute(k_potrf<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_potrf<32><<<1, 512, sm, s>>>(D, n, b, k, rhs, z, ldpart, qpart, status);
-  } else {
-    const size_t sm = ((size_t)16 * 17 + (size_t)b * 17) * 8;
-    cudaFuncSetAttribute(k_potrf<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_potrf<16><<<1, 512, sm, s>>>(D, n, b, k, rhs, z, ldpart, qpart, status);
-  }
-  return (int)cudaGetLastError();
-}
-
 int launch_trsm(const double* D, int n, int b, int k, int nB, const double* U, double* V, double* Wd,
                 const int* rank, int cap, const double* z, double* rhs, const int* status, cudaStream_t s) {
   if (nB - k - 1 <= 0) return 0;
@@ -691,8 +555,10 @@ int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* ra
   const long npairs = mB * (mB - 1) / 2;
   if (npairs <= 0) return 0;
   const int grid = (int)std::min<long>(npairs, nslots);
-  k_recompress<<<grid, 256, 0, s>>>(n, b, k, nB, U, V, rank, cap, rule_fixed, thr_rel, thr_abs, scratch,
-                                    slot_doubles, status);
+  const size_t sm = (size_t)3 * kRcSmemS * kRcSmemS * 8;
+  cudaFuncSetAttribute(k_recompress, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_recompress<<<grid, 256, sm, s>>>(n, b, k, nB, U, V, rank, cap, rule_fixed, thr_rel, thr_abs, scratch,
+                                     slot_doubles, status);
   return (int)cudaGetLastError();
 }
 
