@@ -18,7 +18,7 @@ TLR_RULE_ADAPTIVE = 1
 _lib = None
 
 KERNEL_KINDS = ["fill", "gen_offdiag", "sketch", "orth", "project", "resid", "finalize", "diag_build", "potrf",
-                "trsm", "recompress", "finish"]
+                "trsm", "recompress", "finish", "bwd_gemm", "tri_inv", "bwd_copy", "alpha", "dtrace", "grad_finish"]
 
 
 class TlrInfo(ctypes.Structure):
@@ -48,6 +48,10 @@ SIGNATURES = {
     "tlr_loglik": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_double,
                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(TlrInfo),
                                   ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "tlr_loglik_grad": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                                       ctypes.c_double, ctypes.POINTER(ctypes.c_double),
+                                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(TlrInfo),
+                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "tlr_loglik_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                        ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_double,
                                        ctypes.POINTER(ctypes.c_double), ctypes.POINTER(TlrInfo),

@@ -8,6 +8,7 @@
 #include "tlr_kernels.h"
 
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -75,6 +76,16 @@ struct tlr_plan {
   long long klaunch[TLR_NKINDS] = {0};
   double kflops[TLR_NKINDS] = {0};
   double kbytes[TLR_NKINDS] = {0};
+  // backward pass: one arena sized from the ranks of the evaluation (grown on demand) and the
+  // job tables of the selected inversion
+  double* bw = nullptr;
+  size_t bw_doubles = 0;
+  tlr::GemmJob* d_jobs = nullptr;
+  size_t d_jobs_cap = 0;
+  double** d_ccol = nullptr;
+  size_t d_ccol_cap = 0;
+  tlr::CopyJob* d_copy = nullptr;
+  size_t d_copy_cap = 0;
 };
 
 namespace {
@@ -96,6 +107,14 @@ int dalloc(tlr_plan* p, T** ptr, size_t count) {
 void free_all(tlr_plan* p) {
   for (void* q : p->allocs) cudaFree(q);
   p->allocs.clear();
+  if (p->bw) cudaFree(p->bw);
+  if (p->d_jobs) cudaFree(p->d_jobs);
+  if (p->d_ccol) cudaFree(p->d_ccol);
+  if (p->d_copy) cudaFree(p->d_copy);
+  p->bw = nullptr;
+  p->d_jobs = nullptr;
+  p->d_ccol = nullptr;
+  p->d_copy = nullptr;
 }
 
 #define TRY(x)                      \
@@ -185,6 +204,230 @@ int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugge
     if (ahead) TRY(cuda_check(cudaStreamWaitEvent(s, p->ev_diag, 0), "wait"));
   }
   LAUNCH(TLR_K_FINISH, tlr::launch_finish(p->nB, p->n, p->ldpart, p->qpart, p->out, p->status, s));
+  return 0;
+}
+
+}  // namespace
+
+
+// ------------------------------------------------------------------------------------------
+// Backward pass (gradient).  See csrc/tlr_backward.cu for the recurrence.
+namespace {
+
+template <class T>
+int grow(T** ptr, size_t* cap, size_t need) {
+  if (need <= *cap && *ptr) return 0;
+  if (*ptr) cudaFree(*ptr);
+  *ptr = nullptr;
+  *cap = 0;
+  const size_t want = std::max<size_t>(need, 1) + need / 4;
+  void* q = nullptr;
+  const cudaError_t e = cudaMalloc(&q, want * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(TLR_ERR_NOMEM, std::string("backward arena: ") + cudaGetErrorString(e));
+  }
+  *ptr = static_cast<T*>(q);
+  *cap = want;
+  return 0;
+}
+
+struct LaunchRange {
+  int kind;      // 0 gemm, 1 copy, 2 alpha, 3 dtrace
+  size_t first;  // index of the first job
+  int count;
+  int max_m, max_n;
+  int m;
+  size_t part_off;
+};
+
+int run_backward(tlr_plan* p, double sigma2, double inv_range, double eta, double* grad_host) {
+  const int nB = p->nB, b = p->b, n = p->n;
+  const size_t B = (size_t)b, BB = B * B;
+  auto bsz = [&](int i) { return std::min(b, n - i * b); };
+  auto r = [&](int i, int m) { return p->h_rank[(size_t)i * (i - 1) / 2 + m]; };
+  // layout from the ranks
+  std::vector<std::vector<int>> offU(nB), offV(nB);
+  std::vector<int> Rlt(nB), Rcol(nB);
+  for (int i = 0; i < nB; ++i) {
+    offU[i].assign(i + 1, 0);
+    for (int m = 0; m < i; ++m) offU[i][m + 1] = offU[i][m] + r(i, m);
+    Rlt[i] = offU[i][i];
+  }
+  for (int m = 0; m < nB; ++m) {
+    offV[m].assign(nB + 1, 0);
+    for (int j = m + 1; j < nB; ++j) offV[m][j + 1] = offV[m][j] + r(j, m);
+    Rcol[m] = offV[m][nB];
+  }
+  size_t o = 0;
+  const size_t oLi = o; o += (size_t)nB * BB;
+  const size_t oZ = o; o += (size_t)nB * BB;
+  std::vector<size_t> oUcat(nB);
+  for (int i = 0; i < nB; ++i) { oUcat[i] = o; o += B * Rlt[i]; }
+  std::vector<std::vector<size_t>> oC(nB);
+  for (int i = 0; i < nB; ++i) {
+    oC[i].assign(i + 1, 0);
+    for (int m = 0; m <= i; ++m) { oC[i][m] = o; o += B * Rcol[m]; }
+  }
+  int Rmax = 1;
+  for (int m = 0; m < nB; ++m) Rmax = std::max(Rmax, Rcol[m]);
+  const size_t oVs = o; o += B * Rmax;
+  const size_t oVp = o; o += B * Rmax;
+  const size_t oAl = o; o += (size_t)nB * B;
+  const size_t oWk = o; o += B;
+  const int nb32 = (b + 31) / 32;
+  std::vector<size_t> part_off(nB);
+  size_t nparts = 0;
+  for (int m = 0; m < nB; ++m) { part_off[m] = nparts; nparts += (size_t)(nB - m) * nb32 * nb32; }
+  const size_t oPart = o; o += 3 * nparts;
+  const size_t oGrad = o; o += 4;
+  TRY(grow(&p->bw, &p->bw_doubles, o));
+  double* base = p->bw;
+  double* Li = base + oLi;
+  double* Zb = base + oZ;
+  double* Vs = base + oVs;
+  double* Vp = base + oVp;
+  auto Cp = [&](int i, int m) { return base + oC[i][m]; };
+  auto Ucat = [&](int i) { return base + oUcat[i]; };
+  auto Ut = [&](int i, int m) { return p->U + ((size_t)i * (i - 1) / 2 + m) * B * p->cap; };
+  auto Vt = [&](int i, int m) { return p->V + ((size_t)i * (i - 1) / 2 + m) * B * p->cap; };
+
+  std::vector<tlr::GemmJob> jobs;
+  std::vector<double*> ccol;
+  std::vector<size_t> ccol_first;  // per job: index into ccol, or SIZE_MAX
+  std::vector<tlr::CopyJob> copies;
+  std::vector<LaunchRange> plan;
+  auto gemm = [&](const double* A, int lda, int tA, const double* Bm, int ldb, int tB, double* C, int ldc, int M,
+                  int N, int K, double alpha, double beta) {
+    tlr::GemmJob j{A, Bm, C, nullptr, lda, ldb, ldc, M, N, K, tA, tB, alpha, beta};
+    jobs.push_back(j);
+    ccol_first.push_back(SIZE_MAX);
+  };
+  auto begin_gemm = [&](int m) { plan.push_back({0, jobs.size(), 0, 0, 0, m, 0}); };
+  auto end_gemm = [&]() {
+    LaunchRange& L = plan.back();
+    L.count = (int)(jobs.size() - L.first);
+    for (size_t q = L.first; q < jobs.size(); ++q) {
+      L.max_m = std::max(L.max_m, jobs[q].M);
+      L.max_n = std::max(L.max_n, jobs[q].N);
+    }
+    if (L.count == 0 || L.max_m == 0 || L.max_n == 0) plan.pop_back();
+  };
+  // gather every row's U factors once: Ucat_i = [U_i0 ... U_i,i-1]
+  plan.push_back({1, copies.size(), 0, 0, 0, -1, 0});
+  for (int i = 0; i < nB; ++i)
+    for (int m = 0; m < i; ++m)
+      if (r(i, m)) copies.push_back({Ut(i, m), Ucat(i) + (size_t)offU[i][m] * B, b, b, bsz(i), r(i, m)});
+  plan.back().count = (int)(copies.size() - plan.back().first);
+  for (int m = nB - 1; m >= 0; --m) {
+    const int bm = bsz(m);
+    // Vstack_m = [V_jm]_{j>m}
+    plan.push_back({1, copies.size(), 0, 0, 0, m, 0});
+    for (int j = m + 1; j < nB; ++j)
+      if (r(j, m)) copies.push_back({Vt(j, m), Vs + (size_t)offV[m][j] * B, b, b, bm, r(j, m)});
+    plan.back().count = (int)(copies.size() - plan.back().first);
+    // Vp_m = Li_m^T Vstack_m ; Z_mm = Li_m^T Li_m
+    begin_gemm(m);
+    if (Rcol[m]) gemm(Li + (size_t)m * BB, b, 1, Vs, b, 0, Vp, b, bm, Rcol[m], bm, 1.0, 0.0);
+    gemm(Li + (size_t)m * BB, b, 1, Li + (size_t)m * BB, b, 0, Zb, b, bm, bm, bm, 1.0, 0.0);
+    end_gemm();
+    // Z_im = -C_im Vp_m^T, i > m
+    begin_gemm(m);
+    for (int i = m + 1; i < nB; ++i)
+      gemm(Cp(i, m), b, 0, Vp, b, 1, Zb + (size_t)(i - m) * BB, b, bsz(i), bm, Rcol[m], -1.0, 0.0);
+    end_gemm();
+    // products of Z_im (i > m) with the U panels, scattered into the C buffers
+    begin_gemm(m);
+    for (int i = m + 1; i < nB; ++i) {
+      const double* Zim = Zb + (size_t)(i - m) * BB;
+      const int Nt = offU[i][m + 1];  // PBT_im = Z_im^T [U_i0 .. U_im]
+      if (Nt) {
+        gemm(Zim, b, 1, Ucat(i), b, 0, nullptr, b, bm, Nt, bsz(i), 1.0, 0.0);
+        ccol_first.back() = ccol.size();
+        for (int mp = 0; mp <= m; ++mp)
+          for (int c = 0; c < r(i, mp); ++c) ccol.push_back(Cp(m, mp) + (size_t)(offV[mp][i] + c) * B);
+      }
+      if (m >= 1 && Rlt[m]) {  // PB_im = Z_im [U_m0 .. U_m,m-1]
+        gemm(Zim, b, 0, Ucat(m), b, 0, nullptr, b, bsz(i), Rlt[m], bm, 1.0, 0.0);
+        ccol_first.back() = ccol.size();
+        for (int mp = 0; mp < m; ++mp)
+          for (int c = 0; c < r(m, mp); ++c) ccol.push_back(Cp(i, mp) + (size_t)(offV[mp][m] + c) * B);
+      }
+    }
+    end_gemm();
+    // Z_mm -= C_mm Vp_m^T
+    begin_gemm(m);
+    if (Rcol[m]) gemm(Cp(m, m), b, 0, Vp, b, 1, Zb, b, bm, bm, Rcol[m], -1.0, 1.0);
+    end_gemm();
+    // PB_mm = Z_mm [U_m0 .. U_m,m-1]
+    begin_gemm(m);
+    if (m >= 1 && Rlt[m]) {
+      gemm(Zb, b, 0, Ucat(m), b, 0, nullptr, b, bm, Rlt[m], bm, 1.0, 0.0);
+      ccol_first.back() = ccol.size();
+      for (int mp = 0; mp < m; ++mp)
+        for (int c = 0; c < r(m, mp); ++c) ccol.push_back(Cp(m, mp) + (size_t)(offV[mp][m] + c) * B);
+    }
+    end_gemm();
+    plan.push_back({2, 0, 1, 0, 0, m, 0});
+    plan.push_back({3, 0, 1, 0, 0, m, part_off[m]});
+  }
+  // upload the tables
+  TRY(grow(&p->d_jobs, &p->d_jobs_cap, jobs.size()));
+  TRY(grow(&p->d_ccol, &p->d_ccol_cap, ccol.size()));
+  TRY(grow(&p->d_copy, &p->d_copy_cap, copies.size()));
+  for (size_t q = 0; q < jobs.size(); ++q)
+    if (ccol_first[q] != SIZE_MAX) jobs[q].ccol = p->d_ccol + ccol_first[q];
+  cudaStream_t s = p->stream;
+  if (!jobs.empty())
+    TRY(cuda_check(cudaMemcpyAsync(p->d_jobs, jobs.data(), jobs.size() * sizeof(tlr::GemmJob), cudaMemcpyHostToDevice, s),
+                   "jobs"));
+  if (!ccol.empty())
+    TRY(cuda_check(cudaMemcpyAsync(p->d_ccol, ccol.data(), ccol.size() * sizeof(double*), cudaMemcpyHostToDevice, s),
+                   "ccol"));
+  if (!copies.empty())
+    TRY(cuda_check(cudaMemcpyAsync(p->d_copy, copies.data(), copies.size() * sizeof(tlr::CopyJob),
+                                   cudaMemcpyHostToDevice, s),
+                   "copies"));
+  // launches
+  LAUNCH(TLR_K_TRI_INV, tlr::launch_tri_inv(p->D, Li, n, b, nB, p->status, s));
+  for (const LaunchRange& L : plan) {
+    if (L.kind == 0) {
+      LAUNCH(TLR_K_BWD_GEMM, tlr::launch_dgemm_batched(p->d_jobs + L.first, L.count, L.max_m, L.max_n, p->status,
+                                                        TLR_K_BWD_GEMM, s));
+    } else if (L.kind == 1) {
+      if (L.count) LAUNCH(TLR_K_BWD_COPY, tlr::launch_copy_cols(p->d_copy + L.first, L.count, p->status, s));
+    } else if (L.kind == 2) {
+      LAUNCH(TLR_K_ALPHA, tlr::launch_alpha_step(n, b, L.m, nB, p->U, p->V, p->rank, p->cap, Li, p->z, base + oAl,
+                                                 base + oWk, p->status, s));
+    } else {
+      LAUNCH(TLR_K_DTRACE, tlr::launch_dtrace_step(p->xy, n, b, L.m, nB, sigma2, inv_range, eta, Zb, base + oAl,
+                                                   base + oPart + 3 * L.part_off, p->status, s));
+    }
+  }
+  LAUNCH(TLR_K_GRAD_FINISH, tlr::launch_grad_finish(base + oPart, (long)nparts, base + oGrad, p->status, s));
+  int status = 0;
+  double g[3];
+  double work[2 * TLR_NKINDS];
+  TRY(cuda_check(cudaMemcpyAsync(g, base + oGrad, sizeof(double) * 3, cudaMemcpyDeviceToHost, s), "grad"));
+  TRY(cuda_check(cudaMemcpyAsync(&status, p->status, sizeof(int), cudaMemcpyDeviceToHost, s), "status"));
+  TRY(cuda_check(cudaMemcpyAsync(work, p->status + 4, sizeof(double) * 2 * TLR_NKINDS, cudaMemcpyDeviceToHost, s),
+                 "work"));
+  TRY(cuda_check(cudaStreamSynchronize(s), "backward"));
+  if (p->prof) {
+    for (size_t q = 0; q < p->ev_kind.size(); ++q) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, p->ev_pool[2 * q], p->ev_pool[2 * q + 1]);
+      p->kms[p->ev_kind[q]] += ms;
+    }
+  }
+  p->ev_used = 0;
+  p->ev_kind.clear();
+  for (int q = TLR_K_BWD_GEMM; q < TLR_NKINDS; ++q) {  // the forward's counts were taken already
+    p->kflops[q] += work[2 * q];
+    p->kbytes[q] += work[2 * q + 1];
+  }
+  if (status != 0) return fail(status < 0 ? status : TLR_ERR_CUDA, "backward pass failed");
+  for (int a = 0; a < 3; ++a) grad_host[a] = g[a];
   return 0;
 }
 
@@ -439,6 +682,19 @@ int tlr_loglik(tlr_plan* p, const double theta[3], int rule, double value, doubl
   fill_info(p, status, out, info, factor_ranks, sigma_ranks);
   if (loglik) *loglik = status == 0 ? out[0] : NAN;
   return status;
+}
+
+int tlr_loglik_grad(tlr_plan* p, const double theta[3], int rule, double value, double* loglik, double* grad,
+                    tlr_info* info, int* factor_ranks, int* sigma_ranks) {
+  double ll = 0.0;
+  const int rc = tlr_loglik(p, theta, rule, value, &ll, info, factor_ranks, sigma_ranks);
+  if (loglik) *loglik = ll;
+  if (rc != 0) return rc;
+  double g[3] = {0.0, 0.0, 0.0};
+  TRY(run_backward(p, theta[0], 1.0 / theta[1], theta[2], g));
+  if (grad)
+    for (int a = 0; a < 3; ++a) grad[a] = g[a];
+  return 0;
 }
 
 int tlr_loglik_host(tlr_plan* p, const double* xy_host, const double* y_host, const double theta[3], int rule,

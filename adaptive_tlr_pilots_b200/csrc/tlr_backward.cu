@@ -1,0 +1,333 @@
+// Backward pass: gradient of the TLR log-likelihood in (sigma2, range, eta).
+//
+// No counterpart in the reference (it has no gradient code; its only derivatives are finite
+// differences, codes/15_pilot_standard_errors.py:21-31).  With Sigma_t = L L^T the TLR factor of
+// the forward pass (ranks frozen), the gradient is
+//     dl/dtheta = 1/2 alpha^T dSigma alpha - 1/2 tr(Z dSigma),  alpha = Sigma_t^{-1} y,  Z = Sigma_t^{-1}
+// with Z's tiles from the selected-inversion (Takahashi) recurrence on the tile factor, i.e. the
+// blocked Cholesky adjoint with the truncations passed through unchanged (oracle:
+// oracle/tlr_oracle.py:tlr_loglik_grad).  Reverse step m, with Vp = L_mm^{-T} [V_jm]_{j>m}:
+//     Z_im = -sum_{j>m} (Z_ij U_jm) Vp_j^T                       (i > m; Z_ij = Z_ji^T for j > i)
+//     Z_mm = L_mm^{-T} L_mm^{-1} - sum_{j>m} (Z_jm^T U_jm) Vp_j^T
+// The products Z_ij U_jm are formed once, when Z_ij is, for every m < j, so each dense Z tile is
+// read from HBM a fixed number of times.  dSigma tiles are regenerated from the sites inside the
+// contraction kernel, never stored.
+//
+// With C_im = [Z_ij U_jm]_{j>m} (b_i x R_m, contiguous) these are single GEMMs of inner dimension
+// R_m = sum_j r_jm; the C blocks are written when Z_ij is formed (column-scattered GEMM output).
+// Kernels: a batched FP64 GEMM with optional column scatter, a batched lower-triangular
+// inverse (L^{-1} of every diagonal tile), the TLR backward solve for alpha, and the fused dSigma
+// generation + contraction.
+#include "tlr_device.cuh"
+#include "tlr_kernels.h"
+
+namespace tlr {
+
+// ----------------------------------------------------------------------------------------
+// Batched FP64 GEMM  C = alpha op(A) op(B) + beta C, 64 x 64 output tiles, 256 threads, 4 x 4 outputs
+// per thread, K in slices of 16 through shared memory.  A job may scatter its output columns:
+// column n then goes to ccol[n] (leading rows contiguous) instead of C + n ldc.
+__global__ void __launch_bounds__(256) k_dgemm_batched(const GemmJob* TLR_RESTRICT jobs,
+                                                      const int* TLR_RESTRICT status, int kind) {
+  if (*status != 0) return;
+  const GemmJob jb = jobs[blockIdx.z];
+  const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+  if (m0 >= jb.M || n0 >= jb.N) return;
+  __shared__ double As[16][65];
+  __shared__ double Bs[16][65];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  for (int k0 = 0; k0 < jb.K; k0 += 16) {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + 256 * q;
+      int kk, mm;
+      if (jb.transA) { kk = e & 15; mm = e >> 4; } else { kk = e >> 6; mm = e & 63; }
+      const int gm = m0 + mm, gk = k0 + kk;
+      double v = 0.0;
+      if (gm < jb.M && gk < jb.K)
+        v = jb.transA ? jb.A[(size_t)gm * jb.lda + gk] : jb.A[(size_t)gk * jb.lda + gm];
+      As[kk][mm] = v;
+      int kb, nn;
+      if (jb.transB) { kb = e >> 6; nn = e & 63; } else { kb = e & 15; nn = e >> 4; }
+      const int gn = n0 + nn, gkb = k0 + kb;
+      double w = 0.0;
+      if (gn < jb.N && gkb < jb.K)
+        w = jb.transB ? jb.B[(size_t)gkb * jb.ldb + gn] : jb.B[(size_t)gn * jb.ldb + gkb];
+      Bs[kb][nn] = w;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      double a[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bv[j], acc[i][j]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int gn = n0 + tx + 16 * j;
+    if (gn >= jb.N) continue;
+    double* cc = jb.ccol ? jb.ccol[gn] : jb.C + (size_t)gn * jb.ldc;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int gm = m0 + ty + 16 * i;
+      if (gm >= jb.M) continue;
+      const double v = jb.alpha * acc[i][j];
+      cc[gm] = (jb.beta == 0.0) ? v : fma(jb.beta, cc[gm], v);
+    }
+  }
+  if (tid == 0) {
+    const int mt = min(64, jb.M - m0), nt = min(64, jb.N - n0);
+    add_work(status, kind, 2.0 * jb.K * mt * nt, 8.0 * ((double)mt * nt + (double)(mt + nt) * jb.K));
+  }
+}
+
+int launch_dgemm_batched(const GemmJob* jobs, int njobs, int max_m, int max_n, const int* status, int kind,
+                         cudaStream_t s) {
+  if (njobs <= 0) return 0;
+  dim3 grid((unsigned)((max_n + 63) / 64), (unsigned)((max_m + 63) / 64), (unsigned)njobs);
+  k_dgemm_batched<<<grid, 256, 0, s>>>(jobs, status, kind);
+  return (int)cudaGetLastError();
+}
+
+// ----------------------------------------------------------------------------------------
+// Li_k = L_kk^{-1} for every diagonal tile: blocked forward substitution on the identity, one
+// CTA per (tile, 32-column block); columns are independent.
+__global__ void __launch_bounds__(256) k_tri_inv(const double* TLR_RESTRICT D, double* TLR_RESTRICT Li, int n,
+                                                int b, const int* TLR_RESTRICT status) {
+  if (*status != 0) return;
+  const int k = blockIdx.y, cb = blockIdx.x;
+  const int bk = min(b, n - k * b);
+  const int c0 = cb * 32;
+  if (c0 >= bk) return;
+  const int cw = min(32, bk - c0);
+  const double* L = D + (size_t)k * b * b;
+  double* X = Li + (size_t)k * b * b;
+  __shared__ double L11[32][33];
+  __shared__ double Xp[32][33];
+  const int tid = threadIdx.x;
+  if (tid == 0 && cb == 0) add_work(status, 13, (double)bk * bk * bk / 3.0, 16.0 * bk * bk);
+  // X[:, c0:c0+cw] = identity columns
+  for (int c = 0; c < cw; ++c)
+    for (int a = tid; a < bk; a += 256) X[(size_t)(c0 + c) * b + a] = (a == c0 + c) ? 1.0 : 0.0;
+  __syncthreads();
+  for (int p0 = (c0 / 32) * 32; p0 < bk; p0 += 32) {
+    const int pw = min(32, bk - p0);
+    for (int e = tid; e < 32 * 32; e += 256) {
+      const int a = e & 31, c = e >> 5;
+      L11[a][c] = (a < pw && c < pw && a >= c) ? L[(size_t)(p0 + c) * b + p0 + a] : 0.0;
+    }
+    __syncthreads();
+    if (tid < cw) {
+      double* xc = X + (size_t)(c0 + tid) * b + p0;
+      double x[32];
+#pragma unroll
+      for (int a = 0; a < 32; ++a) x[a] = (a < pw) ? xc[a] : 0.0;
+#pragma unroll
+      for (int a = 0; a < 32; ++a) {
+        if (a < pw) {
+          double s = x[a];
+#pragma unroll
+          for (int c = 0; c < a; ++c) s -= L11[a][c] * x[c];
+          x[a] = s / L11[a][a];
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < 32; ++a)
+        if (a < pw) { xc[a] = x[a]; Xp[a][tid] = x[a]; }
+    }
+    __syncthreads();
+    for (int row = p0 + pw + tid; row < bk; row += 256) {
+      double l[32];
+#pragma unroll
+      for (int c = 0; c < 32; ++c) l[c] = (c < pw) ? L[(size_t)(p0 + c) * b + row] : 0.0;
+      for (int q = 0; q < cw; ++q) {
+        double s = 0.0;
+#pragma unroll
+        for (int c = 0; c < 32; ++c) s = fma(l[c], Xp[c][q], s);
+        X[(size_t)(c0 + q) * b + row] -= s;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+int launch_tri_inv(const double* D, double* Li, int n, int b, int nB, const int* status, cudaStream_t s) {
+  dim3 grid((unsigned)((b + 31) / 32), (unsigned)nB);
+  k_tri_inv<<<grid, 256, 0, s>>>(D, Li, n, b, status);
+  return (int)cudaGetLastError();
+}
+
+// ----------------------------------------------------------------------------------------
+// Column-block copies (gathers of U / V factors into contiguous panels).
+__global__ void k_copy_cols(const CopyJob* TLR_RESTRICT jobs, const int* TLR_RESTRICT status) {
+  if (*status != 0) return;
+  const CopyJob jb = jobs[blockIdx.y];
+  const size_t total = (size_t)jb.rows * jb.cols;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(e % jb.rows), c = (int)(e / jb.rows);
+    jb.dst[(size_t)c * jb.ldd + r] = jb.src[(size_t)c * jb.lds + r];
+  }
+}
+
+int launch_copy_cols(const CopyJob* jobs, int njobs, const int* status, cudaStream_t s) {
+  if (njobs <= 0) return 0;
+  dim3 grid(32u, (unsigned)njobs);
+  k_copy_cols<<<grid, 256, 0, s>>>(jobs, status);
+  return (int)cudaGetLastError();
+}
+
+// ----------------------------------------------------------------------------------------
+// alpha_m = L_mm^{-T} (z_m - sum_{i>m} V_im (U_im^T alpha_i))   (codes/17_tlr_cholesky_pilot.py:243-256
+// restated for one block row).  One CTA.
+__global__ void __launch_bounds__(256) k_alpha_step(int n, int b, int m, int nB, const double* TLR_RESTRICT U,
+                                                   const double* TLR_RESTRICT V, const int* TLR_RESTRICT rank,
+                                                   int cap, const double* TLR_RESTRICT Li,
+                                                   const double* TLR_RESTRICT z, double* TLR_RESTRICT alpha,
+                                                   double* TLR_RESTRICT work, const int* TLR_RESTRICT status) {
+  if (*status != 0) return;
+  const int bm = min(b, n - m * b);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double* rhs = work;  // b
+  __shared__ double tq[1024];
+  for (int a = tid; a < bm; a += 256) rhs[a] = z[(size_t)m * b + a];
+  __syncthreads();
+  for (int i = m + 1; i < nB; ++i) {
+    const int t = i * (i - 1) / 2 + m;
+    const int r = rank[t];
+    if (r == 0) continue;
+    const int bi = min(b, n - i * b);
+    const double* Ut = U + (size_t)t * b * cap;
+    const double* Vt = V + (size_t)t * b * cap;
+    const double* ai = alpha + (size_t)i * b;
+    for (int q = warp; q < r; q += 8) {
+      double s = 0.0;
+      for (int a = lane; a < bi; a += 32) s = fma(Ut[(size_t)q * b + a], ai[a], s);
+      s = warp_sum(s);
+      if (lane == 0) tq[q] = s;
+    }
+    __syncthreads();
+    for (int a = tid; a < bm; a += 256) {
+      double s = 0.0;
+      for (int q = 0; q < r; ++q) s = fma(Vt[(size_t)q * b + a], tq[q], s);
+      rhs[a] -= s;
+    }
+    __syncthreads();
+  }
+  const double* L = Li + (size_t)m * b * b;
+  for (int a = tid; a < bm; a += 256) {
+    // (L^{-T} rhs)_a = sum_{c >= a} Li[c][a] rhs[c]
+    double s = 0.0;
+    const double* col = L + (size_t)a * b;
+    for (int c = a; c < bm; ++c) s = fma(col[c], rhs[c], s);
+    alpha[(size_t)m * b + a] = s;
+  }
+}
+
+int launch_alpha_step(int n, int b, int m, int nB, const double* U, const double* V, const int* rank, int cap,
+                      const double* Li, const double* z, double* alpha, double* work, const int* status,
+                      cudaStream_t s) {
+  k_alpha_step<<<1, 256, 0, s>>>(n, b, m, nB, U, V, rank, cap, Li, z, alpha, work, status);
+  return (int)cudaGetLastError();
+}
+
+// ----------------------------------------------------------------------------------------
+// Contraction of dSigma (regenerated) with Sbar = 1/2 (alpha_i alpha_m^T - Z_im) over the tiles
+// (i, m), i >= m, of block column m; weight 2 for off-diagonal tiles.  One CTA per 32 x 32 block;
+// partial sums [3] per CTA into part (fixed slots: deterministic final reduction).
+__global__ void __launch_bounds__(256) k_dtrace_step(const double* TLR_RESTRICT xy, int n, int b, int m, int nB,
+                                                    double sigma2, double inv_range, double eta,
+                                                    const double* TLR_RESTRICT Zbuf,
+                                                    const double* TLR_RESTRICT alpha, double* TLR_RESTRICT part,
+                                                    const int* TLR_RESTRICT status) {
+  if (*status != 0) return;
+  const int nb32 = (b + 31) / 32;
+  const int per_tile = nb32 * nb32;
+  const int i = m + blockIdx.x / per_tile;
+  const int blk = blockIdx.x % per_tile;
+  const int rb = blk / nb32, cb = blk % nb32;
+  double* out = part + (size_t)blockIdx.x * 3;
+  const int bi = min(b, n - i * b), bm = min(b, n - m * b);
+  const int r0 = rb * 32, c0 = cb * 32;
+  const int tid = threadIdx.x;
+  double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+  if (r0 < bi && c0 < bm) {
+    const double* Z = Zbuf + (size_t)(i - m) * b * b;  // Z_im, column-major, ld b
+    const double2* p2 = reinterpret_cast<const double2*>(xy);
+    const double* ai = alpha + (size_t)i * b;
+    const double* am = alpha + (size_t)m * b;
+    const int cl = tid & 31, rl = tid >> 5;
+    const int c = c0 + cl;
+    if (c < bm) {
+      const double2 pc = p2[(size_t)m * b + c];
+      const double amc = am[c];
+      for (int q = 0; q < 4; ++q) {
+        const int a = r0 + rl + 8 * q;
+        if (a >= bi) continue;
+        const double2 pa = p2[(size_t)i * b + a];
+        const double dx = pa.x - pc.x, dy = pa.y - pc.y;
+        const double x = kSqrt3 * sqrt(fmax(dx * dx + dy * dy, 0.0)) * inv_range;
+        const double e = exp(-x);
+        const double sbar = 0.5 * (ai[a] * amc - Z[(size_t)c * b + a]);
+        double ds = (1.0 + x) * e;
+        const double dr = sigma2 * x * x * e * inv_range;
+        double de = 0.0;
+        if (i == m && a == c) {
+          ds += eta;
+          de = sigma2;
+        }
+        g0 = fma(ds, sbar, g0);
+        g1 = fma(dr, sbar, g1);
+        g2 = fma(de, sbar, g2);
+      }
+    }
+  }
+  __shared__ double red[40];
+  const double w = (i == m) ? 1.0 : 2.0;
+  g0 = block_sum(g0, red);
+  g1 = block_sum(g1, red);
+  g2 = block_sum(g2, red);
+  if (tid == 0) {
+    out[0] = w * g0;
+    out[1] = w * g1;
+    out[2] = w * g2;
+  }
+}
+
+int launch_dtrace_step(const double* xy, int n, int b, int m, int nB, double sigma2, double inv_range, double eta,
+                       const double* Zbuf, const double* alpha, double* part, const int* status, cudaStream_t s) {
+  const int nb32 = (b + 31) / 32;
+  const int ntile = nB - m;
+  k_dtrace_step<<<ntile * nb32 * nb32, 256, 0, s>>>(xy, n, b, m, nB, sigma2, inv_range, eta, Zbuf, alpha, part,
+                                                    status);
+  return (int)cudaGetLastError();
+}
+
+// final deterministic reduction of the gradient partials
+__global__ void k_grad_finish(const double* part, long nparts, double* grad, const int* status) {
+  if (threadIdx.x != 0) return;
+  if (*status != 0) { grad[0] = grad[1] = grad[2] = 0.0; return; }
+  double g[3] = {0.0, 0.0, 0.0};
+  for (long q = 0; q < nparts; ++q)
+    for (int a = 0; a < 3; ++a) g[a] += part[3 * q + a];
+  for (int a = 0; a < 3; ++a) grad[a] = g[a];
+}
+
+int launch_grad_finish(const double* part, long nparts, double* grad, const int* status, cudaStream_t s) {
+  k_grad_finish<<<1, 32, 0, s>>>(part, nparts, grad, status);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace tlr

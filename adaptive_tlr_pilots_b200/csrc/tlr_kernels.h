@@ -44,6 +44,31 @@ int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* ra
 int launch_finish(int nB, int n, const double* ldpart, const double* qpart, double* out, const int* status,
                   cudaStream_t s);
 
+// backward pass
+struct GemmJob {
+  const double* A;
+  const double* B;
+  double* C;
+  double* const* ccol;  // optional per-column destinations of C (then C / ldc are unused)
+  int lda, ldb, ldc, M, N, K, transA, transB;
+  double alpha, beta;
+};
+struct CopyJob {
+  const double* src;
+  double* dst;
+  int lds, ldd, rows, cols;
+};
+int launch_dgemm_batched(const GemmJob* jobs, int njobs, int max_m, int max_n, const int* status, int kind,
+                         cudaStream_t s);
+int launch_tri_inv(const double* D, double* Li, int n, int b, int nB, const int* status, cudaStream_t s);
+int launch_copy_cols(const CopyJob* jobs, int njobs, const int* status, cudaStream_t s);
+int launch_alpha_step(int n, int b, int m, int nB, const double* U, const double* V, const int* rank, int cap,
+                      const double* Li, const double* z, double* alpha, double* work, const int* status,
+                      cudaStream_t s);
+int launch_dtrace_step(const double* xy, int n, int b, int m, int nB, double sigma2, double inv_range, double eta,
+                       const double* Zbuf, const double* alpha, double* part, const int* status, cudaStream_t s);
+int launch_grad_finish(const double* part, long nparts, double* grad, const int* status, cudaStream_t s);
+
 // error reporting shared by the library's translation units (message for tlr_last_error)
 int set_error(int code, const char* msg);
 

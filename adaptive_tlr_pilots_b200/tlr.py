@@ -75,6 +75,7 @@ class Evaluation:
     info: dict
     factor_ranks: np.ndarray    # reference L_off order (for k, for i > k)
     sigma_ranks: np.ndarray     # initial ranks (for i, for j < i)
+    grad: np.ndarray | None = None  # d loglik / d(sigma2, range, eta), when requested
 
 
 class Plan:
@@ -117,7 +118,8 @@ class Plan:
         _lib.check(self.lib.tlr_set_data(self.handle, ctypes.c_void_p(S_t.data_ptr()),
                                          ctypes.c_void_p(y_t.data_ptr())))
 
-    def evaluate(self, theta, rule, value, host_S=None, host_y=None) -> Evaluation:
+    def evaluate(self, theta, rule, value, host_S=None, host_y=None, grad=False) -> Evaluation:
+        """One log-likelihood evaluation (and its gradient when grad=True) on the device."""
         if rule not in RULES:
             raise ValueError(f"rule must be one of {sorted(RULES)}, got {rule!r}")
         th = (ctypes.c_double * 3)(*[float(v) for v in theta])
@@ -126,7 +128,13 @@ class Plan:
         fr = np.zeros(max(self.ntiles, 1), dtype=np.int32)
         sr = np.zeros(max(self.ntiles, 1), dtype=np.int32)
         ip = ctypes.POINTER(ctypes.c_int)
-        if host_S is not None:
+        g = (ctypes.c_double * 3)()
+        if grad:
+            if host_S is not None:
+                self.set_data(host_S, host_y)
+            rc = self.lib.tlr_loglik_grad(self.handle, th, RULES[rule], float(value), ctypes.byref(ll), g,
+                                          ctypes.byref(info), fr.ctypes.data_as(ip), sr.ctypes.data_as(ip))
+        elif host_S is not None:
             S = np.ascontiguousarray(host_S, dtype=np.float64)
             y = np.ascontiguousarray(host_y, dtype=np.float64)
             if S.shape != (self.n, 2) or y.shape != (self.n,):
@@ -147,7 +155,8 @@ class Plan:
                      max_rank_factor=int(info.max_rank_factor), logdet=float(info.logdet), quad=float(info.quad))
         else:
             d.update(failed_at=int(info.failed_at))
-        return Evaluation(rc, float(ll.value) if rc == 0 else None, d, fr[: self.ntiles], sr[: self.ntiles])
+        return Evaluation(rc, float(ll.value) if rc == 0 else None, d, fr[: self.ntiles], sr[: self.ntiles],
+                          np.array(list(g)) if (grad and rc == 0) else None)
 
     def set_profiling(self, on=True):
         """Bracket every launch with CUDA events (per-kernel device time; results unchanged)."""
@@ -226,6 +235,55 @@ def release_plans():
     for p in _PLANS.values():
         p.close()
     _PLANS.clear()
+
+
+class TLRLogLik:
+    """torch.autograd.Function over the plan: loglik(theta) with d loglik / d theta from the
+    hand-written backward kernels (ranks frozen at theta).  The backward kernels run inside the
+    forward call, while the factor is on the device; backward() only scales the stored gradient."""
+
+    _fn = None
+
+    @classmethod
+    def function(cls):
+        if cls._fn is None:
+            import torch
+
+            class _Fn(torch.autograd.Function):
+                @staticmethod
+                def forward(ctx, theta, plan, rule, value):
+                    ev = plan.evaluate(theta.detach().cpu().tolist(), rule, value, grad=True)
+                    if ev.status != 0:
+                        out = torch.tensor(float("-inf"), dtype=torch.float64)
+                        ctx.save_for_backward(torch.zeros(3, dtype=torch.float64))
+                        return out
+                    ctx.save_for_backward(torch.tensor(ev.grad, dtype=torch.float64))
+                    return torch.tensor(ev.loglik, dtype=torch.float64)
+
+                @staticmethod
+                def backward(ctx, g):
+                    (grad,) = ctx.saved_tensors
+                    return g * grad, None, None, None
+
+            cls._fn = _Fn
+        return cls._fn
+
+    @classmethod
+    def apply(cls, theta, plan, rule, value):
+        return cls.function().apply(theta, plan, rule, value)
+
+
+def tlr_loglik_grad(S, y, theta, bounds, rule, value, cap=64, device=0):
+    """(loglik | None, gradient | None, info): the log-likelihood of tlr_loglik and its gradient
+    in (sigma2, range, eta) from the device backward pass."""
+    S = np.asarray(S, dtype=np.float64)
+    n = S.shape[0]
+    b = _tile_size(bounds, n)
+    plan = get_plan(n, b, cap, device)
+    ev = plan.evaluate(theta, rule, value, host_S=S, host_y=np.asarray(y, dtype=np.float64), grad=True)
+    if ev.status != 0:
+        return None, None, ev.info
+    return ev.loglik, ev.grad, ev.info
 
 
 def tlr_loglik(S, y, theta, bounds, rule, value, cap=64, device=0):

@@ -90,6 +90,16 @@ int tlr_set_data(tlr_plan* plan, const double* xy_dev, const double* y_dev);
 int tlr_loglik(tlr_plan* plan, const double theta[3], int rule, double value, double* loglik, tlr_info* info,
                int* factor_ranks, int* sigma_ranks);
 
+/* Log-likelihood and its gradient in theta = (sigma2, range, eta), ranks frozen at theta.
+ * No counterpart in the reference (it has no gradient code; its only derivatives are central
+ * finite differences, codes/15_pilot_standard_errors.py:21-31).  grad = 1/2 alpha^T dSigma alpha
+ * - 1/2 tr(Sigma_t^{-1} dSigma) with Sigma_t = L L^T the TLR factor, alpha = Sigma_t^{-1} y, the
+ * inverse tiles from a selected inversion on the factor (the blocked Cholesky adjoint with the
+ * truncations passed through) and dSigma regenerated from the sites.  Same return convention as
+ * tlr_loglik; grad (host, 3 doubles) is written only on success. */
+int tlr_loglik_grad(tlr_plan* plan, const double theta[3], int rule, double value, double* loglik, double* grad,
+                    tlr_info* info, int* factor_ranks, int* sigma_ranks);
+
 /* The same evaluation with HOST sites and observations (Morton-ordered), copied to the device
  * inside the call: the end-to-end form of tlr_loglik for callers that hold numpy arrays. */
 int tlr_loglik_host(tlr_plan* plan, const double* xy_host, const double* y_host, const double theta[3], int rule,
@@ -114,7 +124,13 @@ int tlr_get_offdiag_tile(tlr_plan* plan, int i, int j, double* u_host, double* v
 #define TLR_K_TRSM 9       /* panel solve */
 #define TLR_K_RECOMPRESS 10 /* Schur update + recompression */
 #define TLR_K_FINISH 11
-#define TLR_NKINDS 12
+#define TLR_K_BWD_GEMM 12   /* backward: batched GEMMs of the selected inversion */
+#define TLR_K_TRI_INV 13    /* backward: inverses of the diagonal factor tiles */
+#define TLR_K_BWD_COPY 14   /* backward: panel gathers */
+#define TLR_K_ALPHA 15      /* backward: TLR solve alpha = Sigma^{-1} y */
+#define TLR_K_DTRACE 16     /* backward: dSigma generation + contraction */
+#define TLR_K_GRAD_FINISH 17
+#define TLR_NKINDS 18
 
 /* Profiling: when on, every launch is bracketed by CUDA events on the plan's stream and the
  * per-kind device time is accumulated (no effect on results).  No reference counterpart. */
