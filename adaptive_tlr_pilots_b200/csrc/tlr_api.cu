@@ -274,7 +274,7 @@ int run_backward(tlr_plan* p, double sigma2, double inv_range, double eta, doubl
   const size_t oVs = o; o += B * Rmax;
   const size_t oVp = o; o += B * Rmax;
   const size_t oAl = o; o += (size_t)nB * B;
-  const size_t oWk = o; o += B;
+  const size_t oWk = o; o += B + (size_t)std::max(Rmax, 1);
   const int nb32 = (b + 31) / 32;
   std::vector<size_t> part_off(nB);
   size_t nparts = 0;
@@ -442,6 +442,7 @@ int tlr_plan_create(tlr_plan** plan, int n, int b, int cap, int device, void* st
   *plan = nullptr;
   if (n < 1 || b < 1) return fail(TLR_ERR_ARG, "n and b must be positive");
   if (b > 1024) return fail(TLR_ERR_ARG, "tile size b must be <= 1024");
+  if ((n + b - 1) / b > 1024) return fail(TLR_ERR_ARG, "at most 1024 tiles per side (N / b <= 1024)");
   if (cap < 1 || cap > 128) return fail(TLR_ERR_ARG, "rank capacity must be in [1, 128]");
   TRY(cuda_check(cudaSetDevice(device), "cudaSetDevice"));
   tlr_plan* p = new tlr_plan();

@@ -200,39 +200,55 @@ __global__ void __launch_bounds__(256) k_alpha_step(int n, int b, int m, int nB,
   if (*status != 0) return;
   const int bm = min(b, n - m * b);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  double* rhs = work;  // b
-  __shared__ double tq[1024];
-  for (int a = tid; a < bm; a += 256) rhs[a] = z[(size_t)m * b + a];
-  __syncthreads();
-  for (int i = m + 1; i < nB; ++i) {
-    const int t = i * (i - 1) / 2 + m;
-    const int r = rank[t];
-    if (r == 0) continue;
-    const int bi = min(b, n - i * b);
-    const double* Ut = U + (size_t)t * b * cap;
-    const double* Vt = V + (size_t)t * b * cap;
-    const double* ai = alpha + (size_t)i * b;
-    for (int q = warp; q < r; q += 8) {
-      double s = 0.0;
-      for (int a = lane; a < bi; a += 32) s = fma(Ut[(size_t)q * b + a], ai[a], s);
-      s = warp_sum(s);
-      if (lane == 0) tq[q] = s;
+  double* rhs = work;      // b
+  double* tq = work + b;   // sum_{i>m} r_im
+  __shared__ int off[1025];
+  if (tid == 0) {
+    int o = 0;
+    for (int i = m + 1; i < nB; ++i) {
+      off[i - m - 1] = o;
+      o += rank[i * (i - 1) / 2 + m];
     }
-    __syncthreads();
-    for (int a = tid; a < bm; a += 256) {
-      double s = 0.0;
-      for (int q = 0; q < r; ++q) s = fma(Vt[(size_t)q * b + a], tq[q], s);
-      rhs[a] -= s;
-    }
-    __syncthreads();
+    off[nB - m - 1] = o;
   }
-  const double* L = Li + (size_t)m * b * b;
-  for (int a = tid; a < bm; a += 256) {
-    // (L^{-T} rhs)_a = sum_{c >= a} Li[c][a] rhs[c]
+  __syncthreads();
+  const int R = off[nB - m - 1];
+  // t = [U_im^T alpha_i]_{i>m}: one warp per entry, lanes over rows (coalesced)
+  for (int e = warp; e < R; e += 8) {
+    int lo = 0, hi = nB - m - 1;  // find i with off[i-m-1] <= e < off[i-m]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (off[mid] <= e) lo = mid; else hi = mid;
+    }
+    const int i = m + 1 + lo, q = e - off[lo];
+    const int bi = min(b, n - i * b);
+    const double* u = U + ((size_t)i * (i - 1) / 2 + m) * b * cap + (size_t)q * b;
+    const double* ai = alpha + (size_t)i * b;
     double s = 0.0;
+    for (int a = lane; a < bi; a += 32) s = fma(u[a], ai[a], s);
+    s = warp_sum(s);
+    if (lane == 0) tq[e] = s;
+  }
+  __syncthreads();
+  // rhs = z_m - sum_i V_im t_i
+  for (int a = tid; a < bm; a += 256) {
+    double s = z[(size_t)m * b + a];
+    for (int lo = 0; lo < nB - m - 1; ++lo) {
+      const int i = m + 1 + lo, r = off[lo + 1] - off[lo];
+      const double* v = V + ((size_t)i * (i - 1) / 2 + m) * b * cap;
+      for (int q = 0; q < r; ++q) s = fma(-v[(size_t)q * b + a], tq[off[lo] + q], s);
+    }
+    rhs[a] = s;
+  }
+  __syncthreads();
+  // alpha_m = L_mm^{-T} rhs: (Li^T rhs)_a = sum_c Li[c][a] rhs[c]; one warp per output, lanes over c
+  const double* L = Li + (size_t)m * b * b;
+  for (int a = warp; a < bm; a += 8) {
     const double* col = L + (size_t)a * b;
-    for (int c = a; c < bm; ++c) s = fma(col[c], rhs[c], s);
-    alpha[(size_t)m * b + a] = s;
+    double s = 0.0;
+    for (int c = a + lane; c < bm; c += 32) s = fma(col[c], rhs[c], s);
+    s = warp_sum(s);
+    if (lane == 0) alpha[(size_t)m * b + a] = s;
   }
 }
 
@@ -315,18 +331,26 @@ int launch_dtrace_step(const double* xy, int n, int b, int m, int nB, double sig
   return (int)cudaGetLastError();
 }
 
-// final deterministic reduction of the gradient partials
-__global__ void k_grad_finish(const double* part, long nparts, double* grad, const int* status) {
-  if (threadIdx.x != 0) return;
-  if (*status != 0) { grad[0] = grad[1] = grad[2] = 0.0; return; }
+// final deterministic reduction of the gradient partials: fixed per-thread strides, then a
+// fixed-order block reduction
+__global__ void __launch_bounds__(1024) k_grad_finish(const double* part, long nparts, double* grad,
+                                                     const int* status) {
+  __shared__ double red[40];
+  if (*status != 0) {
+    if (threadIdx.x == 0) grad[0] = grad[1] = grad[2] = 0.0;
+    return;
+  }
   double g[3] = {0.0, 0.0, 0.0};
-  for (long q = 0; q < nparts; ++q)
+  for (long q = threadIdx.x; q < nparts; q += blockDim.x)
     for (int a = 0; a < 3; ++a) g[a] += part[3 * q + a];
-  for (int a = 0; a < 3; ++a) grad[a] = g[a];
+  for (int a = 0; a < 3; ++a) {
+    const double t = block_sum(g[a], red);
+    if (threadIdx.x == 0) grad[a] = t;
+  }
 }
 
 int launch_grad_finish(const double* part, long nparts, double* grad, const int* status, cudaStream_t s) {
-  k_grad_finish<<<1, 32, 0, s>>>(part, nparts, grad, status);
+  k_grad_finish<<<1, 1024, 0, s>>>(part, nparts, grad, status);
   return (int)cudaGetLastError();
 }
 

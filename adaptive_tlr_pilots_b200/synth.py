@@ -55,3 +55,47 @@ def dense_loglik_gpu(S, y, theta, device=0):
     fails); None when not positive definite."""
     from .tlr import dense_loglik
     return dense_loglik(S, y, theta, device=device)
+
+
+def dense_loglik_grad_gpu(S, y, theta, device=0, chunk=4096):
+    """Dense FP64 log-likelihood and its gradient in (sigma2, range, eta) on the GPU
+    (cuSOLVER Cholesky and inverse through torch; dSigma in row blocks): the dense oracle for the
+    gradient at sizes where a CPU Cholesky fails.  Returns (ll, grad) or (None, None)."""
+    import torch
+    dev = torch.device("cuda", device)
+    sigma2, rg, eta = [float(v) for v in theta]
+    with torch.no_grad():
+        St = torch.as_tensor(np.asarray(S, dtype=np.float64), device=dev)
+        yt = torch.as_tensor(np.asarray(y, dtype=np.float64), device=dev)
+        n = St.shape[0]
+        K = torch.cdist(St, St)
+        K.mul_((3.0 ** 0.5) / rg)
+        E = torch.exp(-K)
+        K.add_(1.0).mul_(E).mul_(sigma2)
+        del E
+        K.diagonal().add_(sigma2 * eta)
+        L, info = torch.linalg.cholesky_ex(K)
+        del K
+        if int(info.item()) != 0:
+            return None, None
+        z = torch.linalg.solve_triangular(L, yt[:, None], upper=False)
+        ll = float(-0.5 * ((z * z).sum() + 2.0 * torch.log(torch.diagonal(L)).sum() + n * np.log(2 * np.pi)))
+        alpha = torch.cholesky_solve(yt[:, None], L)[:, 0]
+        Kinv = torch.cholesky_inverse(L)
+        del L
+        g = np.zeros(3)
+        for r0 in range(0, n, chunk):
+            r1 = min(n, r0 + chunk)
+            x = torch.cdist(St[r0:r1], St) * ((3.0 ** 0.5) / rg)
+            e = torch.exp(-x)
+            W = 0.5 * (alpha[r0:r1, None] * alpha[None, :] - Kinv[r0:r1])
+            g[0] += float(((1.0 + x) * e * W).sum())
+            g[1] += float((sigma2 * x * x * e / rg * W).sum())
+            del x, e
+            idx = torch.arange(r0, r1, device=dev)
+            wd = W[idx - r0, idx]
+            g[0] += float(eta * wd.sum())
+            g[2] += float(sigma2 * wd.sum())
+        del Kinv
+        torch.cuda.empty_cache()
+    return ll, g

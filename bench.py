@@ -3,8 +3,8 @@
 
 Workload: N = 50,000 seeded sites (the reference's data protocol, codes/17_tlr_cholesky_pilot.py:
 313-325), Morton-ordered, tiles b = 500, Matern-3/2 at theta = (1, 0.3, 0.05), adaptive rule
-tau = 0.9; one step = one full log-likelihood evaluation (tile generation, compression, TLR
-Cholesky, solve) on the plain FP64 path.
+tau = 0.9; one step = one log-likelihood + gradient evaluation (tile generation, compression, TLR
+Cholesky, solve, selected-inversion backward, dSigma contraction) on the plain FP64 path.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -43,12 +43,12 @@ def parse():
     return ap.parse_args()
 
 
-METRIC = "TLR loglik evals/s at N=50k, b=500, adaptive tau=0.9 (plain FP64 path)"
+METRIC = "TLR loglik+grad evals/s at N=50k vs plain FP64 on B200; |dl| vs FP64 dense"
 
 
 def workload(a):
     return {"workload": f"TLR log-likelihood, N={a.n}, b={a.b}, Matern-3/2 theta=(1,0.3,0.05), adaptive tau={a.tau}",
-            "n": a.n, "b": a.b, "rule": "adaptive", "tau": a.tau, "precision": "fp64 plain",
+            "n": a.n, "b": a.b, "rule": "adaptive", "tau": a.tau, "precision": "fp64 plain", "theta_per_step": 1,
             "l2": "inputs larger than L2 (per-evaluation working set several GB)"}
 
 
@@ -110,12 +110,17 @@ def cpu_baseline(S, y, a):
     t0 = time.perf_counter()
     sp = SampledPipeline(S, y, THETA, a.b, "adaptive", a.tau, n_pairs=48)
     setup = time.perf_counter() - t0
-    est, wall = sp.step(n_compress=12, n_trsm=16, n_recompress=48)
-    return {"value": 1.0 / est, "unit": "evals/s", "cores": blas_threads(), "kind": "port",
+    est, wall = 0.0, 0.0
+    for rep in range(4):
+        e, w = sp.step(n_compress=24, n_trsm=32, n_recompress=96, seed=rep)
+        est += e / 4
+        wall += w
+    return {"value": 1.0 / (7.0 * est), "unit": "evals/s", "cores": blas_threads(), "kind": "port",
             "sample": (f"oracle (NumPy/SciPy restatement of codes/17_tlr_cholesky_pilot.py) per-tile operations at "
-                       f"N={a.n}, b={a.b}: 12 tile compressions, 1 POTRF, 16 panel solves/diag updates, 48 step-0 "
-                       f"recompressions timed ({wall:.1f} s, setup {setup:.1f} s) and scaled by their counts in one "
-                       f"evaluation; estimated {est:.1f} s per evaluation")}
+                       f"N={a.n}, b={a.b}: 4 x (24 tile compressions, 1 POTRF, 32 panel solves/diag updates, 96 "
+                       f"step-0 recompressions) timed ({wall:.1f} s, setup {setup:.1f} s) and scaled by their counts in "
+                       f"one evaluation: {est:.1f} s per log-likelihood; loglik+grad = 7 evaluations (value and "
+                       f"central differences in 3 parameters, the reference's only derivative method)")}
 
 
 def run_reference(a):
@@ -137,12 +142,13 @@ def run_reference(a):
         ests.append(est)
         walls.append(wall)
     est = sum(ests) / len(ests)
-    value = 1.0 / est
+    value = 1.0 / (7.0 * est)
     sample = (f"oracle port of codes/17_tlr_cholesky_pilot.py per-tile operations at N={a.n}, b={a.b}: per step 6 "
               f"compressions, 1 POTRF, 8 panel solves/diag updates, 24 step-0 recompressions, scaled by their counts "
-              f"in one evaluation ({est:.1f} s per evaluation estimated)")
+              f"in one evaluation ({est:.1f} s per log-likelihood estimated); loglik+grad = 7 evaluations (value "
+              f"and central differences in 3 parameters)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": a.gpus,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 * est, "higher_is_better": True,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 7000.0 * est, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded reference protocol)",
             "config": workload(a),
             "cpu_baseline": {"value": value, "unit": "evals/s", "cores": blas_threads(), "kind": "port",
@@ -179,7 +185,7 @@ def main():
     plan = tlr.Plan(a.n, a.b, cap=64, device=local)
     plan.set_data(S, y)
     for _ in range(a.warmup):
-        ev = plan.evaluate(THETA, "adaptive", a.tau)
+        ev = plan.evaluate(THETA, "adaptive", a.tau, grad=True)
     plan.set_profiling(True)
     plan.kernel_stats(reset=True)
     sampler = ClockSampler(local)
@@ -190,7 +196,7 @@ def main():
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(a.steps):
-        ev = plan.evaluate(THETA, "adaptive", a.tau)
+        ev = plan.evaluate(THETA, "adaptive", a.tau, grad=True)
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
@@ -211,7 +217,7 @@ def main():
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(a.steps):
-        ll_e2e, _, info_e2e = tlr.tlr_loglik(S_pin, y_pin, THETA, bounds, "adaptive", a.tau, device=local)
+        ll_e2e, g_e2e, info_e2e = tlr.tlr_loglik_grad(S_pin, y_pin, THETA, bounds, "adaptive", a.tau, device=local)
     e1.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1)
@@ -221,10 +227,10 @@ def main():
     ms_e2e = float(t.item())
     ntiles = plan.ntiles
     h2d = S_pin.nbytes + y_pin.nbytes
-    d2h = 4 + 8 * 3 + 8 * 2 * 12 + 2 * 4 * ntiles
+    d2h = 4 + 8 * 3 + 8 * 3 + 2 * 8 * 2 * 18 + 2 * 4 * ntiles
 
     if rank == 0:
-        dense = synth.dense_loglik_gpu(S, y, THETA, device=local)
+        dense, gdense = synth.dense_loglik_grad_gpu(S, y, THETA, device=local)
         pk, pk_kind = peaks()
         launches = int(sum(v["launches"] for v in stats.values()))
         top = max(stats, key=lambda k: stats[k]["ms"])
@@ -247,6 +253,9 @@ def main():
                 "config": dict(workload(a), parallelism=f"replicas x{world}"),
                 "loglik": ev.loglik, "dense_loglik": dense,
                 "abs_dloglik_vs_dense": None if dense is None else abs(ev.loglik - dense),
+                "grad": ev.grad.tolist(), "dense_grad": None if gdense is None else list(gdense),
+                "grad_rel_err_vs_dense": None if gdense is None else
+                float(np.linalg.norm(ev.grad - gdense) / np.linalg.norm(gdense)),
                 "mean_rank_factor": ev.info["mean_rank_factor"], "max_rank_factor": ev.info["max_rank_factor"],
                 "e2e": {"value": world * a.steps / (ms_e2e / 1e3), "unit": "evals/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
