@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "libtlr_b200.so")
 
 TLR_RULE_FIXED = 0
 TLR_RULE_ADAPTIVE = 1
+PRECISIONS = {"fp64": 0, "mixed": 1}
 
 _lib = None
 
@@ -59,6 +60,7 @@ SIGNATURES = {
     "tlr_get_diag_tile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "tlr_get_offdiag_tile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                             ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    "tlr_plan_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tlr_plan_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tlr_plan_kernel_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double),

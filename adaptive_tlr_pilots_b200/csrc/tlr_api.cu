@@ -67,6 +67,7 @@ struct tlr_plan {
   // host copies
   std::vector<int> h_rank, h_rank0, h_ti, h_tj;
   std::vector<void*> allocs;
+  int precision = TLR_PRECISION_FP64;
   // launch accounting and optional per-kernel event timing
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -233,7 +234,7 @@ int grow(T** ptr, size_t* cap, size_t need) {
 }
 
 struct LaunchRange {
-  int kind;      // 0 gemm, 1 copy, 2 alpha, 3 dtrace
+  int kind;      // 0 gemm, 1 copy, 2 alpha, 3 dtrace, 4 gemm that stays FP64 in mixed mode
   size_t first;  // index of the first job
   int count;
   int max_m, max_n;
@@ -326,11 +327,15 @@ int run_backward(tlr_plan* p, double sigma2, double inv_range, double eta, doubl
     for (int j = m + 1; j < nB; ++j)
       if (r(j, m)) copies.push_back({Vt(j, m), Vs + (size_t)offV[m][j] * B, b, b, bm, r(j, m)});
     plan.back().count = (int)(copies.size() - plan.back().first);
-    // Vp_m = Li_m^T Vstack_m ; Z_mm = Li_m^T Li_m
+    // Vp_m = Li_m^T Vstack_m ; Z_mm = Li_m^T Li_m (the diagonal blocks carry tr(Z), which nearly
+    // cancels against alpha^T alpha: they stay FP64 in the mixed path)
     begin_gemm(m);
     if (Rcol[m]) gemm(Li + (size_t)m * BB, b, 1, Vs, b, 0, Vp, b, bm, Rcol[m], bm, 1.0, 0.0);
+    end_gemm();
+    begin_gemm(m);
     gemm(Li + (size_t)m * BB, b, 1, Li + (size_t)m * BB, b, 0, Zb, b, bm, bm, bm, 1.0, 0.0);
     end_gemm();
+    if (!plan.empty() && plan.back().kind == 0 && plan.back().m == m) plan.back().kind = 4;
     // Z_im = -C_im Vp_m^T, i > m
     begin_gemm(m);
     for (int i = m + 1; i < nB; ++i)
@@ -355,10 +360,11 @@ int run_backward(tlr_plan* p, double sigma2, double inv_range, double eta, doubl
       }
     }
     end_gemm();
-    // Z_mm -= C_mm Vp_m^T
+    // Z_mm -= C_mm Vp_m^T (FP64 in both paths)
     begin_gemm(m);
     if (Rcol[m]) gemm(Cp(m, m), b, 0, Vp, b, 1, Zb, b, bm, bm, Rcol[m], -1.0, 1.0);
     end_gemm();
+    if (Rcol[m] && !plan.empty() && plan.back().kind == 0 && plan.back().m == m) plan.back().kind = 4;
     // PB_mm = Z_mm [U_m0 .. U_m,m-1]
     begin_gemm(m);
     if (m >= 1 && Rlt[m]) {
@@ -391,9 +397,16 @@ int run_backward(tlr_plan* p, double sigma2, double inv_range, double eta, doubl
   // launches
   LAUNCH(TLR_K_TRI_INV, tlr::launch_tri_inv(p->D, Li, n, b, nB, p->status, s));
   for (const LaunchRange& L : plan) {
-    if (L.kind == 0) {
+    if (L.kind == 4) {
       LAUNCH(TLR_K_BWD_GEMM, tlr::launch_dgemm_batched(p->d_jobs + L.first, L.count, L.max_m, L.max_n, p->status,
                                                         TLR_K_BWD_GEMM, s));
+    } else if (L.kind == 0) {
+      if (p->precision == TLR_PRECISION_MIXED)
+        LAUNCH(TLR_K_BWD_GEMM, tlr::launch_gemm_tc3(p->d_jobs + L.first, L.count, L.max_m, L.max_n, p->status,
+                                                     TLR_K_BWD_GEMM, s));
+      else
+        LAUNCH(TLR_K_BWD_GEMM, tlr::launch_dgemm_batched(p->d_jobs + L.first, L.count, L.max_m, L.max_n, p->status,
+                                                          TLR_K_BWD_GEMM, s));
     } else if (L.kind == 1) {
       if (L.count) LAUNCH(TLR_K_BWD_COPY, tlr::launch_copy_cols(p->d_copy + L.first, L.count, p->status, s));
     } else if (L.kind == 2) {
@@ -675,8 +688,9 @@ int tlr_loglik(tlr_plan* p, const double theta[3], int rule, double value, doubl
     p->kbytes[q] += work[2 * q + 1];
   }
   if (status < 0) {
-    const char* why = status == TLR_ERR_RANK_CAP ? "a tile rank exceeded the plan's rank capacity"
+    const char* why = status == TLR_ERR_RANK_CAP   ? "a tile rank exceeded the plan's rank capacity"
                       : status == TLR_ERR_COMPRESS ? "a tile needed more than 120 singular directions"
+                      : status == TLR_ERR_TIMEOUT  ? "a device wait ran out of its iteration limit"
                                                    : "device error";
     return fail(status, why);
   }
@@ -708,6 +722,13 @@ int tlr_loglik_host(tlr_plan* p, const double* xy_host, const double* y_host, co
                  "copy observations"));
   p->has_data = true;
   return tlr_loglik(p, theta, rule, value, loglik, info, factor_ranks, sigma_ranks);
+}
+
+int tlr_plan_set_precision(tlr_plan* p, int mode) {
+  if (!p) return fail(TLR_ERR_ARG, "plan is NULL");
+  if (mode != TLR_PRECISION_FP64 && mode != TLR_PRECISION_MIXED) return fail(TLR_ERR_ARG, "unknown precision mode");
+  p->precision = mode;
+  return 0;
 }
 
 int tlr_plan_set_profiling(tlr_plan* p, int on) {

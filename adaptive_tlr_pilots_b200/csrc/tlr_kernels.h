@@ -60,6 +60,7 @@ struct CopyJob {
 };
 int launch_dgemm_batched(const GemmJob* jobs, int njobs, int max_m, int max_n, const int* status, int kind,
                          cudaStream_t s);
+int launch_gemm_tc3(const GemmJob* jobs, int njobs, int max_m, int max_n, int* status, int kind, cudaStream_t s);
 int launch_tri_inv(const double* D, double* Li, int n, int b, int nB, const int* status, cudaStream_t s);
 int launch_copy_cols(const CopyJob* jobs, int njobs, const int* status, cudaStream_t s);
 int launch_alpha_step(int n, int b, int m, int nB, const double* U, const double* V, const int* rank, int cap,

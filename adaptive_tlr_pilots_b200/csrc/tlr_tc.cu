@@ -1,0 +1,249 @@
+// Tensor-core (tcgen05) GEMM for the mixed-precision path: C = alpha op(A) op(B) + beta C with FP64
+// operands and result, products formed on the 5th-generation tensor cores as split TF32
+// ("3xTF32": x = hi + lo with hi, lo TF32, A B ~ A_hi B_hi + A_hi B_lo + A_lo B_hi) accumulated in
+// FP32 in tensor memory.  Relative accuracy is that of FP32 (about 1e-7 per product), which keeps
+// the selected-inversion gradient within ~1e-5 of the FP64 one (single-pass TF32 loses ~1e-2 on
+// the range component).
+//
+// One CTA of 256 threads computes a 128 x N_TILE output tile (N_TILE = 128): the accumulator is
+// 128 TMEM lanes x 128 columns.  K advances in slices of 32: every thread converts and splits its
+// share of the FP64 slice into shared memory in the canonical K-major, no-swizzle UMMA layout
+// (core matrices of 8 rows x 16 bytes; rows of a core matrix 16 B apart, 8-row groups 128 B
+// apart, the two 16-byte K halves of one MMA 2048 B apart for A), fences the generic-proxy writes
+// for the async proxy, and thread 0 issues 4 K-steps x 3 tcgen05.mma.kind::tf32 and commits them
+// to the stage's mbarrier.  Two stages alternate, so the conversion of slice s+1 overlaps the MMAs
+// of slice s.  Waits on the mbarriers are bounded: on timeout the kernel sets an error status,
+// frees its tensor memory and returns.
+#include <stdint.h>
+
+#include "tlr_device.cuh"
+#include "tlr_kernels.h"
+
+namespace tlr {
+
+constexpr int kTcM = 128;
+constexpr int kTcN = 128;
+constexpr int kTcBK = 32;
+constexpr int kTcStages = 2;
+// bytes per stage: A_hi, A_lo (128 x 32 x 4), B_hi, B_lo (128 x 32 x 4)
+constexpr int kTcStageBytes = 4 * kTcM * kTcBK * 4;
+constexpr long long kTcWaitLimit = 1ll << 26;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+// K-major, no-swizzle shared-memory matrix descriptor (SM100 UMMA): start address, leading
+// byte offset (between the two 16-byte K halves), stride byte offset (between 8-row groups), all
+// in 16-byte units; version 1; layout type 0 (no swizzle).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // version
+  return d;
+}
+
+// instruction descriptor: D f32, A and B tf32, both K-major, M = 128, N = kTcN
+__device__ __forceinline__ uint32_t umma_idesc_tf32(int M, int N) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}\n"
+      : "=r"(ok)
+      : "r"(mbar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait; false on timeout
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (long long it = 0; it < kTcWaitLimit; ++it)
+    if (mbar_try_wait(mbar, parity)) return true;
+  return false;
+}
+
+__global__ void __launch_bounds__(256) k_gemm_tc3(const GemmJob* TLR_RESTRICT jobs, int* TLR_RESTRICT status,
+                                                 int kind) {
+  if (*status != 0) return;
+  const GemmJob jb = jobs[blockIdx.z];
+  const int m0 = blockIdx.y * kTcM, n0 = blockIdx.x * kTcN;
+  if (m0 >= jb.M || n0 >= jb.N) return;
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  __shared__ __align__(8) uint64_t mbar[kTcStages];
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ int timed_out;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                 "r"(kTcN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < kTcStages; ++s)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[s])));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+    timed_out = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem_d = tmem_base_sh;
+  const uint32_t idesc = umma_idesc_tf32(kTcM, kTcN);
+  const int nk = (jb.K + kTcBK - 1) / kTcBK;
+  int fail = 0;
+  for (int it = 0; it < nk; ++it) {
+    const int st = it & 1;
+    unsigned char* sbase = tc_smem + st * kTcStageBytes;
+    float* Ahi = reinterpret_cast<float*>(sbase);
+    float* Alo = Ahi + kTcM * kTcBK;
+    float* Bhi = Alo + kTcM * kTcBK;
+    float* Blo = Bhi + kTcN * kTcBK;
+    if (it >= kTcStages) {
+      // the MMAs that read this stage two slices ago must be done before it is overwritten
+      if (!mbar_wait(smem_u32(&mbar[st]), (uint32_t)(((it - kTcStages) >> 1) & 1))) {
+        fail = 1;
+      }
+    }
+    if (__syncthreads_or(fail)) {
+      fail = 1;
+      break;
+    }
+    const int k0 = it * kTcBK;
+    // thread -> (row r = tid / 2, K groups (tid & 1) * 4 .. + 3 of 4 consecutive k each): all 16
+    // loads of A and of B are issued before any of them is used, then each group of 4 goes to
+    // shared memory as one 16-byte store (hi and lo)
+    {
+      const int r = tid >> 1, gh = (tid & 1) * 4;
+      double va[16], vb[16];
+      const int gma = m0 + r, gnb = n0 + r;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int gk = k0 + gh * 4 + q;
+        va[q] = (gma < jb.M && gk < jb.K)
+                    ? (jb.transA ? jb.A[(size_t)gma * jb.lda + gk] : jb.A[(size_t)gk * jb.lda + gma])
+                    : 0.0;
+        vb[q] = (gnb < jb.N && gk < jb.K)
+                    ? (jb.transB ? jb.B[(size_t)gk * jb.ldb + gnb] : jb.B[(size_t)gnb * jb.ldb + gk])
+                    : 0.0;
+      }
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {
+        float4 ah, al, bh, bl;
+        float* pah = &ah.x; float* pal = &al.x; float* pbh = &bh.x; float* pbl = &bl.x;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const float fa = (float)va[4 * g + c], fb = (float)vb[4 * g + c];
+          const uint32_t ha = to_tf32(fa), hb = to_tf32(fb);
+          pah[c] = __uint_as_float(ha);
+          pal[c] = __uint_as_float(to_tf32(fa - __uint_as_float(ha)));
+          pbh[c] = __uint_as_float(hb);
+          pbl[c] = __uint_as_float(to_tf32(fb - __uint_as_float(hb)));
+        }
+        const int chunk = gh + g;
+        *reinterpret_cast<float4*>(Ahi + chunk * (kTcM * 4) + r * 4) = ah;
+        *reinterpret_cast<float4*>(Alo + chunk * (kTcM * 4) + r * 4) = al;
+        *reinterpret_cast<float4*>(Bhi + chunk * (kTcN * 4) + r * 4) = bh;
+        *reinterpret_cast<float4*>(Blo + chunk * (kTcN * 4) + r * 4) = bl;
+      }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const uint32_t aH = smem_u32(Ahi), aL = smem_u32(Alo), bH = smem_u32(Bhi), bL = smem_u32(Blo);
+      const uint32_t lboA = kTcM * 16, lboB = kTcN * 16, sbo = 128;
+#pragma unroll
+      for (int ks = 0; ks < kTcBK / 8; ++ks) {
+        const uint32_t oa = ks * 2 * kTcM * 16, ob = ks * 2 * kTcN * 16;
+        const uint64_t dAh = umma_desc(aH + oa, lboA, sbo), dAl = umma_desc(aL + oa, lboA, sbo);
+        const uint64_t dBh = umma_desc(bH + ob, lboB, sbo), dBl = umma_desc(bL + ob, lboB, sbo);
+        const uint32_t first = (it == 0 && ks == 0) ? 0u : 1u;
+        mma_tf32(tmem_d, dAh, dBh, idesc, first);
+        mma_tf32(tmem_d, dAh, dBl, idesc, 1u);
+        mma_tf32(tmem_d, dAl, dBh, idesc, 1u);
+      }
+      mma_commit(smem_u32(&mbar[st]));
+    }
+  }
+  // wait for the last commit (it covers every MMA issued before it)
+  if (!fail && nk > 0 && tid == 0) {
+    const int last = nk - 1;
+    if (!mbar_wait(smem_u32(&mbar[last & 1]), (uint32_t)((last >> 1) & 1))) timed_out = 1;
+  }
+  if (fail && tid == 0) timed_out = 1;
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const bool ok = !timed_out;
+  if (ok) {
+    const int quarter = warp & 3, half = warp >> 2;
+    const int row = quarter * 32 + lane;
+    const int gm = m0 + row;
+    for (int c0 = half * (kTcN / 2); c0 < (half + 1) * (kTcN / 2); c0 += 8) {
+      uint32_t r[8];
+      const uint32_t taddr = tmem_d + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0;
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                   : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                   : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (nk == 0)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) r[q] = 0u;
+      if (gm < jb.M) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int gn = n0 + c0 + q;
+          if (gn >= jb.N) break;
+          double* cc = jb.ccol ? jb.ccol[gn] : jb.C + (size_t)gn * jb.ldc;
+          const double v = jb.alpha * (double)__uint_as_float(r[q]);
+          cc[gm] = (jb.beta == 0.0) ? v : fma(jb.beta, cc[gm], v);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(kTcN));
+  if (tid == 0) {
+    if (!ok) atomicCAS(status, 0, -7);
+    else {
+      const int mt = min(kTcM, jb.M - m0), nt = min(kTcN, jb.N - n0);
+      add_work(status, kind, 2.0 * jb.K * mt * nt, 8.0 * ((double)mt * nt + (double)(mt + nt) * jb.K));
+    }
+  }
+}
+
+int launch_gemm_tc3(const GemmJob* jobs, int njobs, int max_m, int max_n, int* status, int kind, cudaStream_t s) {
+  if (njobs <= 0) return 0;
+  const size_t sm = (size_t)kTcStages * kTcStageBytes + 1024;
+  cudaFuncSetAttribute(k_gemm_tc3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  dim3 grid((unsigned)((max_n + kTcN - 1) / kTcN), (unsigned)((max_m + kTcM - 1) / kTcM), (unsigned)njobs);
+  k_gemm_tc3<<<grid, 256, sm, s>>>(jobs, status, kind);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace tlr

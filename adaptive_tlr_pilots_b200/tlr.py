@@ -158,6 +158,13 @@ class Plan:
         return Evaluation(rc, float(ll.value) if rc == 0 else None, d, fr[: self.ntiles], sr[: self.ntiles],
                           np.array(list(g)) if (grad and rc == 0) else None)
 
+    def set_precision(self, mode="fp64"):
+        """'fp64' (the parity path) or 'mixed' (tensor-core 3xTF32 backward GEMMs)."""
+        if mode not in _lib.PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(_lib.PRECISIONS)}")
+        _lib.check(self.lib.tlr_plan_set_precision(self.handle, _lib.PRECISIONS[mode]))
+        self.precision = mode
+
     def set_profiling(self, on=True):
         """Bracket every launch with CUDA events (per-kernel device time; results unchanged)."""
         _lib.check(self.lib.tlr_plan_set_profiling(self.handle, 1 if on else 0))

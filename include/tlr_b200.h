@@ -36,6 +36,7 @@ extern "C" {
 #define TLR_ERR_NOMEM (-4)        /* device allocation failed */
 #define TLR_ERR_COMPRESS (-5)     /* a tile needed more than the largest sketch width */
 #define TLR_ERR_NOT_READY (-6)    /* tlr_set_data has not been called */
+#define TLR_ERR_TIMEOUT (-7)      /* a bounded device wait gave up (the kernel freed its resources) */
 
 typedef struct tlr_plan tlr_plan;
 
@@ -110,6 +111,15 @@ int tlr_loglik_host(tlr_plan* plan, const double* xy_host, const double* y_host,
  * b_j x r, column-major, r = *rank).  Valid after a successful tlr_loglik. */
 int tlr_get_diag_tile(tlr_plan* plan, int k, double* out_host);
 int tlr_get_offdiag_tile(tlr_plan* plan, int i, int j, double* u_host, double* v_host, int* rank);
+
+/* Arithmetic of a plan.  TLR_PRECISION_FP64 (default): every step in FP64, the parity path.
+ * TLR_PRECISION_MIXED: the backward pass's GEMMs on the tensor cores as split TF32 (3xTF32, FP32
+ * accumulation); FP64 kept for the forward factorization, thresholds, POTRF and all
+ * accumulations of log det, quadratic form and gradient.  No reference counterpart (the
+ * reference is FP64 throughout). */
+#define TLR_PRECISION_FP64 0
+#define TLR_PRECISION_MIXED 1
+int tlr_plan_set_precision(tlr_plan* plan, int mode);
 
 /* Kernel kinds counted by tlr_plan_kernel_stats (launches issued by the plan's evaluations). */
 #define TLR_K_FILL 0

@@ -68,3 +68,24 @@ def test_autograd_function(tlr):
     ll.backward()
     _, g_o, _ = O.tlr_loglik_grad(d["S"], d["y"], (1.0, 0.3, 0.05), O.tile_bounds(1030, 100), "adaptive", 0.9)
     np.testing.assert_allclose(theta.grad.numpy(), g_o, rtol=1e-8)
+
+
+@pytest.mark.parametrize("case,b,rule,value", [
+    ("n1030_b100", 100, "adaptive", 0.9),
+    ("n4000_b250", 250, "adaptive", 0.9),
+])
+def test_mixed_gradient_close_to_fp64(tlr, case, b, rule, value):
+    """Tensor-core 3xTF32 backward: gradient within 1e-4 (relative, 2-norm) of the FP64 backward."""
+    d = np.load(os.path.join(GOLD, case + "_data.npz"))
+    n = len(d["y"])
+    p64 = tlr.Plan(n, b)
+    p64.set_data(d["S"], d["y"])
+    e64 = p64.evaluate((1.0, 0.3, 0.05), rule, value, grad=True)
+    pmx = tlr.Plan(n, b)
+    pmx.set_precision("mixed")
+    pmx.set_data(d["S"], d["y"])
+    emx = pmx.evaluate((1.0, 0.3, 0.05), rule, value, grad=True)
+    assert abs(emx.loglik - e64.loglik) <= 1e-2
+    assert np.linalg.norm(emx.grad - e64.grad) <= 1e-4 * np.linalg.norm(e64.grad), (emx.grad, e64.grad)
+    p64.close()
+    pmx.close()
