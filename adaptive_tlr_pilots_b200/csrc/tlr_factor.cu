@@ -254,9 +254,9 @@ __device__ void cta_atb(const double* A, int lda, const double* B, int ldb, int 
   (void)scale_a_inv_by_norm;
 }
 
-constexpr int kRcSmemS = 64;  // cores with s <= 64 are solved in shared memory
+constexpr int kRcSmemS = 32;  // cores with s <= 32 are solved in shared memory
 
-__global__ void __launch_bounds__(256) k_recompress(int n, int b, int k, int nB, double* TLR_RESTRICT U,
+__global__ void __launch_bounds__(256, 4) k_recompress(int n, int b, int k, int nB, double* TLR_RESTRICT U,
                                                    double* TLR_RESTRICT V, int* TLR_RESTRICT rank, int cap,
                                                    int rule_fixed, double thr_rel, double thr_abs,
                                                    double* TLR_RESTRICT scratch, size_t slot_doubles,
