@@ -280,13 +280,15 @@ class TLRLogLik:
         return cls.function().apply(theta, plan, rule, value)
 
 
-def tlr_loglik_grad(S, y, theta, bounds, rule, value, cap=64, device=0):
+def tlr_loglik_grad(S, y, theta, bounds, rule, value, cap=64, device=0, precision="fp64"):
     """(loglik | None, gradient | None, info): the log-likelihood of tlr_loglik and its gradient
-    in (sigma2, range, eta) from the device backward pass."""
+    in (sigma2, range, eta) from the device backward pass.  precision 'fp64' (every step in FP64)
+    or 'mixed' (tensor-core products where the accuracy budget allows)."""
     S = np.asarray(S, dtype=np.float64)
     n = S.shape[0]
     b = _tile_size(bounds, n)
     plan = get_plan(n, b, cap, device)
+    plan.set_precision(precision)
     ev = plan.evaluate(theta, rule, value, host_S=S, host_y=np.asarray(y, dtype=np.float64), grad=True)
     if ev.status != 0:
         return None, None, ev.info

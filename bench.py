@@ -40,6 +40,8 @@ def parse():
     ap.add_argument("--b", type=int, default=500)
     ap.add_argument("--tau", type=float, default=0.9)
     ap.add_argument("--cpu-sample", type=int, default=1, help="0: skip the CPU baseline leg")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--plain-steps", type=int, default=2, help="timed steps of the plain FP64 comparison (0: skip)")
     return ap.parse_args()
 
 
@@ -48,7 +50,7 @@ METRIC = "TLR loglik+grad evals/s at N=50k vs plain FP64 on B200; |dl| vs FP64 d
 
 def workload(a):
     return {"workload": f"TLR log-likelihood, N={a.n}, b={a.b}, Matern-3/2 theta=(1,0.3,0.05), adaptive tau={a.tau}",
-            "n": a.n, "b": a.b, "rule": "adaptive", "tau": a.tau, "precision": "fp64 plain", "theta_per_step": 1,
+            "n": a.n, "b": a.b, "rule": "adaptive", "tau": a.tau, "precision": a.precision, "theta_per_step": 1,
             "l2": "inputs larger than L2 (per-evaluation working set several GB)"}
 
 
@@ -184,13 +186,34 @@ def main():
     S, y, _, _ = synth.simulate_field(a.n, THETA, device=local)
     plan = tlr.Plan(a.n, a.b, cap=64, device=local)
     plan.set_data(S, y)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    # the plain FP64 path (every step in FP64, one theta per evaluation): the comparison leg
+    plain = None
+    if a.plain_steps > 0:
+        plan.set_precision("fp64")
+        ev64 = plan.evaluate(THETA, "adaptive", a.tau, grad=True)
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(a.plain_steps):
+            ev64 = plan.evaluate(THETA, "adaptive", a.tau, grad=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = torch.tensor([e0.elapsed_time(e1)], device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms64 = float(t.item()) / a.plain_steps
+        plain = {"value": world * 1e3 / ms64, "unit": "evals/s", "ms_per_step": ms64, "steps": a.plain_steps,
+                 "loglik": ev64.loglik, "grad": ev64.grad.tolist()}
+
+    plan.set_precision(a.precision)
     for _ in range(a.warmup):
         ev = plan.evaluate(THETA, "adaptive", a.tau, grad=True)
     plan.set_profiling(True)
     plan.kernel_stats(reset=True)
     sampler = ClockSampler(local)
-    stream = torch.cuda.current_stream()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     sampler.start()
     barrier()
     torch.cuda.synchronize()
@@ -217,7 +240,8 @@ def main():
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(a.steps):
-        ll_e2e, g_e2e, info_e2e = tlr.tlr_loglik_grad(S_pin, y_pin, THETA, bounds, "adaptive", a.tau, device=local)
+        ll_e2e, g_e2e, info_e2e = tlr.tlr_loglik_grad(S_pin, y_pin, THETA, bounds, "adaptive", a.tau, device=local,
+                                                       precision=a.precision)
     e1.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1)
@@ -248,7 +272,7 @@ def main():
                 for k, v in stats.items() if v["launches"]}
         line = {"metric": METRIC, "value": world * a.steps / (ms_max / 1e3), "unit": "evals/s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f64+tf32x3",
                 "data": "synthetic (seeded reference protocol, y = L z with the dense FP64 Cholesky)",
                 "config": dict(workload(a), parallelism=f"replicas x{world}"),
                 "loglik": ev.loglik, "dense_loglik": dense,
@@ -257,6 +281,11 @@ def main():
                 "grad_rel_err_vs_dense": None if gdense is None else
                 float(np.linalg.norm(ev.grad - gdense) / np.linalg.norm(gdense)),
                 "mean_rank_factor": ev.info["mean_rank_factor"], "max_rank_factor": ev.info["max_rank_factor"],
+                "plain_fp64": plain,
+                "speedup_vs_plain_fp64": None if plain is None else (world * a.steps / (ms_max / 1e3)) / plain["value"],
+                "abs_dloglik_vs_plain_fp64": None if plain is None else abs(ev.loglik - plain["loglik"]),
+                "grad_rel_err_vs_plain_fp64": None if plain is None else
+                float(np.linalg.norm(ev.grad - np.array(plain["grad"])) / np.linalg.norm(plain["grad"])),
                 "e2e": {"value": world * a.steps / (ms_e2e / 1e3), "unit": "evals/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches, "roofline": roof, "kernels": kern, "clocks": clocks}
