@@ -4,8 +4,8 @@ Drop-in for the TLR log-likelihood path of marysalvana/adaptive-tlr-pilots
 (codes/17_tlr_cholesky_pilot.py tlr_loglik and its callers), computed by hand-written sm_100a
 CUDA kernels behind the C ABI of include/tlr_b200.h.
 """
-from .tlr import (Likelihood, Plan, TLRFactor, TLRLogLik, dense_loglik, get_plan, loglik,  # noqa: F401
-                  morton_order, neg_loglik_tlr, release_plans, tile_bounds, tlr_loglik, tlr_loglik_grad)
+from .tlr import (Likelihood, Plan, PlanBatch, TLRFactor, TLRLogLik, dense_loglik, get_plan,  # noqa: F401
+                  loglik, morton_order, neg_loglik_tlr, release_plans, tile_bounds, tlr_loglik, tlr_loglik_grad)
 
-__all__ = ["Likelihood", "Plan", "TLRFactor", "TLRLogLik", "dense_loglik", "get_plan", "loglik", "morton_order",
-           "neg_loglik_tlr", "release_plans", "tile_bounds", "tlr_loglik", "tlr_loglik_grad"]
+__all__ = ["Likelihood", "Plan", "PlanBatch", "TLRFactor", "TLRLogLik", "dense_loglik", "get_plan", "loglik",
+           "morton_order", "neg_loglik_tlr", "release_plans", "tile_bounds", "tlr_loglik", "tlr_loglik_grad"]

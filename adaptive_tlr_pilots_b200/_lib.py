@@ -53,6 +53,10 @@ SIGNATURES = {
                                        ctypes.c_double, ctypes.POINTER(ctypes.c_double),
                                        ctypes.POINTER(ctypes.c_double), ctypes.POINTER(TlrInfo),
                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "tlr_loglik_grad_batch": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                             ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_double,
+                                             ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                             ctypes.POINTER(ctypes.c_int)]),
     "tlr_loglik_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                        ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_double,
                                        ctypes.POINTER(ctypes.c_double), ctypes.POINTER(TlrInfo),

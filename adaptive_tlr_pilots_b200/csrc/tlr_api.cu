@@ -30,7 +30,8 @@ int cuda_check(cudaError_t e, const char* what) {
 
 constexpr int kLevels = 4;      // sketch widths 16, 32, 64, 128
 constexpr int kMaxK = 128;
-constexpr int kPowerPasses = 4;  // Z = T^T T P passes per level
+constexpr int kPowerPasses = 4;       // Z = T^T T P passes per level (FP64 parity path)
+constexpr int kPowerPassesMixed = 3;  // mixed path: the exact residual still bounds every tail
 constexpr int kMargin = 8;       // accepted rank must leave k - margin unresolved directions
 
 }  // namespace
@@ -47,7 +48,7 @@ struct tlr_plan {
   // data
   double *xy = nullptr, *y = nullptr, *rhs = nullptr, *z = nullptr;
   // factor
-  double *D = nullptr, *U = nullptr, *V = nullptr, *Wd = nullptr;
+  double *D = nullptr, *U = nullptr, *V = nullptr, *Wd = nullptr, *Yd = nullptr;
   int *rank = nullptr, *rank0 = nullptr, *ti = nullptr, *tj = nullptr;
   // compression chunk
   int chunk = 0, nblk = 0;
@@ -55,17 +56,28 @@ struct tlr_plan {
   double *T = nullptr, *P = nullptr, *Z = nullptr, *C = nullptr, *gscr = nullptr, *gsv = nullptr;
   double *parts = nullptr, *fparts = nullptr;
   // recompression scratch
-  int nslots = 0;
+  int nslots = 0, nsm = 148;
   size_t slot_doubles = 0;
   double* rcs = nullptr;
   // look-ahead: POTRF(k+1) runs on a second stream while step k's recompression runs
   cudaStream_t side = nullptr;
   cudaEvent_t ev_panel = nullptr, ev_diag = nullptr;
+  // backward: the TLR solve for alpha runs on the side stream, one event per block row
+  std::vector<cudaEvent_t> ev_alpha;
   // results
   double *ldpart = nullptr, *qpart = nullptr, *out = nullptr;
   int* status = nullptr;
-  // host copies
-  std::vector<int> h_rank, h_rank0, h_ti, h_tj;
+  // host copies; results land in pinned memory so that evaluations can be queued back to back
+  std::vector<int> h_ti, h_tj;
+  int *h_rank = nullptr, *h_rank0 = nullptr;  // pinned, ntiles each
+  struct HostBlock {
+    int status;
+    int pad;
+    double out[4];
+    double grad[3];
+    double work[2 * TLR_NKINDS];
+  }* hb = nullptr;  // pinned
+  double bw_sigma2 = 0.0, bw_inv_range = 0.0, bw_eta = 0.0;
   std::vector<void*> allocs;
   int precision = TLR_PRECISION_FP64;
   // launch accounting and optional per-kernel event timing
@@ -160,7 +172,8 @@ int run_compression(tlr_plan* p, double sigma2, double inv_range, int rule_fixed
       const int k = 16 << lev;
       double* Pp = p->P;
       double* Zp = p->Z;
-      for (int it = 0; it < kPowerPasses; ++it) {
+      const int passes = p->precision == TLR_PRECISION_MIXED ? kPowerPassesMixed : kPowerPasses;
+      for (int it = 0; it < passes; ++it) {
         LAUNCH(TLR_K_SKETCH, tlr::launch_sketch(p->T, p->n, p->b, k, base, p->ti, p->tj, p->need, Pp, Zp, ldp, it == 0 ? 1 : 0, 0,
                                 nc, p->status, s));
         LAUNCH(TLR_K_ORTH, tlr::launch_orth(Zp, p->n, p->b, k, ldp, base, p->tj, p->need, p->gscr, nc, p->status, s));
@@ -181,11 +194,11 @@ int run_compression(tlr_plan* p, double sigma2, double inv_range, int rule_fixed
 int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugget, int rule_fixed, double thr_rel,
                       double thr_abs) {
   cudaStream_t s = p->stream, sd = p->side;
-  LAUNCH(TLR_K_DIAG, tlr::launch_diag_build(p->xy, p->n, p->b, 0, sigma2, inv_range, nugget, p->U, p->Wd, p->rank,
+  LAUNCH(TLR_K_DIAG, tlr::launch_diag_build(p->xy, p->n, p->b, 0, sigma2, inv_range, nugget, p->U, p->Yd, p->rank,
                                             p->cap, p->D, p->status, s));
   LAUNCH(TLR_K_POTRF, tlr::launch_potrf(p->D, p->n, p->b, 0, p->rhs, p->z, p->ldpart, p->qpart, p->status, s));
   for (int k = 0; k < p->nB; ++k) {
-    LAUNCH(TLR_K_TRSM, tlr::launch_trsm(p->D, p->n, p->b, k, p->nB, p->U, p->V, p->Wd, p->rank, p->cap, p->z, p->rhs,
+    LAUNCH(TLR_K_TRSM, tlr::launch_trsm(p->D, p->n, p->b, k, p->nB, p->U, p->V, p->Wd, p->Yd, p->rank, p->cap, p->z, p->rhs,
                                         p->status, s));
     const bool ahead = k + 1 < p->nB;
     if (ahead) {
@@ -194,14 +207,14 @@ int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugge
       TRY(cuda_check(cudaEventRecord(p->ev_panel, s), "event"));
       TRY(cuda_check(cudaStreamWaitEvent(sd, p->ev_panel, 0), "wait"));
       LAUNCH_ON(sd, TLR_K_DIAG, tlr::launch_diag_build(p->xy, p->n, p->b, k + 1, sigma2, inv_range, nugget, p->U,
-                                                       p->Wd, p->rank, p->cap, p->D, p->status, sd));
+                                                       p->Yd, p->rank, p->cap, p->D, p->status, sd));
       LAUNCH_ON(sd, TLR_K_POTRF, tlr::launch_potrf(p->D, p->n, p->b, k + 1, p->rhs, p->z, p->ldpart, p->qpart,
                                                    p->status, sd));
       TRY(cuda_check(cudaEventRecord(p->ev_diag, sd), "event"));
     }
     LAUNCH(TLR_K_RECOMPRESS, tlr::launch_recompress(p->n, p->b, k, p->nB, p->U, p->V, p->rank, p->cap, rule_fixed,
-                                                    thr_rel, thr_abs, p->rcs, p->slot_doubles, p->nslots, p->status,
-                                                    s));
+                                                    thr_rel, thr_abs, p->rcs, p->slot_doubles, p->nslots, nullptr,
+                                                    nullptr, p->status, s));
     if (ahead) TRY(cuda_check(cudaStreamWaitEvent(s, p->ev_diag, 0), "wait"));
   }
   LAUNCH(TLR_K_FINISH, tlr::launch_finish(p->nB, p->n, p->ldpart, p->qpart, p->out, p->status, s));
@@ -242,7 +255,9 @@ struct LaunchRange {
   size_t part_off;
 };
 
-int run_backward(tlr_plan* p, double sigma2, double inv_range, double eta, double* grad_host) {
+// Queue the backward pass of the last successful forward evaluation on the plan's stream (the
+// ranks of that evaluation are in the pinned host copy); the gradient lands in the pinned block.
+int run_backward(tlr_plan* p, double sigma2, double inv_range, double eta) {
   const int nB = p->nB, b = p->b, n = p->n;
   const size_t B = (size_t)b, BB = B * B;
   auto bsz = [&](int i) { return std::min(b, n - i * b); };
@@ -396,6 +411,20 @@ int run_backward(tlr_plan* p, double sigma2, double inv_range, double eta, doubl
                    "copies"));
   // launches
   LAUNCH(TLR_K_TRI_INV, tlr::launch_tri_inv(p->D, Li, n, b, nB, p->status, s));
+  // alpha = Sigma_t^{-1} y (block rows nB-1 .. 0) needs only the factor, z and the inverses of
+  // the diagonal tiles: it runs on the side stream while the selected-inversion GEMMs run here
+  while ((int)p->ev_alpha.size() < nB) {
+    cudaEvent_t e;
+    TRY(cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event"));
+    p->ev_alpha.push_back(e);
+  }
+  TRY(cuda_check(cudaEventRecord(p->ev_panel, s), "event"));
+  TRY(cuda_check(cudaStreamWaitEvent(p->side, p->ev_panel, 0), "wait"));
+  for (int m = nB - 1; m >= 0; --m) {
+    LAUNCH_ON(p->side, TLR_K_ALPHA, tlr::launch_alpha_step(n, b, m, nB, p->U, p->V, p->rank, p->cap, Li, p->z,
+                                                           base + oAl, base + oWk, p->status, p->side));
+    TRY(cuda_check(cudaEventRecord(p->ev_alpha[m], p->side), "event"));
+  }
   for (const LaunchRange& L : plan) {
     if (L.kind == 4) {
       LAUNCH(TLR_K_BWD_GEMM, tlr::launch_dgemm_batched(p->d_jobs + L.first, L.count, L.max_m, L.max_n, p->status,
@@ -410,22 +439,27 @@ int run_backward(tlr_plan* p, double sigma2, double inv_range, double eta, doubl
     } else if (L.kind == 1) {
       if (L.count) LAUNCH(TLR_K_BWD_COPY, tlr::launch_copy_cols(p->d_copy + L.first, L.count, p->status, s));
     } else if (L.kind == 2) {
-      LAUNCH(TLR_K_ALPHA, tlr::launch_alpha_step(n, b, L.m, nB, p->U, p->V, p->rank, p->cap, Li, p->z, base + oAl,
-                                                 base + oWk, p->status, s));
+      TRY(cuda_check(cudaStreamWaitEvent(s, p->ev_alpha[L.m], 0), "wait"));
     } else {
       LAUNCH(TLR_K_DTRACE, tlr::launch_dtrace_step(p->xy, n, b, L.m, nB, sigma2, inv_range, eta, Zb, base + oAl,
                                                    base + oPart + 3 * L.part_off, p->status, s));
     }
   }
   LAUNCH(TLR_K_GRAD_FINISH, tlr::launch_grad_finish(base + oPart, (long)nparts, base + oGrad, p->status, s));
-  int status = 0;
-  double g[3];
-  double work[2 * TLR_NKINDS];
-  TRY(cuda_check(cudaMemcpyAsync(g, base + oGrad, sizeof(double) * 3, cudaMemcpyDeviceToHost, s), "grad"));
-  TRY(cuda_check(cudaMemcpyAsync(&status, p->status, sizeof(int), cudaMemcpyDeviceToHost, s), "status"));
-  TRY(cuda_check(cudaMemcpyAsync(work, p->status + 4, sizeof(double) * 2 * TLR_NKINDS, cudaMemcpyDeviceToHost, s),
+  TRY(cuda_check(cudaMemcpyAsync(p->hb->grad, base + oGrad, sizeof(double) * 3, cudaMemcpyDeviceToHost, s), "grad"));
+  TRY(cuda_check(cudaMemcpyAsync(&p->hb->status, p->status, sizeof(int), cudaMemcpyDeviceToHost, s), "status"));
+  TRY(cuda_check(cudaMemcpyAsync(p->hb->work, p->status + 4, sizeof(double) * 2 * TLR_NKINDS,
+                                 cudaMemcpyDeviceToHost, s),
                  "work"));
-  TRY(cuda_check(cudaStreamSynchronize(s), "backward"));
+  return 0;
+}
+
+// Wait for the backward pass queued by run_backward and collect its gradient.
+int finish_backward(tlr_plan* p, double* grad_host) {
+  TRY(cuda_check(cudaSetDevice(p->device), "cudaSetDevice"));
+  TRY(cuda_check(cudaStreamSynchronize(p->stream), "backward"));
+  const int status = p->hb->status;
+  const double* work = p->hb->work;
   if (p->prof) {
     for (size_t q = 0; q < p->ev_kind.size(); ++q) {
       float ms = 0.f;
@@ -440,7 +474,7 @@ int run_backward(tlr_plan* p, double sigma2, double inv_range, double eta, doubl
     p->kbytes[q] += work[2 * q + 1];
   }
   if (status != 0) return fail(status < 0 ? status : TLR_ERR_CUDA, "backward pass failed");
-  for (int a = 0; a < 3; ++a) grad_host[a] = g[a];
+  for (int a = 0; a < 3; ++a) grad_host[a] = p->hb->grad[a];
   return 0;
 }
 
@@ -480,6 +514,7 @@ int tlr_plan_create(tlr_plan** plan, int n, int b, int cap, int device, void* st
   A(dalloc(p, &p->U, nt * B * cap));
   A(dalloc(p, &p->V, nt * B * cap));
   A(dalloc(p, &p->Wd, nt * (size_t)cap * cap));
+  A(dalloc(p, &p->Yd, nt * B * cap));
   A(dalloc(p, &p->rank, nt));
   A(dalloc(p, &p->rank0, nt));
   A(dalloc(p, &p->ti, nt));
@@ -500,7 +535,8 @@ int tlr_plan_create(tlr_plan** plan, int n, int b, int cap, int device, void* st
   A(dalloc(p, &p->fparts, ch * p->nblk));
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-  p->nslots = nsm * 4;
+  p->nsm = nsm;
+  p->nslots = nsm * 4;  // resident recompression CTAs (k_recompress: four per SM)
   p->slot_doubles = tlr::rc_slot_doubles(b, cap);
   A(dalloc(p, &p->rcs, (size_t)p->nslots * p->slot_doubles));
   if (rc == 0) {
@@ -536,8 +572,19 @@ int tlr_plan_create(tlr_plan** plan, int n, int b, int cap, int device, void* st
     delete p;
     return rc;
   }
-  p->h_rank.resize(nt);
-  p->h_rank0.resize(nt);
+  void *hr = nullptr, *hr0 = nullptr, *hbk = nullptr;
+  rc = cuda_check(cudaMallocHost(&hr, sizeof(int) * nt), "pinned ranks");
+  if (!rc) rc = cuda_check(cudaMallocHost(&hr0, sizeof(int) * nt), "pinned ranks");
+  if (!rc) rc = cuda_check(cudaMallocHost(&hbk, sizeof(tlr_plan::HostBlock)), "pinned results");
+  p->h_rank = static_cast<int*>(hr);
+  p->h_rank0 = static_cast<int*>(hr0);
+  p->hb = static_cast<tlr_plan::HostBlock*>(hbk);
+  if (rc != 0) {
+    tlr_plan_destroy(p);
+    return rc;
+  }
+  std::memset(p->h_rank, 0, sizeof(int) * nt);
+  std::memset(p->h_rank0, 0, sizeof(int) * nt);
   *plan = p;
   return 0;
 }
@@ -547,9 +594,13 @@ void tlr_plan_destroy(tlr_plan* plan) {
   cudaSetDevice(plan->device);
   if (plan->stream) cudaStreamSynchronize(plan->stream);
   for (cudaEvent_t e : plan->ev_pool) cudaEventDestroy(e);
+  for (cudaEvent_t e : plan->ev_alpha) cudaEventDestroy(e);
   if (plan->ev_panel) cudaEventDestroy(plan->ev_panel);
   if (plan->ev_diag) cudaEventDestroy(plan->ev_diag);
   if (plan->side) cudaStreamDestroy(plan->side);
+  if (plan->h_rank) cudaFreeHost(plan->h_rank);
+  if (plan->h_rank0) cudaFreeHost(plan->h_rank0);
+  if (plan->hb) cudaFreeHost(plan->hb);
   free_all(plan);
   delete plan;
 }
@@ -638,8 +689,13 @@ static void fill_info(const tlr_plan* p, int status, const double* out, tlr_info
   }
 }
 
-int tlr_loglik(tlr_plan* p, const double theta[3], int rule, double value, double* loglik, tlr_info* info,
-               int* factor_ranks, int* sigma_ranks) {
+}  // extern "C"
+
+namespace {
+
+// Queue one forward evaluation (compression, factorization, solve) on the plan's stream; the
+// status, log-likelihood, work counters and ranks are copied to pinned host memory at the end.
+int enqueue_forward(tlr_plan* p, const double theta[3], int rule, double value) {
   if (!p || !theta) return fail(TLR_ERR_ARG, "invalid arguments to tlr_loglik");
   if (!p->has_data) return fail(TLR_ERR_NOT_READY, "tlr_set_data has not been called");
   if (rule != TLR_RULE_FIXED && rule != TLR_RULE_ADAPTIVE) return fail(TLR_ERR_ARG, "rule must be fixed or adaptive");
@@ -660,20 +716,28 @@ int tlr_loglik(tlr_plan* p, const double theta[3], int rule, double value, doubl
     TRY(cuda_check(cudaMemcpyAsync(p->rank0, p->rank, sizeof(int) * p->ntiles, cudaMemcpyDeviceToDevice, s),
                    "rank0"));
   TRY(run_factorization(p, sigma2, 1.0 / range, sigma2 * eta, rule_fixed, thr_rel, thr_abs));
-  int status = 0;
-  double out[4] = {0, 0, 0, 0};
-  TRY(cuda_check(cudaMemcpyAsync(&status, p->status, sizeof(int), cudaMemcpyDeviceToHost, s), "status"));
-  TRY(cuda_check(cudaMemcpyAsync(out, p->out, sizeof(double) * 3, cudaMemcpyDeviceToHost, s), "out"));
-  double work[2 * TLR_NKINDS];
-  TRY(cuda_check(cudaMemcpyAsync(work, p->status + 4, sizeof(double) * 2 * TLR_NKINDS, cudaMemcpyDeviceToHost, s),
+  TRY(cuda_check(cudaMemcpyAsync(&p->hb->status, p->status, sizeof(int), cudaMemcpyDeviceToHost, s), "status"));
+  TRY(cuda_check(cudaMemcpyAsync(p->hb->out, p->out, sizeof(double) * 3, cudaMemcpyDeviceToHost, s), "out"));
+  TRY(cuda_check(cudaMemcpyAsync(p->hb->work, p->status + 4, sizeof(double) * 2 * TLR_NKINDS,
+                                 cudaMemcpyDeviceToHost, s),
                  "work"));
   if (p->ntiles > 0) {
-    TRY(cuda_check(cudaMemcpyAsync(p->h_rank.data(), p->rank, sizeof(int) * p->ntiles, cudaMemcpyDeviceToHost, s),
+    TRY(cuda_check(cudaMemcpyAsync(p->h_rank, p->rank, sizeof(int) * p->ntiles, cudaMemcpyDeviceToHost, s),
                    "ranks"));
-    TRY(cuda_check(cudaMemcpyAsync(p->h_rank0.data(), p->rank0, sizeof(int) * p->ntiles, cudaMemcpyDeviceToHost, s),
+    TRY(cuda_check(cudaMemcpyAsync(p->h_rank0, p->rank0, sizeof(int) * p->ntiles, cudaMemcpyDeviceToHost, s),
                    "ranks0"));
   }
-  TRY(cuda_check(cudaStreamSynchronize(s), "evaluation"));
+  p->bw_sigma2 = sigma2;
+  p->bw_inv_range = 1.0 / range;
+  p->bw_eta = eta;
+  return 0;
+}
+
+// Wait for the forward evaluation queued by enqueue_forward and report it (tlr_loglik's outputs).
+int finish_forward(tlr_plan* p, double* loglik, tlr_info* info, int* factor_ranks, int* sigma_ranks) {
+  TRY(cuda_check(cudaSetDevice(p->device), "cudaSetDevice"));
+  TRY(cuda_check(cudaStreamSynchronize(p->stream), "evaluation"));
+  const int status = p->hb->status;
   if (p->prof) {
     for (size_t q = 0; q < p->ev_kind.size(); ++q) {
       float ms = 0.f;
@@ -684,8 +748,8 @@ int tlr_loglik(tlr_plan* p, const double theta[3], int rule, double value, doubl
   p->ev_used = 0;
   p->ev_kind.clear();
   for (int q = 0; q < TLR_NKINDS; ++q) {
-    p->kflops[q] += work[2 * q];
-    p->kbytes[q] += work[2 * q + 1];
+    p->kflops[q] += p->hb->work[2 * q];
+    p->kbytes[q] += p->hb->work[2 * q + 1];
   }
   if (status < 0) {
     const char* why = status == TLR_ERR_RANK_CAP   ? "a tile rank exceeded the plan's rank capacity"
@@ -694,9 +758,19 @@ int tlr_loglik(tlr_plan* p, const double theta[3], int rule, double value, doubl
                                                    : "device error";
     return fail(status, why);
   }
-  fill_info(p, status, out, info, factor_ranks, sigma_ranks);
-  if (loglik) *loglik = status == 0 ? out[0] : NAN;
+  fill_info(p, status, p->hb->out, info, factor_ranks, sigma_ranks);
+  if (loglik) *loglik = status == 0 ? p->hb->out[0] : NAN;
   return status;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tlr_loglik(tlr_plan* p, const double theta[3], int rule, double value, double* loglik, tlr_info* info,
+               int* factor_ranks, int* sigma_ranks) {
+  TRY(enqueue_forward(p, theta, rule, value));
+  return finish_forward(p, loglik, info, factor_ranks, sigma_ranks);
 }
 
 int tlr_loglik_grad(tlr_plan* p, const double theta[3], int rule, double value, double* loglik, double* grad,
@@ -706,9 +780,44 @@ int tlr_loglik_grad(tlr_plan* p, const double theta[3], int rule, double value, 
   if (loglik) *loglik = ll;
   if (rc != 0) return rc;
   double g[3] = {0.0, 0.0, 0.0};
-  TRY(run_backward(p, theta[0], 1.0 / theta[1], theta[2], g));
+  TRY(run_backward(p, theta[0], 1.0 / theta[1], theta[2]));
+  TRY(finish_backward(p, g));
   if (grad)
     for (int a = 0; a < 3; ++a) grad[a] = g[a];
+  return 0;
+}
+
+int tlr_loglik_grad_batch(tlr_plan* const* plans, int count, const double* thetas, int rule, double value,
+                          double* loglik, double* grad, int* status) {
+  if (!plans || !thetas || count < 0) return fail(TLR_ERR_ARG, "invalid arguments to tlr_loglik_grad_batch");
+  for (int q = 0; q < count; ++q) {
+    if (!plans[q]) return fail(TLR_ERR_ARG, "a plan of the batch is NULL");
+    for (int r = 0; r < q; ++r)
+      if (plans[r] == plans[q]) return fail(TLR_ERR_ARG, "a plan appears twice in the batch");
+  }
+  // every forward pass is queued before any is waited on: the plans' streams overlap on the GPU
+  for (int q = 0; q < count; ++q) TRY(enqueue_forward(plans[q], thetas + 3 * q, rule, value));
+  std::vector<int> st(count, 0);
+  int first_error = 0;
+  for (int q = 0; q < count; ++q) {
+    double ll = NAN;
+    const int rc = finish_forward(plans[q], &ll, nullptr, nullptr, nullptr);
+    if (rc < 0 && !first_error) first_error = rc;
+    st[q] = rc;
+    if (loglik) loglik[q] = ll;
+  }
+  if (first_error) return first_error;
+  for (int q = 0; q < count; ++q)
+    if (st[q] == 0) TRY(run_backward(plans[q], thetas[3 * q], 1.0 / thetas[3 * q + 1], thetas[3 * q + 2]));
+  for (int q = 0; q < count; ++q) {
+    if (st[q] != 0) continue;
+    double g[3];
+    TRY(finish_backward(plans[q], g));
+    if (grad)
+      for (int a = 0; a < 3; ++a) grad[3 * q + a] = g[a];
+  }
+  if (status)
+    for (int q = 0; q < count; ++q) status[q] = st[q];
   return 0;
 }
 

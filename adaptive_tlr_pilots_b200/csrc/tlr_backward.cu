@@ -18,8 +18,12 @@
 // Kernels: a batched FP64 GEMM with optional column scatter, a batched lower-triangular
 // inverse (L^{-1} of every diagonal tile), the TLR backward solve for alpha, and the fused dSigma
 // generation + contraction.
+#include <cooperative_groups.h>
+
 #include "tlr_device.cuh"
 #include "tlr_kernels.h"
+
+namespace cg = cooperative_groups;
 
 namespace tlr {
 
@@ -191,18 +195,29 @@ int launch_copy_cols(const CopyJob* jobs, int njobs, const int* status, cudaStre
 
 // ----------------------------------------------------------------------------------------
 // alpha_m = L_mm^{-T} (z_m - sum_{i>m} V_im (U_im^T alpha_i))   (codes/17_tlr_cholesky_pilot.py:243-256
-// restated for one block row).  One CTA.
-__global__ void __launch_bounds__(256) k_alpha_step(int n, int b, int m, int nB, const double* TLR_RESTRICT U,
-                                                   const double* TLR_RESTRICT V, const int* TLR_RESTRICT rank,
-                                                   int cap, const double* TLR_RESTRICT Li,
-                                                   const double* TLR_RESTRICT z, double* TLR_RESTRICT alpha,
-                                                   double* TLR_RESTRICT work, const int* TLR_RESTRICT status) {
-  if (*status != 0) return;
-  const int bm = min(b, n - m * b);
+// restated for one block row).  One cluster of kAC CTAs, three phases separated by the cluster
+// barrier: t = [U_im^T alpha_i]_{i>m} (one warp per entry, lanes over rows); rhs = z_m - sum_i
+// V_im t_i (rows split across the cluster, four threads per row); alpha_m = L_mm^{-T} rhs (one
+// warp per output, lanes over the column of L_mm^{-1}).  t and rhs live in `work` (L2).
+constexpr int kAC = 8;
+
+__global__ void __cluster_dims__(kAC, 1, 1) __launch_bounds__(256)
+    k_alpha_step(int n, int b, int m, int nB, const double* TLR_RESTRICT U, const double* TLR_RESTRICT V,
+                 const int* TLR_RESTRICT rank, int cap, const double* TLR_RESTRICT Li, const double* TLR_RESTRICT z,
+                 double* TLR_RESTRICT alpha, double* TLR_RESTRICT work, const int* TLR_RESTRICT status) {
+  cg::cluster_group cluster = cg::this_cluster();
+  const int g = (int)cluster.block_rank();
+  __shared__ int go;
+  __shared__ int off[1025];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) go = (g == 0) ? (*status == 0) : 0;
+  cluster.sync();
+  const int ok = *cluster.map_shared_rank(&go, 0);
+  cluster.sync();  // rank 0's shared memory stays valid until every CTA has read it
+  if (!ok) return;
+  const int bm = min(b, n - m * b);
   double* rhs = work;      // b
   double* tq = work + b;   // sum_{i>m} r_im
-  __shared__ int off[1025];
   if (tid == 0) {
     int o = 0;
     for (int i = m + 1; i < nB; ++i) {
@@ -213,9 +228,9 @@ __global__ void __launch_bounds__(256) k_alpha_step(int n, int b, int m, int nB,
   }
   __syncthreads();
   const int R = off[nB - m - 1];
-  // t = [U_im^T alpha_i]_{i>m}: one warp per entry, lanes over rows (coalesced)
-  for (int e = warp; e < R; e += 8) {
-    int lo = 0, hi = nB - m - 1;  // find i with off[i-m-1] <= e < off[i-m]
+  const int nw = kAC * 8, gw = g * 8 + warp;
+  for (int e = gw; e < R; e += nw) {
+    int lo = 0, hi = nB - m - 1;  // off[lo] <= e < off[lo + 1]
     while (hi - lo > 1) {
       const int mid = (lo + hi) >> 1;
       if (off[mid] <= e) lo = mid; else hi = mid;
@@ -224,38 +239,47 @@ __global__ void __launch_bounds__(256) k_alpha_step(int n, int b, int m, int nB,
     const int bi = min(b, n - i * b);
     const double* u = U + ((size_t)i * (i - 1) / 2 + m) * b * cap + (size_t)q * b;
     const double* ai = alpha + (size_t)i * b;
-    double s = 0.0;
-    for (int a = lane; a < bi; a += 32) s = fma(u[a], ai[a], s);
-    s = warp_sum(s);
-    if (lane == 0) tq[e] = s;
+    double sacc = 0.0;
+    for (int a = lane; a < bi; a += 32) sacc = fma(u[a], ai[a], sacc);
+    sacc = warp_sum(sacc);
+    if (lane == 0) tq[e] = sacc;
   }
-  __syncthreads();
-  // rhs = z_m - sum_i V_im t_i
-  for (int a = tid; a < bm; a += 256) {
-    double s = z[(size_t)m * b + a];
-    for (int lo = 0; lo < nB - m - 1; ++lo) {
-      const int i = m + 1 + lo, r = off[lo + 1] - off[lo];
-      const double* v = V + ((size_t)i * (i - 1) / 2 + m) * b * cap;
-      for (int q = 0; q < r; ++q) s = fma(-v[(size_t)q * b + a], tq[off[lo] + q], s);
+  cluster.sync();
+  {
+    const int per = (bm + kAC - 1) / kAC;
+    const int r0 = g * per, r1 = min(bm, r0 + per);
+    const int quarter = tid & 3;
+    for (int base = r0; base < r1; base += 64) {  // the same trip count in every thread (shuffles)
+      const int a = base + (tid >> 2);
+      const bool act = a < r1;
+      double sacc = 0.0;
+      if (act)
+        for (int lo = 0; lo < nB - m - 1; ++lo) {
+          const int i = m + 1 + lo, r = off[lo + 1] - off[lo];
+          const double* v = V + ((size_t)i * (i - 1) / 2 + m) * b * cap;
+          for (int q = quarter; q < r; q += 4) sacc = fma(v[(size_t)q * b + a], tq[off[lo] + q], sacc);
+        }
+      sacc += __shfl_xor_sync(0xffffffffu, sacc, 1);
+      sacc += __shfl_xor_sync(0xffffffffu, sacc, 2);
+      if (act && quarter == 0) rhs[a] = z[(size_t)m * b + a] - sacc;
     }
-    rhs[a] = s;
   }
-  __syncthreads();
-  // alpha_m = L_mm^{-T} rhs: (Li^T rhs)_a = sum_c Li[c][a] rhs[c]; one warp per output, lanes over c
+  cluster.sync();
+  // alpha_m = L_mm^{-T} rhs: (Li^T rhs)_a = sum_{c >= a} Li[c][a] rhs[c]
   const double* L = Li + (size_t)m * b * b;
-  for (int a = warp; a < bm; a += 8) {
+  for (int a = gw; a < bm; a += nw) {
     const double* col = L + (size_t)a * b;
-    double s = 0.0;
-    for (int c = a + lane; c < bm; c += 32) s = fma(col[c], rhs[c], s);
-    s = warp_sum(s);
-    if (lane == 0) alpha[(size_t)m * b + a] = s;
+    double sacc = 0.0;
+    for (int c = a + lane; c < bm; c += 32) sacc = fma(col[c], rhs[c], sacc);
+    sacc = warp_sum(sacc);
+    if (lane == 0) alpha[(size_t)m * b + a] = sacc;
   }
 }
 
 int launch_alpha_step(int n, int b, int m, int nB, const double* U, const double* V, const int* rank, int cap,
                       const double* Li, const double* z, double* alpha, double* work, const int* status,
                       cudaStream_t s) {
-  k_alpha_step<<<1, 256, 0, s>>>(n, b, m, nB, U, V, rank, cap, Li, z, alpha, work, status);
+  k_alpha_step<<<kAC, 256, 0, s>>>(n, b, m, nB, U, V, rank, cap, Li, z, alpha, work, status);
   return (int)cudaGetLastError();
 }
 

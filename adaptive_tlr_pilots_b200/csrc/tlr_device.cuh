@@ -173,8 +173,13 @@ __device__ inline void cta_org2r(double* A, int lda, int m, int n, const double*
 // column norms are computed afresh at the start of every sweep and updated by the rotation
 // formulas within it (a_pp' = a_pp - t a_pq, a_qq' = a_qq + t a_pq), so a pair costs one inner
 // product.  `sig` needs n doubles, `iflag` one int of shared memory.  Returns the sweeps used.
+// With floor_rel > 0, a column whose squared norm is at most floor_rel times the largest squared
+// column norm counts as zero and is not rotated: columns at the rounding level of the others
+// (from cores assembled out of Gram matrices) would otherwise keep the relative test of their
+// pairs failing forever.
 __device__ inline int cta_jacobi_svd(double* M, int ldm, int m, int n, double* V, int ldv, double* sig,
-                                     int* perm, int* iflag, int max_sweeps = 40) {
+                                     int* perm, int* iflag, int max_sweeps = 40, double floor_rel = 0.0) {
+  __shared__ double s_floor2;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   for (int j = warp; j < n; j += nwarp)
     for (int i = lane; i < n; i += 32) V[(size_t)j * ldv + i] = (i == j) ? 1.0 : 0.0;
@@ -193,8 +198,16 @@ __device__ inline int cta_jacobi_svd(double* M, int ldm, int m, int n, double* V
         a = warp_sum(a);
         if (lane == 0) sig[c] = a;
       }
-      if (threadIdx.x == 0) *iflag = 0;
+      if (floor_rel > 0.0) __syncthreads();  // the column norms above come from every warp
+      if (threadIdx.x == 0) {
+        *iflag = 0;
+        double mx = 0.0;
+        if (floor_rel > 0.0)
+          for (int c = 0; c < n; ++c) mx = fmax(mx, sig[c]);
+        s_floor2 = floor_rel * mx;
+      }
       __syncthreads();
+      const double floor2 = s_floor2;
       for (int round = 0; round < np - 1; ++round) {
         for (int pr = warp; pr < np / 2; pr += nwarp) {
           // circle method: player 0 fixed, the others rotate
@@ -208,7 +221,7 @@ __device__ inline int cta_jacobi_svd(double* M, int ldm, int m, int n, double* V
           for (int t = lane; t < m; t += 32) apq += mp[t] * mq[t];
           apq = warp_sum(apq);
           const double app = sig[p], aqq = sig[q];
-          if (apq != 0.0 && apq * apq > tol2 * app * aqq) {
+          if (apq != 0.0 && apq * apq > tol2 * app * aqq && fmin(app, aqq) > floor2) {
             // t = tan of the rotation angle, the smaller root of t^2 + 2 zeta t - 1 = 0 with
             // zeta = (a_qq - a_pp) / (2 a_pq); for |zeta| > 1e7, t = 1 / (2 zeta) to full precision
             const double d = aqq - app;

@@ -3,10 +3,11 @@
 // Reference: codes/17_tlr_cholesky_pilot.py:168-205 (factorization), 230-240 (forward solve)
 // and 259-266 (log-likelihood).  Per step k, in stream order:
 //   k_diag_build(k)   A_kk = Sigma_kk - sum_{m<k} U_km (V_km^T V_km) U_km^T   (deferred updates,
-//                     same subtraction order m = 0, 1, ... as the reference's step-by-step updates)
+//                     subtracted in the order m = 0, 1, ... of the reference's step-by-step updates)
 //   k_potrf(k)        blocked Cholesky of A_kk (status k+1 when a pivot is not positive, as LAPACK
 //                     potrf), log det partial, z_k = L_kk^{-1} rhs_k
-//   k_trsm(k)         V_ik <- L_kk^{-1} V_ik for i > k; W_ik = V_ik^T V_ik; rhs_i -= U_ik (V_ik^T z_k)
+//   k_trsm(k)         V_ik <- L_kk^{-1} V_ik for i > k; W_ik = V_ik^T V_ik; Y_ik = U_ik W_ik;
+//                     rhs_i -= U_ik (V_ik^T z_k)
 //   k_recompress(k)   A_ij <- truncate([U_ij, -U_ik W], [V_ij, U_jk]) for k < j < i, W = V_ik^T V_jk,
 //                     skipped when r_ik = 0 or r_jk = 0 (17:189-194)
 // Layout in HBM: diagonal tiles column-major (ld b); off-diagonal factors U, V column-major
@@ -19,75 +20,89 @@ namespace tlr {
 __device__ __forceinline__ int tidx(int i, int j) { return i * (i - 1) / 2 + j; }
 
 // ----------------------------------------------------------------------------------------
+// A_kk = Sigma_kk - sum_{m<k} Y_km U_km^T, Y_km = U_km W_km (written by the panel solve of step m):
+// the deferred diagonal updates as one product of inner dimension R_k = sum_m r_km.  One CTA per
+// lower-triangular 32 x 32 block; the inner index runs over (m, q) in ascending order, 32 at a
+// time through shared memory.
 __global__ void __launch_bounds__(256) k_diag_build(const double* TLR_RESTRICT xy, int n, int b, int k,
                                                    double sigma2, double inv_range, double nugget,
-                                                   const double* TLR_RESTRICT U, const double* TLR_RESTRICT Wd,
+                                                   const double* TLR_RESTRICT U, const double* TLR_RESTRICT Y,
                                                    const int* TLR_RESTRICT rank, int cap, double* TLR_RESTRICT D,
                                                    const int* TLR_RESTRICT status) {
   if (*status != 0) return;
-  // lower-triangular 32x32 block (rb, cb), rb >= cb
   int blk = blockIdx.x, rb = 0;
   while (blk > rb) { blk -= rb + 1; ++rb; }
   const int cb = blk;
   const int bk = min(b, n - k * b);
   const int r0 = rb * 32, c0 = cb * 32;
-  if (threadIdx.x == 0 && rb == cb && rb == 0) {
-    double fl = 0.0;
-    for (int mt = 0; mt < k; ++mt) fl += 2.0 * bk * bk * rank[tidx(k, mt)];
-    add_work(status, 7, 0.5 * fl, 4.0 * bk * bk);
+  __shared__ int off[1025];
+  __shared__ int cm[32], cq[32];
+  __shared__ double Ya[32][33], Uc[32][33];
+  const int tid = threadIdx.x, cl = tid & 31, rl = tid >> 5;
+  if (tid == 0) {
+    int o = 0;
+    for (int m = 0; m < k; ++m) {
+      off[m] = o;
+      o += rank[tidx(k, m)];
+    }
+    off[k] = o;
+    if (rb == 0 && cb == 0) add_work(status, 7, 0.5 * 2.0 * bk * bk * o, 4.0 * bk * bk);
   }
-  __shared__ double Ua[32][33], Uc[32][33], Xc[32][33];
-  const int cl = threadIdx.x & 31, rl = threadIdx.x >> 5;
   double acc[4];
   const double2* p2 = reinterpret_cast<const double2*>(xy);
   const int cg = c0 + cl;
   const double2 pc = p2[k * b + min(cg, bk - 1)];
 #pragma unroll
-  for (int m = 0; m < 4; ++m) {
-    const int ag = r0 + rl + 8 * m;
+  for (int q = 0; q < 4; ++q) {
+    const int ag = r0 + rl + 8 * q;
     const double2 pa = p2[k * b + min(ag, bk - 1)];
-    acc[m] = matern32_cov(pa.x, pa.y, pc.x, pc.y, sigma2, inv_range) + (ag == cg ? nugget : 0.0);
+    acc[q] = matern32_cov(pa.x, pa.y, pc.x, pc.y, sigma2, inv_range) + (ag == cg ? nugget : 0.0);
   }
-  for (int mt = 0; mt < k; ++mt) {
-    const int t = tidx(k, mt);
-    const int r = rank[t];
-    if (r == 0) continue;
-    const double* Ut = U + (size_t)t * b * cap;
-    for (int q0 = 0; q0 < r; q0 += 32) {  // r <= cap; chunks of 32 columns of the inner dimension
-      const int rq = min(32, r - q0);
-      __syncthreads();
-      for (int e = threadIdx.x; e < 32 * rq; e += 256) {
-        const int rr = e & 31, q = e >> 5;
-        Ua[rr][q] = (r0 + rr < bk) ? Ut[(size_t)(q0 + q) * b + r0 + rr] : 0.0;
-        Uc[rr][q] = (c0 + rr < bk) ? Ut[(size_t)(q0 + q) * b + c0 + rr] : 0.0;
-      }
-      __syncthreads();
-      // Xc[c][p] = sum_q W[p][q] Uc[c][q] over the full inner range of W (needs all of U's columns)
-      for (int e = threadIdx.x; e < 32 * rq; e += 256) {
-        const int cc = e & 31, p = e >> 5;
-        double s = 0.0;
-        for (int q = 0; q < r; ++q) {
-          const double uq = (q >= q0 && q < q0 + rq) ? Uc[cc][q - q0]
-                                                     : ((c0 + cc < bk) ? Ut[(size_t)q * b + c0 + cc] : 0.0);
-          s = fma(Wd[(size_t)t * cap * cap + (size_t)q * cap + (q0 + p)], uq, s);
+  __syncthreads();
+  const int R = off[k];
+  for (int i0 = 0; i0 < R; i0 += 32) {
+    if (tid < 32) {
+      const int c = i0 + tid;
+      int m = -1, q = 0;
+      if (c < R) {
+        int lo = 0, hi = k;  // off[lo] <= c < off[hi]
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (off[mid] <= c) lo = mid; else hi = mid;
         }
-        Xc[cc][p] = s;
+        m = lo;
+        q = c - off[lo];
       }
-      __syncthreads();
-#pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        const int rr = rl + 8 * m;
-        double s = 0.0;
-        for (int p = 0; p < rq; ++p) s = fma(Ua[rr][p], Xc[cl][p], s);
-        acc[m] -= s;
-      }
+      cm[tid] = m;
+      cq[tid] = q;
     }
+    __syncthreads();
+    for (int e = tid; e < 32 * 32; e += 256) {
+      const int rr = e & 31, cc = e >> 5;
+      const int m = cm[cc];
+      double ya = 0.0, uc = 0.0;
+      if (m >= 0) {
+        const size_t off_t = (size_t)tidx(k, m) * b * cap + (size_t)cq[cc] * b;
+        if (r0 + rr < bk) ya = Y[off_t + r0 + rr];
+        if (c0 + rr < bk) uc = U[off_t + c0 + rr];
+      }
+      Ya[rr][cc] = ya;
+      Uc[rr][cc] = uc;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int cc = 0; cc < 32; ++cc) {
+      const double u = Uc[cl][cc];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] = fma(-Ya[rl + 8 * q][cc], u, acc[q]);
+    }
+    __syncthreads();
   }
   double* A = D + (size_t)k * b * b;
 #pragma unroll
-  for (int m = 0; m < 4; ++m) {
-    const int ag = r0 + rl + 8 * m;
-    if (ag < bk && cg < bk && ag >= cg) A[(size_t)cg * b + ag] = acc[m];
+  for (int q = 0; q < 4; ++q) {
+    const int ag = r0 + rl + 8 * q;
+    if (ag < bk && cg < bk && ag >= cg) A[(size_t)cg * b + ag] = acc[q];
   }
 }
 
@@ -95,7 +110,8 @@ __global__ void __launch_bounds__(256) k_diag_build(const double* TLR_RESTRICT x
 // Panel solve for column k: one CTA per row tile i > k.
 __global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int n, int b, int k, int nB,
                                              const double* TLR_RESTRICT U, double* TLR_RESTRICT V,
-                                             double* TLR_RESTRICT Wd, const int* TLR_RESTRICT rank, int cap,
+                                             double* TLR_RESTRICT Wd, double* TLR_RESTRICT Y,
+                                             const int* TLR_RESTRICT rank, int cap,
                                              const double* TLR_RESTRICT z, double* TLR_RESTRICT rhs,
                                              const int* TLR_RESTRICT status) {
   if (*status != 0) return;
@@ -111,6 +127,7 @@ __global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int 
   if (threadIdx.x == 0) add_work(status, 9, (double)bk * bk * r + 2.0 * bk * r * r + 4.0 * bk * r,
                                  8.0 * ((double)bk * bk * 0.5 + 2.0 * bk * r + bi * r));
   __shared__ double L11[32][33];
+  __shared__ double dinv[32];
   __shared__ double Xp[32][65];
   __shared__ double red[40];
   __shared__ double zt[64];
@@ -124,6 +141,7 @@ __global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int 
         const int a = e & 31, c = e >> 5;
         L11[a][c] = (a < pw && c < pw && a >= c) ? L[(size_t)(p0 + c) * b + p0 + a] : 0.0;
       }
+      if (tid < 32) dinv[tid] = tid < pw ? 1.0 / L[(size_t)(p0 + tid) * b + p0 + tid] : 0.0;
       __syncthreads();
       // diagonal block solve, one thread per column
       if (tid < rq) {
@@ -137,7 +155,7 @@ __global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int 
             double s = x[a];
 #pragma unroll
             for (int c = 0; c < a; ++c) s -= L11[a][c] * x[c];
-            x[a] = s / L11[a][a];
+            x[a] = s * dinv[a];
           }
         }
 #pragma unroll
@@ -184,6 +202,14 @@ __global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int 
   }
   __syncthreads();
   (void)red;
+  // Y_ik = U_ik W_ik, the factor of the deferred diagonal update of tile i
+  double* Yt = Y + (size_t)t * b * cap;
+  for (int a = tid; a < bi; a += 256)
+    for (int q = 0; q < r; ++q) {
+      double s = 0.0;
+      for (int p = 0; p < r; ++p) s = fma(Ut[(size_t)p * b + a], W[(size_t)q * cap + p], s);
+      Yt[(size_t)q * b + a] = s;
+    }
   double* ri = rhs + (size_t)i * b;
   if (r <= 64) {
     for (int a = tid; a < bi; a += 256) {
@@ -255,15 +281,20 @@ __device__ void cta_atb(const double* A, int lda, const double* B, int ldb, int 
 }
 
 constexpr int kRcSmemS = 32;  // cores with s <= 32 are solved in shared memory
+constexpr int kRcT = 256;     // threads per pair
+constexpr int kRcW = kRcT / 32;
+constexpr int kRcMinBlocks = 4;
 
-__global__ void __launch_bounds__(256, 4) k_recompress(int n, int b, int k, int nB, double* TLR_RESTRICT U,
+__global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b, int k, int nB, double* TLR_RESTRICT U,
                                                    double* TLR_RESTRICT V, int* TLR_RESTRICT rank, int cap,
                                                    int rule_fixed, double thr_rel, double thr_abs,
                                                    double* TLR_RESTRICT scratch, size_t slot_doubles,
+                                                   const int* TLR_RESTRICT list, const int* TLR_RESTRICT list_count,
                                                    int* TLR_RESTRICT status) {
   if (*status != 0) return;
   const int mB = nB - k - 1;  // trailing tiles
-  const long npairs = (long)mB * (mB - 1) / 2;
+  // every pair of the step, or only the listed ones (those the mixed path's warp kernels pass on)
+  const long npairs = list ? (long)*list_count : (long)mB * (mB - 1) / 2;
   RcScratch S = rc_slot(scratch + (size_t)blockIdx.x * slot_doubles, b, cap);
   extern __shared__ double rc_smem[];
   double* Msm = rc_smem;                            // kRcSmemS^2
@@ -280,12 +311,13 @@ __global__ void __launch_bounds__(256, 4) k_recompress(int n, int b, int k, int 
   __shared__ int rsel;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int ls = 2 * cap;
-  if (blockIdx.x == 0 && tid == 0) {  // the panel column k is read once per step
+  if (blockIdx.x == 0 && tid == 0 && !list) {  // the panel column k is read once per step
     double by = 0.0;
     for (int i = k + 1; i < nB; ++i) by += 8.0 * 2.0 * b * rank[tidx(i, k)];
     add_work(status, 10, 0.0, by);
   }
-  for (long pp = blockIdx.x; pp < npairs; pp += gridDim.x) {
+  for (long qq = blockIdx.x; qq < npairs; qq += gridDim.x) {
+    const long pp = list ? (long)list[qq] : qq;
     // decode pp -> (ii, jj), ii > jj >= 0 within the trailing block
     int ii = (int)((1.0 + sqrt(1.0 + 8.0 * (double)pp)) * 0.5);
     while ((long)ii * (ii - 1) / 2 > pp) --ii;
@@ -311,7 +343,7 @@ __global__ void __launch_bounds__(256, 4) k_recompress(int n, int b, int k, int 
     __syncthreads();
     // W = V_ik^T V_jk (ri x rj); column norms of U_ij
     cta_atb(Vik, b, Vjk, b, bk, ri, rj, S.W, cap, 0.0);
-    for (int c = warp; c < r1; c += 8) {
+    for (int c = warp; c < r1; c += kRcW) {
       const double* u = Uij + (size_t)c * b;
       const double* v = Vij + (size_t)c * b;
       double a = 0.0, av = 0.0;
@@ -329,7 +361,7 @@ __global__ void __launch_bounds__(256, 4) k_recompress(int n, int b, int k, int 
     __syncthreads();
     // X = -U_ik W (bi x rj)
     for (int q = 0; q < rj; ++q)
-      for (int a = tid; a < bi; a += 256) {
+      for (int a = tid; a < bi; a += kRcT) {
         double acc = 0.0;
         for (int p = 0; p < ri; ++p) acc = fma(Uik[(size_t)p * b + a], S.W[(size_t)q * cap + p], acc);
         S.X[(size_t)q * b + a] = -acc;
@@ -338,7 +370,7 @@ __global__ void __launch_bounds__(256, 4) k_recompress(int n, int b, int k, int 
     // block Gram-Schmidt twice against Q1 = U_ij diag(1/n1): C = Q1^T X, X -= Q1 C
     for (int pass = 0; pass < 2; ++pass) {
       if (r1 > 0) {
-        for (int e = warp; e < r1 * rj; e += 8) {
+        for (int e = warp; e < r1 * rj; e += kRcW) {
           const int u = e % r1, v = e / r1;
           const double* a = Uij + (size_t)u * b;
           const double* x = S.X + (size_t)v * b;
@@ -349,12 +381,12 @@ __global__ void __launch_bounds__(256, 4) k_recompress(int n, int b, int k, int 
         }
         __syncthreads();
         for (int v = 0; v < rj; ++v)
-          for (int a = tid; a < bi; a += 256) {
+          for (int a = tid; a < bi; a += kRcT) {
             double acc = 0.0;
             for (int u = 0; u < r1; ++u) acc = fma(Uij[(size_t)u * b + a] * ninv[u], S.G[(size_t)v * cap + u], acc);
             S.X[(size_t)v * b + a] -= acc;
           }
-        for (int e = tid; e < r1 * rj; e += 256) {
+        for (int e = tid; e < r1 * rj; e += kRcT) {
           const int u = e % r1, v = e / r1;
           const double inc = S.G[(size_t)v * cap + u];
           S.Cc[(size_t)v * cap + u] = pass == 0 ? inc : S.Cc[(size_t)v * cap + u] + inc;
@@ -366,21 +398,21 @@ __global__ void __launch_bounds__(256, 4) k_recompress(int n, int b, int k, int 
     cta_geqr2(S.X, b, bi, rj, sig, red);
     // V side: D = V_ij^T U_jk, Y = U_jk - V_ij D (twice)
     for (int v = 0; v < rj; ++v)
-      for (int a = tid; a < bj; a += 256) S.Y[(size_t)v * b + a] = Ujk[(size_t)v * b + a];
+      for (int a = tid; a < bj; a += kRcT) S.Y[(size_t)v * b + a] = Ujk[(size_t)v * b + a];
     __syncthreads();
     for (int pass = 0; pass < 2; ++pass) {
       if (r1 > 0) {
         cta_atb(Vij, b, S.Y, b, bj, r1, rj, S.G, cap, 0.0);
         __syncthreads();
-        for (int e = tid; e < r1 * rj; e += 256) S.G[(size_t)(e / r1) * cap + (e % r1)] *= nvinv[e % r1];
+        for (int e = tid; e < r1 * rj; e += kRcT) S.G[(size_t)(e / r1) * cap + (e % r1)] *= nvinv[e % r1];
         __syncthreads();
         for (int v = 0; v < rj; ++v)
-          for (int a = tid; a < bj; a += 256) {
+          for (int a = tid; a < bj; a += kRcT) {
             double acc = 0.0;
             for (int u = 0; u < r1; ++u) acc = fma(Vij[(size_t)u * b + a] * nvinv[u], S.G[(size_t)v * cap + u], acc);
             S.Y[(size_t)v * b + a] -= acc;
           }
-        for (int e = tid; e < r1 * rj; e += 256) {
+        for (int e = tid; e < r1 * rj; e += kRcT) {
           const int u = e % r1, v = e / r1;
           const double inc = S.G[(size_t)v * cap + u];
           S.Dd[(size_t)v * cap + u] = pass == 0 ? inc : S.Dd[(size_t)v * cap + u] + inc;
@@ -390,7 +422,7 @@ __global__ void __launch_bounds__(256, 4) k_recompress(int n, int b, int k, int 
     }
     // R_u = [[diag(n1), C], [0, R2]] (s x s, ld ls)
     for (int c = 0; c < s; ++c)
-      for (int a = tid; a < s; a += 256) {
+      for (int a = tid; a < s; a += kRcT) {
         double vu = 0.0;
         if (a < r1) vu = (c < r1) ? (a == c ? n1[a] : 0.0) : S.Cc[(size_t)(c - r1) * cap + a];
         else if (c >= r1 && a <= c && a - r1 < bi) vu = S.X[(size_t)(c - r1) * b + (a - r1)];
@@ -401,7 +433,7 @@ __global__ void __launch_bounds__(256, 4) k_recompress(int n, int b, int k, int 
     cta_geqr2(S.Y, b, bj, rj, tau3, red);
     // R_v = [[I, D], [0, R3]]
     for (int c = 0; c < s; ++c)
-      for (int a = tid; a < s; a += 256) {
+      for (int a = tid; a < s; a += kRcT) {
         double vv = 0.0;
         if (a < r1) vv = (c < r1) ? (a == c ? nvv[a] : 0.0) : S.Dd[(size_t)(c - r1) * cap + a];
         else if (c >= r1 && a <= c && a - r1 < bj) vv = S.Y[(size_t)(c - r1) * b + (a - r1)];
@@ -411,7 +443,7 @@ __global__ void __launch_bounds__(256, 4) k_recompress(int n, int b, int k, int 
     cta_org2r(S.Y, b, bj, rj, tau3);
     if (rj > bj) {  // a ragged tile shorter than the rank: the extra basis columns are zero
       for (int v = bj; v < rj; ++v)
-        for (int a = tid; a < bj; a += 256) S.Y[(size_t)v * b + a] = 0.0;
+        for (int a = tid; a < bj; a += kRcT) S.Y[(size_t)v * b + a] = 0.0;
       __syncthreads();
     }
     // re-orthogonalise Q3 against the normalised V_ij once
@@ -419,7 +451,7 @@ __global__ void __launch_bounds__(256, 4) k_recompress(int n, int b, int k, int 
       cta_atb(Vij, b, S.Y, b, bj, r1, rj, S.G, cap, 0.0);
       __syncthreads();
       for (int v = 0; v < rj; ++v)
-        for (int a = tid; a < bj; a += 256) {
+        for (int a = tid; a < bj; a += kRcT) {
           double acc = 0.0;
           for (int u = 0; u < r1; ++u)
             acc = fma(Vij[(size_t)u * b + a] * nvinv[u], S.G[(size_t)v * cap + u] * nvinv[u], acc);
@@ -429,7 +461,7 @@ __global__ void __launch_bounds__(256, 4) k_recompress(int n, int b, int k, int 
     }
     // core M = R_u R_v^T (s x s); both factors are upper triangular
     for (int c = 0; c < s; ++c)
-      for (int a = tid; a < s; a += 256) {
+      for (int a = tid; a < s; a += kRcT) {
         double acc = 0.0;
         const int t0 = a > c ? a : c;
         for (int t = t0; t < s; ++t) acc = fma(S.Ru[(size_t)t * ls + a], S.Rv[(size_t)t * ls + c], acc);
@@ -442,11 +474,11 @@ __global__ void __launch_bounds__(256, 4) k_recompress(int n, int b, int k, int 
     // instead of 6-16 on M itself.
     cta_geqr2(Mc, lc, s, s, sig, red);
     for (int c = 0; c < s; ++c)
-      for (int a = tid; a < s; a += 256) Zc[(size_t)c * lc + a] = (a >= c) ? Mc[(size_t)a * lc + c] : 0.0;
+      for (int a = tid; a < s; a += kRcT) Zc[(size_t)c * lc + a] = (a >= c) ? Mc[(size_t)a * lc + c] : 0.0;
     __syncthreads();
     cta_jacobi_svd(Zc, lc, s, s, Vc, lc, sig, perm, &iflag);
     // Vc <- normalised Z (right singular vectors of M), in place of the rotation matrix
-    for (int c = warp; c < s; c += 8) {
+    for (int c = warp; c < s; c += kRcW) {
       const double inv = sig[c] > 0.0 ? 1.0 / sig[c] : 0.0;
       for (int a = lane; a < s; a += 32) Vc[(size_t)c * lc + a] = Zc[(size_t)c * lc + a] * inv;
     }
@@ -473,14 +505,14 @@ __global__ void __launch_bounds__(256, 4) k_recompress(int n, int b, int k, int 
                8.0 * ((double)(bi + bj) * r1 + (double)(bi + bj) * rn));
     // G = R_v^T Vs_r (s x rn), H = W G_bottom (ri x rn)
     for (int c = 0; c < rn; ++c)
-      for (int t = tid; t < s; t += 256) {
+      for (int t = tid; t < s; t += kRcT) {
         const double* vc = Vc + (size_t)perm[c] * lc;
         double acc = 0.0;
         for (int a = 0; a <= t; ++a) acc = fma(S.Rv[(size_t)t * ls + a], vc[a], acc);
         S.G[(size_t)c * ls + t] = acc;
       }
     __syncthreads();
-    for (int e = tid; e < ri * rn; e += 256) {
+    for (int e = tid; e < ri * rn; e += kRcT) {
       const int p = e % ri, c = e / ri;
       double acc = 0.0;
       for (int q = 0; q < rj; ++q) acc = fma(S.W[(size_t)q * cap + p], S.G[(size_t)c * ls + r1 + q], acc);
@@ -492,13 +524,13 @@ __global__ void __launch_bounds__(256, 4) k_recompress(int n, int b, int k, int 
       const double* gc = S.G + (size_t)c * ls;
       const double* hc = S.Hh + (size_t)c * cap;
       const double* vc = Vc + (size_t)perm[c] * lc;
-      for (int a = tid; a < bi; a += 256) {
+      for (int a = tid; a < bi; a += kRcT) {
         double acc = 0.0;
         for (int t = 0; t < r1; ++t) acc = fma(Uij[(size_t)t * b + a], gc[t], acc);
         for (int p = 0; p < ri; ++p) acc = fma(-Uik[(size_t)p * b + a], hc[p], acc);
         S.Uo[(size_t)c * b + a] = acc;
       }
-      for (int a = tid; a < bj; a += 256) {
+      for (int a = tid; a < bj; a += kRcT) {
         double acc = 0.0;
         for (int t = 0; t < r1; ++t) acc = fma(Vij[(size_t)t * b + a] * nvinv[t], vc[t], acc);
         for (int t = 0; t < rj; ++t) acc = fma(S.Y[(size_t)t * b + a], vc[r1 + t], acc);
@@ -509,8 +541,8 @@ __global__ void __launch_bounds__(256, 4) k_recompress(int n, int b, int k, int 
     double* Uw = U + (size_t)tij * b * cap;
     double* Vw = V + (size_t)tij * b * cap;
     for (int c = 0; c < rn; ++c) {
-      for (int a = tid; a < bi; a += 256) Uw[(size_t)c * b + a] = S.Uo[(size_t)c * b + a];
-      for (int a = tid; a < bj; a += 256) Vw[(size_t)c * b + a] = S.Vo[(size_t)c * b + a];
+      for (int a = tid; a < bi; a += kRcT) Uw[(size_t)c * b + a] = S.Uo[(size_t)c * b + a];
+      for (int a = tid; a < bj; a += kRcT) Vw[(size_t)c * b + a] = S.Vo[(size_t)c * b + a];
     }
     if (tid == 0) rank[tij] = rn;
     __syncthreads();
@@ -532,33 +564,33 @@ __global__ void k_finish(int nB, int n, const double* ldpart, const double* qpar
 
 // ----------------------------------------------------------------------------------------
 int launch_diag_build(const double* xy, int n, int b, int k, double sigma2, double inv_range, double nugget,
-                      const double* U, const double* Wd, const int* rank, int cap, double* D, const int* status,
+                      const double* U, const double* Y, const int* rank, int cap, double* D, const int* status,
                       cudaStream_t s) {
   const int bk = std::min(b, n - k * b);
   const int nb = (bk + 31) / 32;
-  k_diag_build<<<nb * (nb + 1) / 2, 256, 0, s>>>(xy, n, b, k, sigma2, inv_range, nugget, U, Wd, rank, cap, D,
+  k_diag_build<<<nb * (nb + 1) / 2, 256, 0, s>>>(xy, n, b, k, sigma2, inv_range, nugget, U, Y, rank, cap, D,
                                                  status);
   return (int)cudaGetLastError();
 }
 
-int launch_trsm(const double* D, int n, int b, int k, int nB, const double* U, double* V, double* Wd,
+int launch_trsm(const double* D, int n, int b, int k, int nB, const double* U, double* V, double* Wd, double* Y,
                 const int* rank, int cap, const double* z, double* rhs, const int* status, cudaStream_t s) {
   if (nB - k - 1 <= 0) return 0;
-  k_trsm<<<nB - k - 1, 256, 0, s>>>(D, n, b, k, nB, U, V, Wd, rank, cap, z, rhs, status);
+  k_trsm<<<nB - k - 1, 256, 0, s>>>(D, n, b, k, nB, U, V, Wd, Y, rank, cap, z, rhs, status);
   return (int)cudaGetLastError();
 }
 
 int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, int rule_fixed,
                       double thr_rel, double thr_abs, double* scratch, size_t slot_doubles, int nslots,
-                      int* status, cudaStream_t s) {
+                      const int* list, const int* list_count, int* status, cudaStream_t s) {
   const long mB = nB - k - 1;
   const long npairs = mB * (mB - 1) / 2;
   if (npairs <= 0) return 0;
   const int grid = (int)std::min<long>(npairs, nslots);
   const size_t sm = (size_t)3 * kRcSmemS * kRcSmemS * 8;
   cudaFuncSetAttribute(k_recompress, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_recompress<<<grid, 256, sm, s>>>(n, b, k, nB, U, V, rank, cap, rule_fixed, thr_rel, thr_abs, scratch,
-                                     slot_doubles, status);
+  k_recompress<<<grid, kRcT, sm, s>>>(n, b, k, nB, U, V, rank, cap, rule_fixed, thr_rel, thr_abs, scratch,
+                                     slot_doubles, list, list_count, status);
   return (int)cudaGetLastError();
 }
 

@@ -31,16 +31,20 @@ int launch_finalize(int n, int b, int k, int ldp, int cap, int margin, int rule_
 
 // factorization
 int launch_diag_build(const double* xy, int n, int b, int k, double sigma2, double inv_range, double nugget,
-                      const double* U, const double* Wd, const int* rank, int cap, double* D, const int* status,
+                      const double* U, const double* Y, const int* rank, int cap, double* D, const int* status,
                       cudaStream_t s);
 int launch_potrf(double* D, int n, int b, int k, double* rhs, double* z, double* ldpart, double* qpart,
                  int* status, cudaStream_t s);
-int launch_trsm(const double* D, int n, int b, int k, int nB, const double* U, double* V, double* Wd,
+// nbatch tiles, tile q at D + q sD, rhs / z + q sV, ldpart / qpart / status + q sS
+int launch_potrf_batched(double* D, int n, int b, int k, double* rhs, double* z, double* ldpart, double* qpart,
+                         int* status, int nbatch, size_t sD, size_t sV, int sS, cudaStream_t s);
+int launch_trsm(const double* D, int n, int b, int k, int nB, const double* U, double* V, double* Wd, double* Y,
                 const int* rank, int cap, const double* z, double* rhs, const int* status, cudaStream_t s);
 size_t rc_slot_doubles(int b, int cap);
+// every trailing pair of step k, or (list != NULL) the *list_count pairs listed
 int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, int rule_fixed,
                       double thr_rel, double thr_abs, double* scratch, size_t slot_doubles, int nslots,
-                      int* status, cudaStream_t s);
+                      const int* list, const int* list_count, int* status, cudaStream_t s);
 int launch_finish(int nB, int n, const double* ldpart, const double* qpart, double* out, const int* status,
                   cudaStream_t s);
 

@@ -1,17 +1,22 @@
-// Cholesky of one diagonal tile spread over several SMs, then the tile's forward-solve block.
+// Cholesky of one diagonal tile per thread-block cluster, then the tile's forward-solve block.
 //
 // Reference: codes/17_tlr_cholesky_pilot.py:171-177 (scipy.linalg.cholesky of A_kk; a pivot that
 // is not positive stops the factorization, failed_at = k) and 230-240 (z_k = L_kk^{-1} rhs_k).
 //
-// One cooperative grid of G CTAs works on the column-major lower triangle of A_kk (L2-resident),
-// right-looking in panels of 32 columns:
-//   every CTA factors the 32 x 32 diagonal block redundantly in shared memory (identical inputs,
-//   identical results, so a non-positive pivot is seen by all CTAs at the same point and they all
-//   leave together); the rows below the block are split across CTAs (X = A21 L11^{-T});
-//   grid sync; the lower-triangular 32 x 32 blocks of the trailing matrix are split across CTAs
-//   (A22 -= X X^T); grid sync.
-// The forward solve is fused: each CTA solves z_p = L11^{-1} rhs_p for the panel's rows and
-// subtracts X z_p from the right-hand side rows it owns; CTA 0 writes z_k, log det and z_k^T z_k.
+// A cluster of kPC CTAs works on the column-major lower triangle of A_kk (L2-resident),
+// right-looking in panels of 32 columns, with the cluster's hardware barrier between phases:
+//   every CTA factors the 32 x 32 diagonal block redundantly (warp 0, the rows in registers;
+//   identical inputs give identical results, so a non-positive pivot stops every CTA at the same
+//   panel) and inverts it (lane c forms column c of L11^{-1});
+//   the panel rows below are split across the cluster, four threads per row: X = A21 L11^{-T} as
+//   independent dot products (no substitution chain), and rhs_rows -= X z_p with
+//   z_p = L11^{-1} rhs_p (the fused forward solve);
+//   cluster barrier; the lower-triangular 32 x 32 blocks of the trailing matrix are split across
+//   the cluster (A22 -= X X^T); cluster barrier.
+// Several tiles (one per parameter vector of a batch) are factored by independent clusters of
+// one launch.  The status word is read once by rank 0 and shared through distributed shared
+// memory, so every CTA of a cluster takes the same branch even when another stream writes the
+// status meanwhile.
 #include <cooperative_groups.h>
 
 #include "tlr_device.cuh"
@@ -22,34 +27,46 @@ namespace cg = cooperative_groups;
 namespace tlr {
 
 constexpr int kPB = 32;  // panel width
+constexpr int kPC = 8;   // CTAs per cluster (one cluster per tile)
 
-__global__ void __launch_bounds__(256) k_potrf_coop(double* TLR_RESTRICT D, int n, int b, int k,
-                                                   double* TLR_RESTRICT rhs, double* TLR_RESTRICT z,
-                                                   double* TLR_RESTRICT ldpart, double* TLR_RESTRICT qpart,
-                                                   int* TLR_RESTRICT status) {
-  cg::grid_group grid = cg::this_grid();
-  if (*status != 0) return;  // every CTA reads the same value: all leave together
+__global__ void __cluster_dims__(kPC, 1, 1) __launch_bounds__(256)
+    k_potrf_cluster(double* TLR_RESTRICT D, int n, int b, int k, double* TLR_RESTRICT rhs, double* TLR_RESTRICT z,
+                    double* TLR_RESTRICT ldpart, double* TLR_RESTRICT qpart, int* TLR_RESTRICT status,
+                    size_t sD, size_t sV, int sS) {
+  cg::cluster_group cluster = cg::this_cluster();
+  const int g = (int)cluster.block_rank(), G = kPC;
+  const int bz = blockIdx.x / kPC;  // which tile of the batch
+  D += bz * sD;
+  rhs += bz * sV;
+  z += bz * sV;
+  ldpart += bz * (size_t)sS;
+  qpart += bz * (size_t)sS;
+  status += bz * sS;
+  __shared__ double L11[kPB][kPB + 1];
+  __shared__ double Li[kPB][kPB + 1];  // L11^{-1}
+  __shared__ double dinv[kPB];
+  __shared__ double zp[kPB];
+  __shared__ double Pa[kPB][kPB + 1];
+  __shared__ double Pc[kPB][kPB + 1];
+  __shared__ int go, fail;
+  __shared__ double logdet_acc, quad_acc;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    go = (g == 0) ? (*status == 0) : 0;
+    logdet_acc = 0.0;
+    quad_acc = 0.0;
+  }
+  cluster.sync();
+  const int ok = *cluster.map_shared_rank(&go, 0);
+  cluster.sync();  // rank 0's shared memory stays valid until every CTA has read it
+  if (!ok) return;
   const int bk = min(b, n - k * b);
   double* A = D + (size_t)k * b * b;
   double* rk = rhs + (size_t)k * b;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int G = gridDim.x, g = blockIdx.x;
-  __shared__ double L11[kPB][kPB + 1];
-  __shared__ double Pa[kPB][kPB + 1];
-  __shared__ double Pc[kPB][kPB + 1];
-  __shared__ double zp[kPB];
-  __shared__ int fail;
-  __shared__ double logdet_acc, quad_acc;
-  if (tid == 0) {
-    fail = 0;
-    logdet_acc = 0.0;
-    quad_acc = 0.0;
-    if (g == 0) add_work(status, 8, (double)bk * bk * bk / 3.0 + (double)bk * bk, 8.0 * bk * bk);
-  }
+  if (g == 0 && tid == 0) add_work(status, 8, (double)bk * bk * bk / 3.0 + (double)bk * bk, 8.0 * bk * bk);
   for (int p0 = 0; p0 < bk; p0 += kPB) {
     const int pw = min(kPB, bk - p0);
     const int m = bk - p0 - pw;
-    __syncthreads();
     if (warp == 0) {
       // Cholesky of the pw x pw diagonal block, lane = row, the row in registers
       double row[kPB];
@@ -64,9 +81,9 @@ __global__ void __launch_bounds__(256) k_potrf_coop(double* TLR_RESTRICT D, int 
           if (!(d > 0.0)) {
             bad = 1;  // the same pivot in every lane: the whole warp stops here
           } else {
-            const double sd = sqrt(d);
+            const double sd = sqrt(d), rsd = 1.0 / sd;
             if (lane == c) row[c] = sd;
-            if (lane > c) row[c] /= sd;
+            if (lane > c) row[c] *= rsd;
 #pragma unroll
             for (int j = c + 1; j < kPB; ++j) {
               const double ljc = __shfl_sync(0xffffffffu, row[c], j);
@@ -76,71 +93,91 @@ __global__ void __launch_bounds__(256) k_potrf_coop(double* TLR_RESTRICT D, int 
         }
       }
 #pragma unroll
-      for (int j = 0; j < kPB; ++j) L11[lane][j] = (j <= lane) ? row[j] : 0.0;
+      for (int j = 0; j < kPB; ++j) L11[lane][j] = (j <= lane && lane < pw && j < pw) ? row[j] : 0.0;
+      if (lane == 0) fail = bad;
       __syncwarp();
-      if (lane == 0) {
-        fail = bad;
-        if (!bad) {
-          double s = logdet_acc;
-          for (int c = 0; c < pw; ++c) s += log(L11[c][c]);
-          logdet_acc = s;
-        }
-      }
-      // z_p = L11^{-1} rhs_p (the forward solve of this block, fused)
+      dinv[lane] = (!bad && lane < pw) ? 1.0 / L11[lane][lane] : 0.0;
+      __syncwarp();
       if (!bad) {
-        double v = (lane < pw) ? rk[p0 + lane] : 0.0;
-        for (int c = 0; c < pw; ++c) {
-          const double xc = __shfl_sync(0xffffffffu, v, c) / L11[c][c];
-          if (lane == c) v = xc;
-          if (lane > c) v = fma(-L11[lane][c], xc, v);
+        // column `lane` of L11^{-1} by forward substitution
+        double x[kPB];
+#pragma unroll
+        for (int r = 0; r < kPB; ++r) {
+          double s = (r == lane) ? 1.0 : 0.0;
+#pragma unroll
+          for (int q = 0; q < r; ++q) s = fma(-L11[r][q], x[q], s);
+          x[r] = (r < pw) ? s * dinv[r] : 0.0;
         }
-        zp[lane] = (lane < pw) ? v : 0.0;
+#pragma unroll
+        for (int r = 0; r < kPB; ++r) Li[r][lane] = x[r];
+        __syncwarp();
+        // z_p = L11^{-1} rhs_p (one load per lane, broadcast by shuffles), log det
+        const double rv = lane < pw ? rk[p0 + lane] : 0.0;
+        double v = 0.0;
+#pragma unroll
+        for (int q = 0; q < kPB; ++q) v = fma(Li[lane][q], __shfl_sync(0xffffffffu, rv, q), v);
+        zp[lane] = lane < pw ? v : 0.0;
+        if (g == 0) {
+          const double ld = warp_sum(lane < pw ? log(L11[lane][lane]) : 0.0);
+          if (lane == 0) logdet_acc += ld;
+        }
       }
     }
     __syncthreads();
     if (fail) {
       if (g == 0 && tid == 0) atomicCAS(status, 0, k + 1);
-      return;  // all CTAs of the grid take this branch at the same panel
+      return;  // every CTA of the cluster leaves at the same panel
     }
-    if (g == 0 && tid == 0) {
-      double q = quad_acc;
-      for (int c = 0; c < pw; ++c) {
-        z[(size_t)k * b + p0 + c] = zp[c];
-        q += zp[c] * zp[c];
-      }
-      quad_acc = q;
-    }
-    // panel rows below, split across CTAs: X = A21 L11^{-T}; rhs_rows -= X z_p
-    const int per = (m + G - 1) / G;
-    const int r0 = g * per, r1 = min(m, r0 + per);
-    for (int row = r0 + tid; row < r1; row += blockDim.x) {
-      double x[kPB];
+    // panel rows below, split across the cluster, four threads per row (eight outputs each)
+    {
+      const int per = (m + G - 1) / G;
+      const int r0 = g * per, r1 = min(m, r0 + per);
+      const int quarter = tid & 3;
+      for (int base = r0; base < r1; base += 64) {  // the same trip count in every thread (shuffles)
+        const int row = base + (tid >> 2);
+        const bool act = row < r1;
+        const size_t ar = (size_t)p0 + pw + (act ? row : 0);
+        double a[kPB];
 #pragma unroll
-      for (int c = 0; c < kPB; ++c) x[c] = (c < pw) ? A[(size_t)(p0 + c) * b + p0 + pw + row] : 0.0;
-      double dz = 0.0;
+        for (int q = 0; q < kPB; ++q) a[q] = (act && q < pw) ? A[(size_t)(p0 + q) * b + ar] : 0.0;
+        double xo[8];
+        double dz = 0.0;
 #pragma unroll
-      for (int c = 0; c < kPB; ++c) {
-        if (c < pw) {
-          double s = x[c];
+        for (int u = 0; u < 8; ++u) {
+          const int c = quarter * 8 + u;
+          double s = 0.0;
 #pragma unroll
-          for (int j = 0; j < c; ++j) s = fma(-x[j], L11[c][j], s);
-          x[c] = s / L11[c][c];
-          dz = fma(x[c], zp[c], dz);
+          for (int q = 0; q < kPB; ++q) s = fma(a[q], Li[c][q], s);
+          xo[u] = s;
+          dz = fma(s, zp[c], dz);
+        }
+        dz += __shfl_xor_sync(0xffffffffu, dz, 1);
+        dz += __shfl_xor_sync(0xffffffffu, dz, 2);
+        if (act) {
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int c = quarter * 8 + u;
+            if (c < pw) A[(size_t)(p0 + c) * b + ar] = xo[u];
+          }
+          if (quarter == 0) rk[ar] -= dz;
         }
       }
-#pragma unroll
-      for (int c = 0; c < kPB; ++c)
-        if (c < pw) A[(size_t)(p0 + c) * b + p0 + pw + row] = x[c];
-      rk[p0 + pw + row] -= dz;
     }
-    __threadfence();
-    grid.sync();
-    // the factored diagonal block goes back only now: every CTA has finished reading it
-    if (g == 0)
+    cluster.sync();
+    if (g == 0) {
       for (int e = tid; e < pw * pw; e += blockDim.x) {
         const int i = e % pw, j = e / pw;
         if (i >= j) A[(size_t)(p0 + j) * b + p0 + i] = L11[i][j];
       }
+      if (tid == 0) {
+        double q = quad_acc;
+        for (int c = 0; c < pw; ++c) {
+          z[(size_t)k * b + p0 + c] = zp[c];
+          q += zp[c] * zp[c];
+        }
+        quad_acc = q;
+      }
+    }
     // trailing update of the lower triangle in 32 x 32 blocks
     const int mb = (m + 31) / 32;
     const int nblk = mb * (mb + 1) / 2;
@@ -159,7 +196,8 @@ __global__ void __launch_bounds__(256) k_potrf_coop(double* TLR_RESTRICT D, int 
       __syncthreads();
       const int cl = tid & 31, rl = tid >> 5;  // column cl, rows rl + 8q
       double acc[4] = {0.0, 0.0, 0.0, 0.0};
-      for (int t = 0; t < pw; ++t) {
+#pragma unroll 8
+      for (int t = 0; t < kPB; ++t) {
         const double pc = Pc[cl][t];
 #pragma unroll
         for (int q = 0; q < 4; ++q) acc[q] = fma(Pa[rl + 8 * q][t], pc, acc[q]);
@@ -174,8 +212,7 @@ __global__ void __launch_bounds__(256) k_potrf_coop(double* TLR_RESTRICT D, int 
         }
       }
     }
-    __threadfence();
-    grid.sync();
+    cluster.sync();
   }
   if (g == 0 && tid == 0) {
     ldpart[k] = 2.0 * logdet_acc;
@@ -185,17 +222,12 @@ __global__ void __launch_bounds__(256) k_potrf_coop(double* TLR_RESTRICT D, int 
 
 int launch_potrf(double* D, int n, int b, int k, double* rhs, double* z, double* ldpart, double* qpart,
                  int* status, cudaStream_t s) {
-  static int grid_cache = 0;
-  if (grid_cache == 0) {
-    int dev = 0, nsm = 0, per = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_potrf_coop, 256, 0);
-    grid_cache = std::max(1, std::min(64, nsm * std::max(per, 1)));
-  }
-  int G = grid_cache;
-  void* args[] = {&D, &n, &b, &k, &rhs, &z, &ldpart, &qpart, &status};
-  cudaLaunchCooperativeKernel((void*)k_potrf_coop, dim3(G), dim3(256), args, 0, s);
+  return launch_potrf_batched(D, n, b, k, rhs, z, ldpart, qpart, status, 1, 0, 0, 0, s);
+}
+
+int launch_potrf_batched(double* D, int n, int b, int k, double* rhs, double* z, double* ldpart, double* qpart,
+                         int* status, int nbatch, size_t sD, size_t sV, int sS, cudaStream_t s) {
+  k_potrf_cluster<<<kPC * nbatch, 256, 0, s>>>(D, n, b, k, rhs, z, ldpart, qpart, status, sD, sV, sS);
   return (int)cudaGetLastError();
 }
 

@@ -199,6 +199,66 @@ class Plan:
         return np.ascontiguousarray(u[:r].T), np.ascontiguousarray(v[:r].T)
 
 
+class PlanBatch:
+    """`count` plans on one device, each with its own stream, sharing the sites and observations:
+    evaluate(thetas) runs one batched call (tlr_loglik_grad_batch) in which every plan's forward
+    pass is queued before any is waited on, so the GPU overlaps the plans' latency-bound
+    factorization steps.  The batch of MCMC chains or optimizer restarts of one iteration."""
+
+    def __init__(self, n, b, count, cap=64, device=0, precision="mixed"):
+        torch = _torch()
+        self.n, self.b, self.count, self.device = int(n), int(b), int(count), int(device)
+        self.lib = _lib.load()
+        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(self.count)]
+        self.plans = []
+        for st in self.streams:
+            with torch.cuda.stream(st):
+                p = Plan(self.n, self.b, cap, self.device)
+            p.set_precision(precision)
+            self.plans.append(p)
+        self.nB = self.plans[0].nB
+
+    def set_data(self, S, y):
+        """One host-to-device copy (numpy or torch, pinned host memory welcome), then a device copy
+        into every plan."""
+        torch = _torch()
+        dev = torch.device("cuda", self.device)
+        S_t = torch.as_tensor(S, dtype=torch.float64).to(dev, non_blocking=True).contiguous()
+        y_t = torch.as_tensor(y, dtype=torch.float64).to(dev, non_blocking=True).contiguous()
+        if S_t.shape != (self.n, 2) or y_t.shape != (self.n,):
+            raise ValueError(f"expected S of shape ({self.n}, 2) and y of shape ({self.n},)")
+        torch.cuda.current_stream(dev).synchronize()
+        for p in self.plans:
+            p._data = (S_t, y_t)
+            _lib.check(p.lib.tlr_set_data(p.handle, ctypes.c_void_p(S_t.data_ptr()), ctypes.c_void_p(y_t.data_ptr())))
+
+    def evaluate(self, thetas, rule, value):
+        """[(loglik | None, grad | None, status)] for up to `count` parameter vectors."""
+        if rule not in RULES:
+            raise ValueError(f"rule must be one of {sorted(RULES)}, got {rule!r}")
+        th = np.ascontiguousarray(np.atleast_2d(np.asarray(thetas, dtype=np.float64)))
+        m = th.shape[0]
+        if m > self.count or th.shape[1] != 3:
+            raise ValueError(f"thetas must be at most {self.count} x 3")
+        handles = (ctypes.c_void_p * m)(*[p.handle.value for p in self.plans[:m]])
+        ll = np.full(m, np.nan)
+        g = np.zeros((m, 3))
+        st = np.zeros(m, dtype=np.int32)
+        dp = ctypes.POINTER(ctypes.c_double)
+        _lib.check(self.lib.tlr_loglik_grad_batch(handles, m, th.ctypes.data_as(dp), RULES[rule], float(value),
+                                                  ll.ctypes.data_as(dp), g.ctypes.data_as(dp),
+                                                  st.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        for p in self.plans[:m]:
+            p.generation += 1
+        return [(float(ll[q]) if st[q] == 0 else None, g[q].copy() if st[q] == 0 else None, int(st[q]))
+                for q in range(m)]
+
+    def close(self):
+        for p in self.plans:
+            p.close()
+        self.plans = []
+
+
 class TLRFactor:
     """Lazy view of the factor left in a plan by the last evaluation (L_diag, L_off as in
     codes/17_tlr_cholesky_pilot.py:215).  Invalidated by the plan's next evaluation."""

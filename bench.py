@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=1, help="0: skip the CPU baseline leg")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--plain-steps", type=int, default=2, help="timed steps of the plain FP64 comparison (0: skip)")
+    ap.add_argument("--batch", type=int, default=4, help="parameter vectors per step (one batched call)")
+    ap.add_argument("--dense", type=int, default=1, help="0: skip the dense FP64 oracle")
     return ap.parse_args()
 
 
@@ -50,7 +52,8 @@ METRIC = "TLR loglik+grad evals/s at N=50k vs plain FP64 on B200; |dl| vs FP64 d
 
 def workload(a):
     return {"workload": f"TLR log-likelihood, N={a.n}, b={a.b}, Matern-3/2 theta=(1,0.3,0.05), adaptive tau={a.tau}",
-            "n": a.n, "b": a.b, "rule": "adaptive", "tau": a.tau, "precision": a.precision, "theta_per_step": 1,
+            "n": a.n, "b": a.b, "rule": "adaptive", "tau": a.tau, "precision": a.precision,
+            "theta_per_step": a.batch, "batch": "theta_0 = (1, 0.3, 0.05), the others theta_0 exp(0.05 z), seeded",
             "l2": "inputs larger than L2 (per-evaluation working set several GB)"}
 
 
@@ -183,15 +186,25 @@ def main():
         if world > 1:
             dist.barrier()
 
+    def max_over_ranks(ms):
+        t = torch.tensor([ms], device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     S, y, _, _ = synth.simulate_field(a.n, THETA, device=local)
-    plan = tlr.Plan(a.n, a.b, cap=64, device=local)
-    plan.set_data(S, y)
+    # dense FP64 oracle at the bench's theta (cuSOLVER through torch; not part of the timed path)
+    dense, gdense = (synth.dense_loglik_grad_gpu(S, y, THETA, device=local) if rank == 0 and a.dense
+                     else (None, None))
+    torch.cuda.empty_cache()
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
     # the plain FP64 path (every step in FP64, one theta per evaluation): the comparison leg
     plain = None
     if a.plain_steps > 0:
+        plan = tlr.Plan(a.n, a.b, cap=64, device=local)
+        plan.set_data(S, y)
         plan.set_precision("fp64")
         ev64 = plan.evaluate(THETA, "adaptive", a.tau, grad=True)
         barrier()
@@ -201,60 +214,64 @@ def main():
             ev64 = plan.evaluate(THETA, "adaptive", a.tau, grad=True)
         e1.record(stream)
         torch.cuda.synchronize()
-        t = torch.tensor([e0.elapsed_time(e1)], device="cuda")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms64 = float(t.item()) / a.plain_steps
+        ms64 = max_over_ranks(e0.elapsed_time(e1)) / a.plain_steps
         plain = {"value": world * 1e3 / ms64, "unit": "evals/s", "ms_per_step": ms64, "steps": a.plain_steps,
-                 "loglik": ev64.loglik, "grad": ev64.grad.tolist()}
+                 "loglik": ev64.loglik, "grad": ev64.grad.tolist(), "batch": 1, "precision": "fp64"}
+        plan.close()
+        torch.cuda.empty_cache()
 
-    plan.set_precision(a.precision)
+    # the headline: B parameter vectors per step (chains near the mode, the first at theta), each
+    # step one batched call through the public PlanBatch / tlr_loglik_grad_batch
+    B = a.batch
+    rng = np.random.default_rng(20261021)
+    thetas = np.array(THETA)[None, :] * np.exp(0.05 * rng.standard_normal((B, 3)))
+    thetas[0] = THETA
+    pb = tlr.PlanBatch(a.n, a.b, B, cap=64, device=local, precision=a.precision)
+    pb.set_data(S, y)
     for _ in range(a.warmup):
-        ev = plan.evaluate(THETA, "adaptive", a.tau, grad=True)
-    plan.set_profiling(True)
-    plan.kernel_stats(reset=True)
+        out = pb.evaluate(thetas, "adaptive", a.tau)
+    for p in pb.plans:
+        p.set_profiling(True)
+        p.kernel_stats(reset=True)
     sampler = ClockSampler(local)
     sampler.start()
     barrier()
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(a.steps):
-        ev = plan.evaluate(THETA, "adaptive", a.tau, grad=True)
+        out = pb.evaluate(thetas, "adaptive", a.tau)
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
     clocks = sampler.stop()
-    ms = e0.elapsed_time(e1)
-    stats = plan.kernel_stats(reset=True)
-    plan.set_profiling(False)
-    t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(e0.elapsed_time(e1))
+    stats = {}
+    for p in pb.plans:
+        for k, v in p.kernel_stats(reset=True).items():
+            acc = stats.setdefault(k, dict(ms=0.0, launches=0, flops=0.0, bytes=0.0))
+            for f in acc:
+                acc[f] += v[f]
+        p.set_profiling(False)
+    ll0, g0, st0 = out[0]
 
-    # end to end through the public drop-in (host buffers in pinned memory, copies inside)
-    S_pin = torch.from_numpy(np.ascontiguousarray(S)).pin_memory().numpy()
-    y_pin = torch.from_numpy(np.ascontiguousarray(y)).pin_memory().numpy()
-    bounds = tlr.tile_bounds(a.n, a.b)
+    # end to end through the public API: every step copies the sites and observations from pinned
+    # host memory to the device, evaluates the batch and reads the results back
+    S_pin = torch.from_numpy(np.ascontiguousarray(S)).pin_memory()
+    y_pin = torch.from_numpy(np.ascontiguousarray(y)).pin_memory()
     barrier()
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(a.steps):
-        ll_e2e, g_e2e, info_e2e = tlr.tlr_loglik_grad(S_pin, y_pin, THETA, bounds, "adaptive", a.tau, device=local,
-                                                       precision=a.precision)
+        pb.set_data(S_pin, y_pin)
+        out_e2e = pb.evaluate(thetas, "adaptive", a.tau)
     e1.record(stream)
     torch.cuda.synchronize()
-    ms_e2e = e0.elapsed_time(e1)
-    t = torch.tensor([ms_e2e], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_e2e = float(t.item())
-    ntiles = plan.ntiles
-    h2d = S_pin.nbytes + y_pin.nbytes
-    d2h = 4 + 8 * 3 + 8 * 3 + 2 * 8 * 2 * 18 + 2 * 4 * ntiles
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+    h2d = S_pin.numel() * 8 + y_pin.numel() * 8 + thetas.nbytes
+    d2h = B * (8 + 3 * 8 + 4)
+    pb.close()
 
     if rank == 0:
-        dense, gdense = synth.dense_loglik_grad_gpu(S, y, THETA, device=local)
         pk, pk_kind = peaks()
         launches = int(sum(v["launches"] for v in stats.values()))
         top = max(stats, key=lambda k: stats[k]["ms"])
@@ -270,29 +287,28 @@ def main():
         kern = {k: {"ms_per_step": v["ms"] / a.steps, "launches_per_step": v["launches"] / a.steps,
                     "gflop_per_step": v["flops"] / a.steps / 1e9, "gb_per_step": v["bytes"] / a.steps / 1e9}
                 for k, v in stats.items() if v["launches"]}
-        line = {"metric": METRIC, "value": world * a.steps / (ms_max / 1e3), "unit": "evals/s", "n_gpus": world,
+        value = world * a.steps * B / (ms_max / 1e3)
+        line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f64+tf32x3",
                 "data": "synthetic (seeded reference protocol, y = L z with the dense FP64 Cholesky)",
                 "config": dict(workload(a), parallelism=f"replicas x{world}"),
-                "loglik": ev.loglik, "dense_loglik": dense,
-                "abs_dloglik_vs_dense": None if dense is None else abs(ev.loglik - dense),
-                "grad": ev.grad.tolist(), "dense_grad": None if gdense is None else list(gdense),
-                "grad_rel_err_vs_dense": None if gdense is None else
-                float(np.linalg.norm(ev.grad - gdense) / np.linalg.norm(gdense)),
-                "mean_rank_factor": ev.info["mean_rank_factor"], "max_rank_factor": ev.info["max_rank_factor"],
+                "loglik": ll0, "dense_loglik": dense,
+                "abs_dloglik_vs_dense": None if (dense is None or ll0 is None) else abs(ll0 - dense),
+                "grad": None if g0 is None else g0.tolist(), "dense_grad": None if gdense is None else list(gdense),
+                "grad_rel_err_vs_dense": None if (gdense is None or g0 is None) else
+                float(np.linalg.norm(g0 - gdense) / np.linalg.norm(gdense)),
                 "plain_fp64": plain,
-                "speedup_vs_plain_fp64": None if plain is None else (world * a.steps / (ms_max / 1e3)) / plain["value"],
-                "abs_dloglik_vs_plain_fp64": None if plain is None else abs(ev.loglik - plain["loglik"]),
-                "grad_rel_err_vs_plain_fp64": None if plain is None else
-                float(np.linalg.norm(ev.grad - np.array(plain["grad"])) / np.linalg.norm(plain["grad"])),
-                "e2e": {"value": world * a.steps / (ms_e2e / 1e3), "unit": "evals/s", "h2d_bytes_per_step": h2d,
+                "speedup_vs_plain_fp64": None if plain is None else value / plain["value"],
+                "abs_dloglik_vs_plain_fp64": None if (plain is None or ll0 is None) else abs(ll0 - plain["loglik"]),
+                "grad_rel_err_vs_plain_fp64": None if (plain is None or g0 is None) else
+                float(np.linalg.norm(g0 - np.array(plain["grad"])) / np.linalg.norm(plain["grad"])),
+                "e2e": {"value": world * a.steps * B / (ms_e2e / 1e3), "unit": "evals/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches, "roofline": roof, "kernels": kern, "clocks": clocks}
         if world == 1 and a.cpu_sample:
             line["cpu_baseline"] = cpu_baseline(S, y, a)
         print(json.dumps(line), flush=True)
-    plan.close()
     tlr.release_plans()
     if world > 1:
         dist.destroy_process_group()

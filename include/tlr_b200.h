@@ -101,6 +101,18 @@ int tlr_loglik(tlr_plan* plan, const double theta[3], int rule, double value, do
 int tlr_loglik_grad(tlr_plan* plan, const double theta[3], int rule, double value, double* loglik, double* grad,
                     tlr_info* info, int* factor_ranks, int* sigma_ranks);
 
+/* Batched log-likelihood and gradient: plans[q] evaluates thetas[3q .. 3q+2] (count plans, all
+ * distinct, same device, each with its own stream and its data loaded).  Every forward pass is
+ * queued before any is waited on, then every backward pass likewise, so the GPU overlaps the
+ * plans' latency-bound factorization steps (a batch of MCMC chains or optimizer restarts shares
+ * one call).  loglik[q] (NaN when not PD), grad[3q .. 3q+2] (when status[q] == 0) and status[q]
+ * (0 ok, k + 1 when diagonal tile k is not positive definite) are host arrays; loglik, grad and
+ * status may be NULL.  Returns 0 when every evaluation ran, < 0 on an error of any of them.  No
+ * counterpart in the reference (its MCMC evaluates one chain at a time,
+ * codes/19_tlr_mcmc_gpu.py:170-202). */
+int tlr_loglik_grad_batch(tlr_plan* const* plans, int count, const double* thetas, int rule, double value,
+                          double* loglik, double* grad, int* status);
+
 /* The same evaluation with HOST sites and observations (Morton-ordered), copied to the device
  * inside the call: the end-to-end form of tlr_loglik for callers that hold numpy arrays. */
 int tlr_loglik_host(tlr_plan* plan, const double* xy_host, const double* y_host, const double theta[3], int rule,
