@@ -5,7 +5,9 @@ Drop-in for the TLR log-likelihood path of marysalvana/adaptive-tlr-pilots
 CUDA kernels behind the C ABI of include/tlr_b200.h.
 """
 from .tlr import (Likelihood, Plan, PlanBatch, TLRFactor, TLRLogLik, dense_loglik, get_plan,  # noqa: F401
-                  loglik, morton_order, neg_loglik_tlr, release_plans, tile_bounds, tlr_loglik, tlr_loglik_grad)
+                  loglik, morton_order, neg_loglik_tlr, release_plans, skill, tile_bounds, tlr_loglik,
+                  tlr_loglik_grad, tlr_predict)
 
 __all__ = ["Likelihood", "Plan", "PlanBatch", "TLRFactor", "TLRLogLik", "dense_loglik", "get_plan", "loglik",
-           "morton_order", "neg_loglik_tlr", "release_plans", "tile_bounds", "tlr_loglik", "tlr_loglik_grad"]
+           "morton_order", "neg_loglik_tlr", "release_plans", "skill", "tile_bounds", "tlr_loglik",
+           "tlr_loglik_grad", "tlr_predict"]

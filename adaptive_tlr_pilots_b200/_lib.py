@@ -61,6 +61,8 @@ SIGNATURES = {
                                        ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_double,
                                        ctypes.POINTER(ctypes.c_double), ctypes.POINTER(TlrInfo),
                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "tlr_factor_solve": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "tlr_factor_matvec": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
     "tlr_get_diag_tile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "tlr_get_offdiag_tile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                             ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),

@@ -78,6 +78,7 @@ struct tlr_plan {
     double work[2 * TLR_NKINDS];
   }* hb = nullptr;  // pinned
   double bw_sigma2 = 0.0, bw_inv_range = 0.0, bw_eta = 0.0;
+  bool factor_ok = false;  // the last evaluation completed: D, U, V, rank hold its factor
   std::vector<void*> allocs;
   int precision = TLR_PRECISION_FP64;
   // launch accounting and optional per-kernel event timing
@@ -704,6 +705,7 @@ int enqueue_forward(tlr_plan* p, const double theta[3], int rule, double value) 
     return fail(TLR_ERR_ARG, "theta must be finite with range > 0");
   TRY(cuda_check(cudaSetDevice(p->device), "cudaSetDevice"));
   cudaStream_t s = p->stream;
+  p->factor_ok = false;
   // thresholds: codes/17_tlr_cholesky_pilot.py:143-150 (b = largest tile = b)
   const int rule_fixed = rule == TLR_RULE_FIXED;
   const double thr_rel = rule_fixed ? value : 0.0;
@@ -760,6 +762,7 @@ int finish_forward(tlr_plan* p, double* loglik, tlr_info* info, int* factor_rank
   }
   fill_info(p, status, p->hb->out, info, factor_ranks, sigma_ranks);
   if (loglik) *loglik = status == 0 ? p->hb->out[0] : NAN;
+  p->factor_ok = status == 0;
   return status;
 }
 
@@ -863,6 +866,29 @@ int tlr_plan_kernel_stats(tlr_plan* p, double* ms, long long* launches, double* 
       p->kbytes[q] = 0.0;
     }
   return 0;
+}
+
+int tlr_factor_solve(tlr_plan* p, double* x_dev, int m, int trans) {
+  if (!p || !x_dev || m < 0 || (trans != 0 && trans != 1)) return fail(TLR_ERR_ARG, "invalid arguments to tlr_factor_solve");
+  if (!p->factor_ok) return fail(TLR_ERR_NOT_READY, "the plan holds no completed factorization");
+  if (m == 0) return 0;
+  TRY(cuda_check(cudaSetDevice(p->device), "cudaSetDevice"));
+  const int rc = tlr::launch_factor_solve(p->D, p->U, p->V, p->rank, p->cap, p->n, p->b, p->nB, x_dev, m, trans,
+                                          p->stream);
+  if (rc) return fail(TLR_ERR_CUDA, std::string("solve launch: ") + cudaGetErrorString((cudaError_t)rc));
+  return cuda_check(cudaStreamSynchronize(p->stream), "solve");
+}
+
+int tlr_factor_matvec(tlr_plan* p, const double* z_dev, double* y_dev, int m) {
+  if (!p || !z_dev || !y_dev || m < 0 || z_dev == y_dev)
+    return fail(TLR_ERR_ARG, "invalid arguments to tlr_factor_matvec");
+  if (!p->factor_ok) return fail(TLR_ERR_NOT_READY, "the plan holds no completed factorization");
+  if (m == 0) return 0;
+  TRY(cuda_check(cudaSetDevice(p->device), "cudaSetDevice"));
+  const int rc = tlr::launch_factor_matvec(p->D, p->U, p->V, p->rank, p->cap, p->n, p->b, p->nB, z_dev, y_dev, m,
+                                           p->stream);
+  if (rc) return fail(TLR_ERR_CUDA, std::string("matvec launch: ") + cudaGetErrorString((cudaError_t)rc));
+  return cuda_check(cudaStreamSynchronize(p->stream), "matvec");
 }
 
 int tlr_get_diag_tile(tlr_plan* p, int k, double* out_host) {

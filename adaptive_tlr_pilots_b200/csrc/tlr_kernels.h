@@ -74,6 +74,12 @@ int launch_dtrace_step(const double* xy, int n, int b, int m, int nB, double sig
                        const double* Zbuf, const double* alpha, double* part, const int* status, cudaStream_t s);
 int launch_grad_finish(const double* part, long nparts, double* grad, const int* status, cudaStream_t s);
 
+// solves and products with the factor (tlr_solve.cu); column-major n x m, ld n
+int launch_factor_solve(const double* D, const double* U, const double* V, const int* rank, int cap, int n, int b,
+                        int nB, double* X, int m, int trans, cudaStream_t s);
+int launch_factor_matvec(const double* D, const double* U, const double* V, const int* rank, int cap, int n, int b,
+                         int nB, const double* Z, double* Y, int m, cudaStream_t s);
+
 // error reporting shared by the library's translation units (message for tlr_last_error)
 int set_error(int code, const char* msg);
 

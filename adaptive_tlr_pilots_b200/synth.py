@@ -99,3 +99,35 @@ def dense_loglik_grad_gpu(S, y, theta, device=0, chunk=4096):
         del Kinv
         torch.cuda.empty_cache()
     return ll, g
+
+
+def simulate_field_tlr(n, theta=(1.0, 0.3, 0.05), b=1000, tau=0.02, n_pred=300, seed=20261020, device=0):
+    """Field for sizes where no dense factor fits (codes/17_tlr_cholesky_pilot.py:326-339, --sim tlr):
+    sites and split as the dense protocol, then y = L z with L the TLR factor of Sigma(S; theta)
+    at the tight adaptive budget tau = 0.02 (tlr_factor_matvec on the device), and held-out values
+    from the TLR predictive mean plus noise.  Returns (S, y, Sp, yp, info) with S, y Morton-ordered."""
+    import torch
+
+    from .tlr import Plan, TLRFactor, morton_order, tlr_predict, tile_bounds
+    rng = np.random.default_rng(seed)
+    n_tot = n + n_pred
+    S_all = rng.random((n_tot, 2))
+    perm = rng.permutation(n_tot)
+    obs, hold = perm[:n], perm[n:]
+    S, Sp = S_all[obs], S_all[hold]
+    S = S[morton_order(S, device=device)]
+    plan = Plan(n, b, cap=128, device=device)  # tau = 0.02 keeps ranks up to ~100 near the diagonal
+    plan.set_data(S, np.zeros(n))
+    ev = plan.evaluate(theta, "adaptive", tau)
+    if ev.status != 0:
+        plan.close()
+        raise RuntimeError("simulation factor did not complete")
+    z = rng.standard_normal(n_tot)
+    y = plan.matvec_L(torch.from_numpy(z[:n])).cpu().numpy()
+    plan.set_data(S, y)  # the factor does not depend on y; the solves below use it as is
+    fac = TLRFactor(plan)
+    mu_p, sd_p = tlr_predict(S, y, Sp, theta, tile_bounds(n, b), fac)
+    yp = mu_p + sd_p * z[n:]
+    info = dict(ev.info, factor_fraction_of_dense=ev.info["stored_factor"] / (n * (n + 1) / 2))
+    plan.close()
+    return S, y, Sp, yp, info

@@ -180,6 +180,33 @@ class Plan:
         _lib.check(self.lib.tlr_plan_kernel_stats(self.handle, ms, cnt, fl, by, nk, 1 if reset else 0))
         return {k: dict(ms=ms[q], launches=cnt[q], flops=fl[q], bytes=by[q]) for q, k in enumerate(_lib.KERNEL_KINDS)}
 
+    # products and solves with the factor of the last successful evaluation (device, in place)
+    def _cols(self, X):
+        torch = _torch()
+        X = torch.as_tensor(X, dtype=torch.float64, device=self.dev)
+        squeeze = X.dim() == 1
+        X2 = X[:, None] if squeeze else X
+        if X2.shape[0] != self.n:
+            raise ValueError(f"expected {self.n} rows")
+        return X2.t().contiguous().clone(), squeeze  # column-major n x m storage = row-major m x n
+
+    def solve(self, B, trans=False):
+        """L^{-1} B (trans False) or L^{-T} B (trans True) on the device; B n or n x m."""
+        Xt, squeeze = self._cols(B)
+        _lib.check(self.lib.tlr_factor_solve(self.handle, ctypes.c_void_p(Xt.data_ptr()), Xt.shape[0],
+                                             1 if trans else 0))
+        X = Xt.t()
+        return X[:, 0] if squeeze else X
+
+    def matvec_L(self, Z):
+        """L Z on the device; Z n or n x m."""
+        Zt, squeeze = self._cols(Z)
+        Yt = _torch().empty_like(Zt)
+        _lib.check(self.lib.tlr_factor_matvec(self.handle, ctypes.c_void_p(Zt.data_ptr()),
+                                              ctypes.c_void_p(Yt.data_ptr()), Zt.shape[0]))
+        Y = Yt.t()
+        return Y[:, 0] if squeeze else Y
+
     # factor access (checking / prediction)
     def diag_tile(self, k):
         bk = min(self.b, self.n - k * self.b)
@@ -276,6 +303,21 @@ class TLRFactor:
         self._check()
         return [self.plan.diag_tile(k) for k in range(self.plan.nB)]
 
+    def forward(self, B):
+        """Solve L X = B on the device (codes/17_tlr_cholesky_pilot.py:230-240 tlr_forward)."""
+        self._check()
+        return self.plan.solve(B, trans=False)
+
+    def backward(self, Z):
+        """Solve L^T X = Z on the device (17:243-256 tlr_backward)."""
+        self._check()
+        return self.plan.solve(Z, trans=True)
+
+    def matvec(self, Z):
+        """L Z on the device (17:218-227 tlr_matvec_L)."""
+        self._check()
+        return self.plan.matvec_L(Z)
+
     @property
     def L_off(self):
         self._check()
@@ -369,6 +411,43 @@ def tlr_loglik(S, y, theta, bounds, rule, value, cap=64, device=0):
     if ev.status != 0:
         return None, None, ev.info
     return ev.loglik, TLRFactor(plan), ev.info
+
+
+def _cross_cov(Sp, S, theta, device=0):
+    """sigma2 * matern32(dist(Sp, S)) on the device (np x n), codes/17_tlr_cholesky_pilot.py:270."""
+    torch = _torch()
+    dev = torch.device("cuda", device)
+    A = torch.as_tensor(np.asarray(Sp, dtype=np.float64), device=dev)
+    B = torch.as_tensor(np.asarray(S, dtype=np.float64), device=dev)
+    x = torch.cdist(A, B) * ((3.0 ** 0.5) / float(theta[1]))
+    return float(theta[0]) * (1.0 + x) * torch.exp(-x)
+
+
+def tlr_predict(S, y, Sp, theta, bounds, fac):
+    """Kriging mean and standard deviation at Sp with the TLR factor (drop-in for
+    codes/17_tlr_cholesky_pilot.py:269-276): alpha = L^-T L^-1 y, mu = Kp alpha, W = L^-1 Kp^T,
+    var = sigma2 (1 + eta) - colsum(W^2).  The solves run on the device through the C ABI."""
+    torch = _torch()
+    fac._check()
+    plan = fac.plan
+    Kp = _cross_cov(Sp, S, theta, plan.device)
+    yt = torch.as_tensor(np.asarray(y, dtype=np.float64), device=plan.dev)
+    alpha = fac.backward(fac.forward(yt))
+    mu = Kp @ alpha
+    W = fac.forward(Kp.t())
+    var = float(theta[0]) * (1.0 + float(theta[2])) - (W * W).sum(0)
+    return mu.cpu().numpy(), torch.sqrt(torch.clamp(var, min=1e-12)).cpu().numpy()
+
+
+def skill(yp, mu, sig):
+    """RMSE, CRPS of the Gaussian predictive and 90% coverage (codes/11_tlr_rank_rules.py:142-165)."""
+    from math import erf, pi, sqrt
+    yp, mu, sig = (np.asarray(v, dtype=np.float64) for v in (yp, mu, sig))
+    z = (yp - mu) / sig
+    pdf = np.exp(-0.5 * z ** 2) / sqrt(2 * pi)
+    cdf = 0.5 * (1 + np.vectorize(erf)(z / sqrt(2)))
+    crps = float((sig * (z * (2 * cdf - 1) + 2 * pdf - 1 / sqrt(pi))).mean())
+    return dict(rmse=float(np.sqrt(((yp - mu) ** 2).mean())), crps=crps, cover90=float((np.abs(z) <= 1.6448536).mean()))
 
 
 def neg_loglik_tlr(logth, S, y, bounds, rule, value, trace):

@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--plain-steps", type=int, default=2, help="timed steps of the plain FP64 comparison (0: skip)")
     ap.add_argument("--batch", type=int, default=4, help="parameter vectors per step (one batched call)")
     ap.add_argument("--dense", type=int, default=1, help="0: skip the dense FP64 oracle")
+    ap.add_argument("--sim", choices=["dense", "tlr"], default="dense",
+                    help="field from a dense Cholesky, or from a tau = 0.02 TLR factor (large N)")
     return ap.parse_args()
 
 
@@ -192,10 +194,14 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    S, y, _, _ = synth.simulate_field(a.n, THETA, device=local)
+    if a.sim == "dense":
+        S, y, _, _ = synth.simulate_field(a.n, THETA, device=local)
+        sim_info = None
+    else:  # N where no dense factor fits: the reference's --sim tlr protocol (17:326-339)
+        S, y, _, _, sim_info = synth.simulate_field_tlr(a.n, THETA, b=a.b, device=local)
     # dense FP64 oracle at the bench's theta (cuSOLVER through torch; not part of the timed path)
     dense, gdense = (synth.dense_loglik_grad_gpu(S, y, THETA, device=local) if rank == 0 and a.dense
-                     else (None, None))
+                     and a.sim == "dense" else (None, None))
     torch.cuda.empty_cache()
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -228,6 +234,7 @@ def main():
     thetas[0] = THETA
     pb = tlr.PlanBatch(a.n, a.b, B, cap=64, device=local, precision=a.precision)
     pb.set_data(S, y)
+    free_b, total_b = torch.cuda.mem_get_info(local)
     for _ in range(a.warmup):
         out = pb.evaluate(thetas, "adaptive", a.tau)
     for p in pb.plans:
@@ -253,6 +260,7 @@ def main():
                 acc[f] += v[f]
         p.set_profiling(False)
     ll0, g0, st0 = out[0]
+    info0 = pb.plans[0].evaluate(THETA, "adaptive", a.tau).info  # storage of the factor at theta_0
 
     # end to end through the public API: every step copies the sites and observations from pinned
     # host memory to the device, evaluates the batch and reads the results back
@@ -305,7 +313,15 @@ def main():
                 float(np.linalg.norm(g0 - np.array(plain["grad"])) / np.linalg.norm(plain["grad"])),
                 "e2e": {"value": world * a.steps * B / (ms_e2e / 1e3), "unit": "evals/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
-                "gpu_launches": launches, "roofline": roof, "kernels": kern, "clocks": clocks}
+                "gpu_launches": launches, "roofline": roof, "kernels": kern, "clocks": clocks,
+                "memory": {"device_used_gb_with_batch": (total_b - free_b) / 1e9, "device_gb": total_b / 1e9,
+                           "per_plan_gb_approx": (total_b - free_b) / 1e9 / B},
+                "storage": {"stored_factor": info0.get("stored_factor"),
+                            "fraction_of_dense_factor": None if info0.get("stored_factor") is None else
+                            info0["stored_factor"] / (a.n * (a.n + 1) / 2),
+                            "mean_rank_factor": info0.get("mean_rank_factor"),
+                            "max_rank_factor": info0.get("max_rank_factor")},
+                "simulation": sim_info}
         if world == 1 and a.cpu_sample:
             line["cpu_baseline"] = cpu_baseline(S, y, a)
         print(json.dumps(line), flush=True)

@@ -118,6 +118,18 @@ int tlr_loglik_grad_batch(tlr_plan* const* plans, int count, const double* theta
 int tlr_loglik_host(tlr_plan* plan, const double* xy_host, const double* y_host, const double theta[3], int rule,
                     double value, double* loglik, tlr_info* info, int* factor_ranks, int* sigma_ranks);
 
+/* Triangular solves with the factor left by the last successful evaluation of the plan, for m
+ * right-hand sides in place (x: device, n x m, column-major, ld n): trans 0 solves L X = B
+ * (replaces tlr_forward, codes/17_tlr_cholesky_pilot.py:230-240), trans 1 solves L^T X = Z
+ * (tlr_backward, 17:243-256).  Together they give Sigma_t^{-1} B for kriging (tlr_predict,
+ * 17:269-276).  TLR_ERR_NOT_READY when the plan holds no completed factorization. */
+int tlr_factor_solve(tlr_plan* plan, double* x_dev, int m, int trans);
+
+/* Y = L Z with the factor of the last successful evaluation (z, y: device, n x m, column-major,
+ * distinct): replaces tlr_matvec_L, codes/17_tlr_cholesky_pilot.py:218-227, with which the
+ * reference simulates fields too large for a dense factor (17:326-339). */
+int tlr_factor_matvec(tlr_plan* plan, const double* z_dev, double* y_dev, int m);
+
 /* Copy factor pieces to the host for checking: the dense lower factor of diagonal tile k
  * (bk x bk, column-major) or the (U, V) pair of off-diagonal tile (i, j), i > j (b_i x r and
  * b_j x r, column-major, r = *rank).  Valid after a successful tlr_loglik. */

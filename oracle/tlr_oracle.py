@@ -266,6 +266,27 @@ def tlr_backward(L_diag, L_off, bounds, Z):
     return X
 
 
+def tlr_predict(S, y, Sp, theta, bounds, fac):
+    """Kriging mean and standard deviation with the tile factor.  codes/17_tlr_cholesky_pilot.py:269-276."""
+    L_diag, L_off = fac
+    Kp = theta[0] * matern32(pairwise_dist(Sp, S), theta[1])
+    alpha = tlr_backward(L_diag, L_off, bounds, tlr_forward(L_diag, L_off, bounds, y[:, None]))[:, 0]
+    mu = Kp @ alpha
+    W = tlr_forward(L_diag, L_off, bounds, Kp.T)
+    var = theta[0] * (1 + theta[2]) - (W ** 2).sum(0)
+    return mu, np.sqrt(np.maximum(var, 1e-12))
+
+
+def skill(yp, mu, sig):
+    """RMSE, Gaussian CRPS and 90% coverage.  codes/11_tlr_rank_rules.py:142-146, 162-165."""
+    from scipy.special import erf
+    z = (yp - mu) / sig
+    pdf = np.exp(-0.5 * z ** 2) / np.sqrt(2 * np.pi)
+    cdf = 0.5 * (1 + erf(z / np.sqrt(2)))
+    crps = float((sig * (z * (2 * cdf - 1) + 2 * pdf - 1 / np.sqrt(np.pi))).mean())
+    return dict(rmse=float(np.sqrt(((yp - mu) ** 2).mean())), crps=crps, cover90=float((np.abs(z) <= 1.6448536).mean()))
+
+
 def tlr_loglik(S, y, theta, bounds, rule, value, rank_log=None, frozen=None):
     """(loglik | None, (L_diag, L_off) | None, info).
 

@@ -93,3 +93,27 @@ def test_dense_gradient_matches_finite_differences():
         tp[a] += h; tm[a] -= h
         fd = (O.loglik_dense(O.cov_dense(S, tp), y)[0] - O.loglik_dense(O.cov_dense(S, tm), y)[0]) / (2 * h)
         assert abs(fd - g[a]) <= 1e-5 * max(1.0, abs(g[a]))
+
+
+def test_oracle_prediction_matches_reference():
+    """The restated kriging, factor product, solves and skill scores reproduce the reference's own
+    outputs on the N = 1,030 field (fixture from tests/golden/make_golden_predict.py)."""
+    d = np.load(os.path.join(GOLD, "n1030_b100_data.npz"))
+    f = np.load(os.path.join(GOLD, "predict_n1030.npz"))
+    S, y = d["S"], d["y"]
+    theta = (1.0, 0.3, 0.05)
+    bounds = O.tile_bounds(len(y), 100)
+    ll, fac, _ = O.tlr_loglik(S, y, theta, bounds, "adaptive", 0.9)
+    assert abs(ll - float(f["loglik"])) <= 1e-10 * abs(ll)
+    mu, sd = O.tlr_predict(S, y, f["Sp"], theta, bounds, fac)
+    np.testing.assert_allclose(mu, f["mu"], rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(sd, f["sd"], rtol=1e-9)
+    np.testing.assert_allclose(O.tlr_matvec_L(fac[0], fac[1], bounds, f["z"][:, None])[:, 0], f["Lz"], rtol=1e-9,
+                               atol=1e-12)
+    fwd = O.tlr_forward(fac[0], fac[1], bounds, y[:, None])[:, 0]
+    np.testing.assert_allclose(fwd, f["fwd"], rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(O.tlr_backward(fac[0], fac[1], bounds, fwd[:, None])[:, 0], f["bwd"], rtol=1e-9,
+                               atol=1e-12)
+    sk = O.skill(f["yp"], f["mu"], f["sd"])
+    assert abs(sk["rmse"] - float(f["rmse"])) <= 1e-12 and abs(sk["crps"] - float(f["crps"])) <= 1e-12
+    assert sk["cover90"] == float(f["cover90"])
