@@ -163,6 +163,146 @@ __global__ void __launch_bounds__(256) k_sketch(const double* TLR_RESTRICT T, in
 }
 
 // ----------------------------------------------------------------------------------------
+// The same two products on the FP64 tensor cores (tiles up to 512 wide, even b).
+//   One CTA of 16 warps per (tile, 16-column group); warp w owns columns [32w, 32w + 32) of T.
+//   T streams through shared memory in slabs of 16 rows, double-buffered with cp.async (the
+//   next slab's copy runs under this slab's products).  Per slab R:
+//     phase A  Y_R = T_R P: each warp multiplies its 32-column strip by its 32 rows of P (held in
+//              registers for the whole kernel) -> a 16 x 16 partial; the 16 partials are summed
+//              in a fixed order (mode 1 writes that sum: the rows R of C = T P);
+//     phase B  Z[strip] += T_R[:, strip]^T Y_R, accumulated in registers across slabs.
+//   Every T element is read from HBM once per launch and used by both phases from shared memory.
+constexpr int kSkW = 16;                 // warps per CTA
+constexpr int kSkH = 16;                 // rows of T per slab
+constexpr int kSkCols = 32 * kSkW;       // widest tile handled (512)
+constexpr int kSkPitch = kSkCols + 4;    // slab row pitch in doubles (conflict-free fragments)
+constexpr int kSkYp = 18;                // pitch of the per-warp partials
+constexpr int kSkYs = 17;                // pitch of the summed Y_R
+
+static size_t sketch_mma_smem() {
+  return ((size_t)2 * kSkH * kSkPitch + (size_t)kSkW * kSkH * kSkYp + (size_t)kSkH * kSkYs) * sizeof(double);
+}
+
+__global__ void __launch_bounds__(kSkW * 32, 1)
+    k_sketch_mma(const double* TLR_RESTRICT T, int n, int b, int tile_base, const int* TLR_RESTRICT ti,
+                 const int* TLR_RESTRICT tj, const int* TLR_RESTRICT need, const double* TLR_RESTRICT P,
+                 double* TLR_RESTRICT out, int ldp, int omega, int mode, const int* TLR_RESTRICT status) {
+  if (*status != 0) return;
+  const int c = blockIdx.x, grp = blockIdx.y;
+  if (!need[c]) return;
+  const int t = tile_base + c;
+  const int bi = min(b, n - ti[t] * b), bj = min(b, n - tj[t] * b);
+  if (threadIdx.x == 0)
+    add_work(status, mode == 0 ? 2 : 4, (mode == 0 ? 4.0 : 2.0) * bi * bj * 16,
+             8.0 * ((double)bi * bj + (omega ? 0.0 : bj * 16.0) + (mode == 0 ? bj : bi) * 16.0));
+  extern __shared__ __align__(16) double sk_smem[];
+  double* Ts = sk_smem;                                   // [2][kSkH][kSkPitch]
+  double* Yp = Ts + (size_t)2 * kSkH * kSkPitch;          // [kSkW][kSkH][kSkYp]
+  double* Ys = Yp + (size_t)kSkW * kSkH * kSkYp;          // [kSkH][kSkYs]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, tg = lane & 3;
+  const double* Tc = T + (size_t)c * b * b;
+  const size_t pbase = (size_t)c * b * ldp;
+  const int col0 = warp * 32;
+  const int nslab = (bi + kSkH - 1) / kSkH;
+
+  // slab s -> stage s & 1: kSkH rows x kSkCols columns in 16-byte pieces, zero past bi / bj
+  auto issue = [&](int s) {
+    double* dst = Ts + (size_t)(s & 1) * kSkH * kSkPitch;
+    const int a0 = s * kSkH;
+    for (int e = tid; e < kSkH * (kSkCols / 2); e += kSkW * 32) {
+      const int r = e / (kSkCols / 2), col = 2 * (e % (kSkCols / 2));
+      const int row = a0 + r;
+      const int bytes = row < bi ? (col + 1 < bj ? 16 : (col < bj ? 8 : 0)) : 0;
+      cp_async16(dst + (size_t)r * kSkPitch + col, bytes ? Tc + (size_t)row * b + col : Tc, bytes);
+    }
+    cp_async_commit();
+  };
+  issue(0);
+
+  // B fragments of P for phase A: rows col0 + 4 kk + tg, columns 8 nt + g of the group
+  double pf[8][2];
+#pragma unroll
+  for (int kk = 0; kk < 8; ++kk)
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt) {
+      const int row = col0 + 4 * kk + tg, q = grp * 16 + 8 * nt + g;
+      pf[kk][nt] = row < bj ? (omega ? omega_entry((uint32_t)t, (uint32_t)row, (uint32_t)q)
+                                     : P[pbase + (size_t)q * b + row])
+                            : 0.0;
+    }
+  double za[4][2][2];
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt) za[m][nt][0] = za[m][nt][1] = 0.0;
+
+  for (int s = 0; s < nslab; ++s) {
+    cp_async_wait_all();
+    __syncthreads();  // slab s visible to all; every warp is done with slab s - 1
+    if (s + 1 < nslab) issue(s + 1);
+    const double* Tsl = Ts + (size_t)(s & 1) * kSkH * kSkPitch;
+    double ya[2][2][2];
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) ya[m][nt][0] = ya[m][nt][1] = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk)
+#pragma unroll
+      for (int m = 0; m < 2; ++m) {
+        const double a = Tsl[(size_t)(8 * m + g) * kSkPitch + col0 + 4 * kk + tg];
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) dmma884(ya[m][nt][0], ya[m][nt][1], a, pf[kk][nt]);
+      }
+    double* yp = Yp + (size_t)warp * kSkH * kSkYp;
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) yp[(8 * m + g) * kSkYp + 8 * nt + 2 * tg + h] = ya[m][nt][h];
+    __syncthreads();
+    if (tid < kSkH * 16) {
+      const int r = tid >> 4, q = tid & 15;
+      double sum = 0.0;
+#pragma unroll
+      for (int w = 0; w < kSkW; ++w) sum += Yp[(size_t)w * kSkH * kSkYp + r * kSkYp + q];
+      if (mode == 1) {
+        const int row = s * kSkH + r;
+        if (row < bi) out[pbase + (size_t)(grp * 16 + q) * b + row] = sum;
+      } else {
+        Ys[r * kSkYs + q] = sum;
+      }
+    }
+    if (mode == 1) continue;
+    __syncthreads();
+#pragma unroll
+    for (int kq = 0; kq < kSkH / 4; ++kq) {
+      double bf[2];
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) bf[nt] = Ys[(4 * kq + tg) * kSkYs + 8 * nt + g];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const double a = Tsl[(size_t)(4 * kq + tg) * kSkPitch + col0 + 8 * m + g];
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) dmma884(za[m][nt][0], za[m][nt][1], a, bf[nt]);
+      }
+    }
+  }
+  if (mode == 0) {
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      const int col = col0 + 8 * m + g;
+      if (col < bj)
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) out[pbase + (size_t)(grp * 16 + 8 * nt + 2 * tg + h) * b + col] = za[m][nt][h];
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------------------
 // P <- Q of the Householder QR of Z (bj x k); the panel is staged in shared memory.
 __global__ void __launch_bounds__(256) k_orth(double* TLR_RESTRICT Z, int n, int b, int k, int ldp,
                                              int tile_base, const int* TLR_RESTRICT tj,
@@ -349,7 +489,11 @@ int launch_sketch(const double* T, int n, int b, int k, int tile_base, const int
                   const int* need, const double* P, double* out, int ldp, int omega, int mode, int nchunk,
                   const int* status, cudaStream_t s) {
   dim3 grid((unsigned)nchunk, (unsigned)(k / 16));
-  if (b <= 512) {
+  if (b <= kSkCols && b % 2 == 0) {  // 16-byte aligned rows: the tensor-core form
+    const size_t sm = sketch_mma_smem();
+    cudaFuncSetAttribute(k_sketch_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_sketch_mma<<<grid, kSkW * 32, sm, s>>>(T, n, b, tile_base, ti, tj, need, P, out, ldp, omega, mode, status);
+  } else if (b <= 512) {
     const size_t sm = sketch_smem(b, 16);
     cudaFuncSetAttribute(k_sketch<16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_sketch<16, 2><<<grid, 256, sm, s>>>(T, n, b, k, tile_base, ti, tj, need, P, out, ldp, omega, mode, status);

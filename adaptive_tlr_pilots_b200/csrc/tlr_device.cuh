@@ -16,6 +16,24 @@ namespace tlr {
 
 constexpr double kSqrt3 = 1.7320508075688772935;
 
+// ---------------------------------------------------------------- FP64 tensor cores, async copies
+// D = A B + D on the FP64 tensor cores, one 8 x 8 x 4 step per warp (g = lane / 4, t = lane % 4):
+// a = A[g][t], b = B[t][g], d0 = D[g][2t], d1 = D[g][2t + 1].  Exact FP64 fused multiply-adds.
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// 16-byte global -> shared copy that completes asynchronously; bytes beyond src_bytes are zero.
+// Both addresses 16-byte aligned.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 // ---------------------------------------------------------------- reductions
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
