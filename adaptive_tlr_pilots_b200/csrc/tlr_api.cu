@@ -180,13 +180,19 @@ int run_compression(tlr_plan* p, double sigma2, double inv_range, int rule_fixed
         LAUNCH(TLR_K_ORTH, tlr::launch_orth(Zp, p->n, p->b, k, ldp, base, p->tj, p->need, p->gscr, nc, p->status, s));
         std::swap(Pp, Zp);
       }
-      LAUNCH(TLR_K_PROJECT, tlr::launch_sketch(p->T, p->n, p->b, k, base, p->ti, p->tj, p->need, Pp, p->C, ldp, 0, 1, nc, p->status,
-                              s));
-      LAUNCH(TLR_K_RESID, tlr::launch_resid(p->T, p->n, p->b, k, ldp, base, p->ti, p->tj, p->need, Pp, p->C, p->parts, p->fparts,
-                             p->nblk, nc, p->status, s));
+      const bool fused = tlr::project_resid_fused(p->b, k);  // residual inside the projection pass
+      if (fused) {
+        LAUNCH(TLR_K_PROJECT, tlr::launch_project_resid(p->T, p->n, p->b, base, p->ti, p->tj, p->need, Pp, p->C, ldp,
+                                                        p->parts, p->fparts, nc, p->status, s));
+      } else {
+        LAUNCH(TLR_K_PROJECT, tlr::launch_sketch(p->T, p->n, p->b, k, base, p->ti, p->tj, p->need, Pp, p->C, ldp, 0, 1, nc,
+                                                 p->status, s));
+        LAUNCH(TLR_K_RESID, tlr::launch_resid(p->T, p->n, p->b, k, ldp, base, p->ti, p->tj, p->need, Pp, p->C, p->parts,
+                                              p->fparts, p->nblk, nc, p->status, s));
+      }
       LAUNCH(TLR_K_FINALIZE, tlr::launch_finalize(p->n, p->b, k, ldp, p->cap, kMargin, rule_fixed, thr_rel, thr_abs, base, p->ti,
-                                p->tj, p->need, Pp, p->C, p->parts, p->fparts, p->nblk, p->gscr, p->gsv, p->U, p->V,
-                                p->rank, lev == kLevels - 1 ? 1 : 0, nc, p->status, s));
+                                p->tj, p->need, Pp, p->C, p->parts, p->fparts, fused ? 1 : p->nblk, p->gscr, p->gsv, p->U,
+                                p->V, p->rank, lev == kLevels - 1 ? 1 : 0, nc, p->status, s));
     }
   }
   return 0;

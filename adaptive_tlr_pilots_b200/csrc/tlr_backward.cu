@@ -28,70 +28,93 @@ namespace cg = cooperative_groups;
 namespace tlr {
 
 // ----------------------------------------------------------------------------------------
-// Batched FP64 GEMM  C = alpha op(A) op(B) + beta C, 64 x 64 output tiles, 256 threads, 4 x 4 outputs
-// per thread, K in slices of 16 through shared memory.  A job may scatter its output columns:
-// column n then goes to ccol[n] (leading rows contiguous) instead of C + n ldc.
-__global__ void __launch_bounds__(256) k_dgemm_batched(const GemmJob* TLR_RESTRICT jobs,
+// Batched FP64 GEMM  C = alpha op(A) op(B) + beta C on the FP64 tensor cores (mma m8n8k4, exact
+// FP64 fused multiply-adds).  64 x 64 output tiles, 256 threads: warp w owns rows 32 (w & 1) and
+// columns 16 (w >> 1) of the tile (4 x 2 fragments of 8 x 8).  K advances in slices of 16 through
+// shared memory, double-buffered: the next slice is loaded into registers while the tensor cores
+// work on the current one.  A job may scatter its output columns: column n then goes to ccol[n]
+// (leading rows contiguous) instead of C + n ldc.
+constexpr int kDgP = 72;  // slice row pitch in doubles (fragment reads hit every bank pair twice)
+
+__global__ void __launch_bounds__(256, 3) k_dgemm_batched(const GemmJob* TLR_RESTRICT jobs,
                                                       const int* TLR_RESTRICT status, int kind) {
   if (*status != 0) return;
   const GemmJob jb = jobs[blockIdx.z];
   const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
   if (m0 >= jb.M || n0 >= jb.N) return;
-  __shared__ double As[16][65];
-  __shared__ double Bs[16][65];
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  double acc[4][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-  for (int k0 = 0; k0 < jb.K; k0 += 16) {
-    __syncthreads();
+  __shared__ double As[2][16][kDgP];
+  __shared__ double Bs[2][16][kDgP];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
+  const int wm0 = (warp & 1) * 32, wn0 = (warp >> 1) * 16;
+  double ra[4], rb[4];
+  // slice k0 -> registers, coalesced along whichever index is contiguous in memory
+  auto load = [&](int k0) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int e = tid + 256 * q;
-      int kk, mm;
-      if (jb.transA) { kk = e & 15; mm = e >> 4; } else { kk = e >> 6; mm = e & 63; }
+      const int kk = jb.transA ? (e & 15) : (e >> 6), mm = jb.transA ? (e >> 4) : (e & 63);
       const int gm = m0 + mm, gk = k0 + kk;
-      double v = 0.0;
-      if (gm < jb.M && gk < jb.K)
-        v = jb.transA ? jb.A[(size_t)gm * jb.lda + gk] : jb.A[(size_t)gk * jb.lda + gm];
-      As[kk][mm] = v;
-      int kb, nn;
-      if (jb.transB) { kb = e >> 6; nn = e & 63; } else { kb = e & 15; nn = e >> 4; }
+      ra[q] = (gm < jb.M && gk < jb.K) ? (jb.transA ? jb.A[(size_t)gm * jb.lda + gk] : jb.A[(size_t)gk * jb.lda + gm])
+                                       : 0.0;
+      const int kb = jb.transB ? (e >> 6) : (e & 15), nn = jb.transB ? (e & 63) : (e >> 4);
       const int gn = n0 + nn, gkb = k0 + kb;
-      double w = 0.0;
-      if (gn < jb.N && gkb < jb.K)
-        w = jb.transB ? jb.B[(size_t)gkb * jb.ldb + gn] : jb.B[(size_t)gn * jb.ldb + gkb];
-      Bs[kb][nn] = w;
+      rb[q] = (gn < jb.N && gkb < jb.K) ? (jb.transB ? jb.B[(size_t)gkb * jb.ldb + gn] : jb.B[(size_t)gn * jb.ldb + gkb])
+                                        : 0.0;
     }
-    __syncthreads();
+  };
+  auto store = [&](int buf) {
 #pragma unroll
-    for (int kk = 0; kk < 16; ++kk) {
-      double a[4], bv[4];
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + 256 * q;
+      const int kk = jb.transA ? (e & 15) : (e >> 6), mm = jb.transA ? (e >> 4) : (e & 63);
+      As[buf][kk][mm] = ra[q];
+      const int kb = jb.transB ? (e >> 6) : (e & 15), nn = jb.transB ? (e & 63) : (e >> 4);
+      Bs[buf][kb][nn] = rb[q];
+    }
+  };
+  double acc[4][2][2];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bv[j] = Bs[kk][tx + 16 * j];
+    for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  if (jb.K > 0) {
+    load(0);
+    store(0);
+  }
+  __syncthreads();
+  for (int k0 = 0, buf = 0; k0 < jb.K; k0 += 16, buf ^= 1) {
+    const bool more = k0 + 16 < jb.K;
+    if (more) load(k0 + 16);
+#pragma unroll
+    for (int kq = 0; kq < 4; ++kq) {
+      double a[4], bv[2];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[buf][4 * kq + t][wm0 + 8 * i + g];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) bv[j] = Bs[buf][4 * kq + t][wn0 + 8 * j + g];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bv[j], acc[i][j]);
+        for (int j = 0; j < 2; ++j) dmma884(acc[i][j][0], acc[i][j][1], a[i], bv[j]);
     }
+    if (more) store(buf ^ 1);
+    __syncthreads();
   }
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int gn = n0 + tx + 16 * j;
-    if (gn >= jb.N) continue;
-    double* cc = jb.ccol ? jb.ccol[gn] : jb.C + (size_t)gn * jb.ldc;
+  for (int j = 0; j < 2; ++j)
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int gm = m0 + ty + 16 * i;
-      if (gm >= jb.M) continue;
-      const double v = jb.alpha * acc[i][j];
-      cc[gm] = (jb.beta == 0.0) ? v : fma(jb.beta, cc[gm], v);
+    for (int h = 0; h < 2; ++h) {
+      const int gn = n0 + wn0 + 8 * j + 2 * t + h;
+      if (gn >= jb.N) continue;
+      double* cc = jb.ccol ? jb.ccol[gn] : jb.C + (size_t)gn * jb.ldc;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int gm = m0 + wm0 + 8 * i + g;
+        if (gm >= jb.M) continue;
+        const double v = jb.alpha * acc[i][j][h];
+        cc[gm] = (jb.beta == 0.0) ? v : fma(jb.beta, cc[gm], v);
+      }
     }
-  }
   if (tid == 0) {
     const int mt = min(64, jb.M - m0), nt = min(64, jb.N - n0);
     add_work(status, kind, 2.0 * jb.K * mt * nt, 8.0 * ((double)mt * nt + (double)(mt + nt) * jb.K));

@@ -172,6 +172,11 @@ __global__ void __launch_bounds__(256) k_sketch(const double* TLR_RESTRICT T, in
 //              in a fixed order (mode 1 writes that sum: the rows R of C = T P);
 //     phase B  Z[strip] += T_R[:, strip]^T Y_R, accumulated in registers across slabs.
 //   Every T element is read from HBM once per launch and used by both phases from shared memory.
+//   MODE 0: the sketch Z = T^T T P.  MODE 1: the projection C = T P.  MODE 2 (one 16-column group,
+//   k = 16): the projection and, in place of phase B, the residual of the slab on the tensor cores,
+//   E_R = T_R - C_R P^T (accumulator started at T_R, operand -C_R), with rho^2 = sum E^2 and
+//   ||T||^2 summed per lane in a fixed order and over the CTA in warp order into parts[c],
+//   fparts[c] (one block per tile): T leaves HBM once for both.
 constexpr int kSkW = 16;                 // warps per CTA
 constexpr int kSkH = 16;                 // rows of T per slab
 constexpr int kSkCols = 32 * kSkW;       // widest tile handled (512)
@@ -183,18 +188,23 @@ static size_t sketch_mma_smem() {
   return ((size_t)2 * kSkH * kSkPitch + (size_t)kSkW * kSkH * kSkYp + (size_t)kSkH * kSkYs) * sizeof(double);
 }
 
+template <int MODE>
 __global__ void __launch_bounds__(kSkW * 32, 1)
     k_sketch_mma(const double* TLR_RESTRICT T, int n, int b, int tile_base, const int* TLR_RESTRICT ti,
                  const int* TLR_RESTRICT tj, const int* TLR_RESTRICT need, const double* TLR_RESTRICT P,
-                 double* TLR_RESTRICT out, int ldp, int omega, int mode, const int* TLR_RESTRICT status) {
+                 double* TLR_RESTRICT out, int ldp, int omega, double* TLR_RESTRICT parts,
+                 double* TLR_RESTRICT fparts, const int* TLR_RESTRICT status) {
+  constexpr int mode = MODE == 0 ? 0 : 1;
   if (*status != 0) return;
   const int c = blockIdx.x, grp = blockIdx.y;
   if (!need[c]) return;
   const int t = tile_base + c;
   const int bi = min(b, n - ti[t] * b), bj = min(b, n - tj[t] * b);
-  if (threadIdx.x == 0)
+  if (threadIdx.x == 0) {
     add_work(status, mode == 0 ? 2 : 4, (mode == 0 ? 4.0 : 2.0) * bi * bj * 16,
              8.0 * ((double)bi * bj + (omega ? 0.0 : bj * 16.0) + (mode == 0 ? bj : bi) * 16.0));
+    if (MODE == 2) add_work(status, 5, 2.0 * bi * bj * 17, 0.0);
+  }
   extern __shared__ __align__(16) double sk_smem[];
   double* Ts = sk_smem;                                   // [2][kSkH][kSkPitch]
   double* Yp = Ts + (size_t)2 * kSkH * kSkPitch;          // [kSkW][kSkH][kSkYp]
@@ -235,6 +245,18 @@ __global__ void __launch_bounds__(kSkW * 32, 1)
   for (int m = 0; m < 4; ++m)
 #pragma unroll
     for (int nt = 0; nt < 2; ++nt) za[m][nt][0] = za[m][nt][1] = 0.0;
+  // MODE 2: B fragments of P^T for the residual, P rows col0 + 8 j + g, columns 4 kq + tg
+  double pt[4][4];
+  double rho = 0.0, fro = 0.0;
+  if (MODE == 2) {
+#pragma unroll
+    for (int kq = 0; kq < 4; ++kq)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int row = col0 + 8 * j + g;
+        pt[kq][j] = row < bj ? P[pbase + (size_t)(4 * kq + tg) * b + row] : 0.0;
+      }
+  }
 
   for (int s = 0; s < nslab; ++s) {
     cp_async_wait_all();
@@ -270,12 +292,44 @@ __global__ void __launch_bounds__(kSkW * 32, 1)
       if (mode == 1) {
         const int row = s * kSkH + r;
         if (row < bi) out[pbase + (size_t)(grp * 16 + q) * b + row] = sum;
-      } else {
-        Ys[r * kSkYs + q] = sum;
       }
+      if (MODE != 1) Ys[r * kSkYs + q] = sum;
     }
-    if (mode == 1) continue;
+    if (MODE == 1) continue;
     __syncthreads();
+    if (MODE == 2) {
+      // E_R[:, strip] = T_R[:, strip] - C_R P[strip, :]^T
+      double e[2][4][2];
+#pragma unroll
+      for (int m = 0; m < 2; ++m)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) e[m][j][h] = Tsl[(size_t)(8 * m + g) * kSkPitch + col0 + 8 * j + 2 * tg + h];
+#pragma unroll
+      for (int kq = 0; kq < 4; ++kq)
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+          const double a = -Ys[(8 * m + g) * kSkYs + 4 * kq + tg];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) dmma884(e[m][j][0], e[m][j][1], a, pt[kq][j]);
+        }
+#pragma unroll
+      for (int m = 0; m < 2; ++m) {
+        const bool rin = s * kSkH + 8 * m + g < bi;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            if (rin && col0 + 8 * j + 2 * tg + h < bj) {
+              const double tv = Tsl[(size_t)(8 * m + g) * kSkPitch + col0 + 8 * j + 2 * tg + h];
+              rho = fma(e[m][j][h], e[m][j][h], rho);
+              fro = fma(tv, tv, fro);
+            }
+          }
+      }
+      continue;
+    }
 #pragma unroll
     for (int kq = 0; kq < kSkH / 4; ++kq) {
       double bf[2];
@@ -289,7 +343,26 @@ __global__ void __launch_bounds__(kSkW * 32, 1)
       }
     }
   }
-  if (mode == 0) {
+  if (MODE == 2) {
+    rho = warp_sum(rho);
+    fro = warp_sum(fro);
+    __syncthreads();
+    if (lane == 0) {
+      Yp[warp] = rho;
+      Yp[kSkW + warp] = fro;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double a = 0.0, f = 0.0;
+      for (int w = 0; w < kSkW; ++w) {
+        a += Yp[w];
+        f += Yp[kSkW + w];
+      }
+      parts[c] = a;
+      fparts[c] = f;
+    }
+  }
+  if (MODE == 0) {
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
       const int col = col0 + 8 * m + g;
@@ -491,8 +564,15 @@ int launch_sketch(const double* T, int n, int b, int k, int tile_base, const int
   dim3 grid((unsigned)nchunk, (unsigned)(k / 16));
   if (b <= kSkCols && b % 2 == 0) {  // 16-byte aligned rows: the tensor-core form
     const size_t sm = sketch_mma_smem();
-    cudaFuncSetAttribute(k_sketch_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_sketch_mma<<<grid, kSkW * 32, sm, s>>>(T, n, b, tile_base, ti, tj, need, P, out, ldp, omega, mode, status);
+    if (mode == 0) {
+      cudaFuncSetAttribute(k_sketch_mma<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      k_sketch_mma<0><<<grid, kSkW * 32, sm, s>>>(T, n, b, tile_base, ti, tj, need, P, out, ldp, omega, nullptr,
+                                                  nullptr, status);
+    } else {
+      cudaFuncSetAttribute(k_sketch_mma<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      k_sketch_mma<1><<<grid, kSkW * 32, sm, s>>>(T, n, b, tile_base, ti, tj, need, P, out, ldp, omega, nullptr,
+                                                  nullptr, status);
+    }
   } else if (b <= 512) {
     const size_t sm = sketch_smem(b, 16);
     cudaFuncSetAttribute(k_sketch<16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -502,6 +582,19 @@ int launch_sketch(const double* T, int n, int b, int k, int tile_base, const int
     cudaFuncSetAttribute(k_sketch<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_sketch<8, 4><<<grid, 256, sm, s>>>(T, n, b, k, tile_base, ti, tj, need, P, out, ldp, omega, mode, status);
   }
+  return (int)cudaGetLastError();
+}
+
+bool project_resid_fused(int b, int k) { return k == 16 && b <= kSkCols && b % 2 == 0; }
+
+int launch_project_resid(const double* T, int n, int b, int tile_base, const int* ti, const int* tj,
+                         const int* need, const double* P, double* C, int ldp, double* parts, double* fparts,
+                         int nchunk, const int* status, cudaStream_t s) {
+  if (!project_resid_fused(b, 16)) return (int)cudaErrorInvalidValue;
+  const size_t sm = sketch_mma_smem();
+  cudaFuncSetAttribute(k_sketch_mma<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_sketch_mma<2><<<dim3((unsigned)nchunk, 1), kSkW * 32, sm, s>>>(T, n, b, tile_base, ti, tj, need, P, C, ldp, 0,
+                                                                   parts, fparts, status);
   return (int)cudaGetLastError();
 }
 

@@ -20,6 +20,12 @@ int launch_sketch(const double* T, int n, int b, int k, int tile_base, const int
                   cudaStream_t s);
 int launch_orth(double* Z, int n, int b, int k, int ldp, int tile_base, const int* tj, const int* need,
                 double* gscratch, int nchunk, const int* status, cudaStream_t s);
+// k = 16 and b <= 512 even: projection C = T P and its residual in one pass (parts / fparts get
+// one block per tile)
+bool project_resid_fused(int b, int k);
+int launch_project_resid(const double* T, int n, int b, int tile_base, const int* ti, const int* tj,
+                         const int* need, const double* P, double* C, int ldp, double* parts, double* fparts,
+                         int nchunk, const int* status, cudaStream_t s);
 int launch_resid(const double* T, int n, int b, int k, int ldp, int tile_base, const int* ti, const int* tj,
                  const int* need, const double* P, const double* C, double* parts, double* fparts, int nblk,
                  int nchunk, const int* status, cudaStream_t s);
