@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(kSkW * 32, 1)
 
 // ----------------------------------------------------------------------------------------
 // P <- Q of the Householder QR of Z (bj x k); the panel is staged in shared memory.
-__global__ void __launch_bounds__(256) k_orth(double* TLR_RESTRICT Z, int n, int b, int k, int ldp,
+__global__ void __launch_bounds__(1024) k_orth(double* TLR_RESTRICT Z, int n, int b, int k, int ldp,
                                              int tile_base, const int* TLR_RESTRICT tj,
                                              const int* TLR_RESTRICT need, double* TLR_RESTRICT gscratch,
                                              int in_smem, const int* TLR_RESTRICT status) {
@@ -403,6 +403,155 @@ __global__ void __launch_bounds__(256) k_orth(double* TLR_RESTRICT Z, int n, int
   for (int e = threadIdx.x; e < bj * k; e += blockDim.x) {
     const int row = e % bj, q = e / bj;
     Z[pbase + (size_t)q * b + row] = (q < ke) ? W[(size_t)q * bj + row] : 0.0;
+  }
+}
+
+// ----------------------------------------------------------------------------------------
+// The same orthonormalisation for k = 16 and 32 (8 or 16 warps) and tiles up to 512 rows with the
+// panel in registers: warp w holds columns 2w and 2w + 1, lane l rows l + 32 i (i < 16).  Per column c the owning
+// warp forms the reflector (LAPACK dlarfg convention, as cta_geqr2) and publishes it to shared
+// memory; every warp applies it to its own later columns (one warp reduction per column), so a
+// column costs two block barriers and no shared-memory traffic for the panel itself.  Q is formed
+// backwards from the reflectors kept in the owners' registers (dorg2r order, as cta_org2r).
+constexpr int kOrCpw = 2;   // columns per warp
+constexpr int kOrRpl = 16;  // rows per lane (tiles up to 512 rows)
+
+// One column of k_orth_reg's QR: the reflector of column cc, held by this warp as its column
+// `sel` (lane l rows l + 32 i), in the dlarfg convention; v (unit at cc) to vs, tau to taus[cc],
+// beta on the diagonal.  The column is picked by value (sel ? a[1] : a[0]) so that the register
+// panel is never indexed at run time.
+__device__ __forceinline__ void orth_reflector(double (&a)[kOrCpw][kOrRpl], int sel, int cc, int bj, double* vs,
+                                               double* taus) {
+  const int lane = threadIdx.x & 31;
+  double s2 = 0.0, xa = 0.0;
+#pragma unroll
+  for (int i = 0; i < kOrRpl; ++i) {
+    const int row = lane + 32 * i;
+    const double x = sel ? a[1][i] : a[0][i];
+    if (row > cc && row < bj) s2 = fma(x, x, s2);
+    if (i == cc / 32) xa = x;
+  }
+  const double sig2 = warp_sum(s2);
+  const double alpha = __shfl_sync(0xffffffffu, xa, cc % 32);
+  double beta, tc, scale;
+  if (sig2 == 0.0) { tc = 0.0; beta = alpha; scale = 1.0; }
+  else {
+    beta = -copysign(sqrt(alpha * alpha + sig2), alpha);
+    tc = (beta - alpha) / beta;
+    scale = 1.0 / (alpha - beta);
+  }
+#pragma unroll
+  for (int i = 0; i < kOrRpl; ++i) {
+    const int row = lane + 32 * i;
+    const double x = sel ? a[1][i] : a[0][i];
+    double v = 0.0, y = x;
+    if (row > cc && row < bj) {
+      y = tc != 0.0 ? x * scale : x;
+      v = y;
+    } else if (row == cc) {
+      v = 1.0;
+      y = beta;
+    }
+    if (sel) a[1][i] = y; else a[0][i] = y;
+    vs[row] = v;
+  }
+  if (lane == 0) taus[cc] = tc;
+}
+
+// The reflector of column cc (kept below its diagonal in column `sel`) back to vs for Q.
+__device__ __forceinline__ void orth_publish(const double (&a)[kOrCpw][kOrRpl], int sel, int cc, int bj, double* vs) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int i = 0; i < kOrRpl; ++i) {
+    const int row = lane + 32 * i;
+    const double x = sel ? a[1][i] : a[0][i];
+    vs[row] = (row > cc && row < bj) ? x : (row == cc ? 1.0 : 0.0);
+  }
+}
+
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 16 / WARPS) k_orth_reg(double* TLR_RESTRICT Z, int n, int b, int ldp,
+                                                                   int tile_base, const int* TLR_RESTRICT tj,
+                                                                   const int* TLR_RESTRICT need,
+                                                                   const int* TLR_RESTRICT status) {
+  if (*status != 0) return;
+  const int c = blockIdx.x;
+  if (!need[c]) return;
+  constexpr int k = WARPS * kOrCpw;
+  const int bj = min(b, n - tj[(tile_base + c)] * b);
+  const int ke = min(k, bj);  // a tile narrower than k gets a full basis and zero columns
+  if (threadIdx.x == 0) add_work(status, 3, 4.0 * bj * ke * ke, 16.0 * bj * k);
+  __shared__ double vs[32 * kOrRpl];  // the current reflector, zero above its pivot
+  __shared__ double taus[k];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const size_t pbase = (size_t)c * b * ldp;
+  double a[kOrCpw][kOrRpl];
+#pragma unroll
+  for (int j = 0; j < kOrCpw; ++j) {
+    const int col = warp * kOrCpw + j;
+#pragma unroll
+    for (int i = 0; i < kOrRpl; ++i) {
+      const int row = lane + 32 * i;
+      a[j][i] = (col < ke && row < bj) ? Z[pbase + (size_t)col * b + row] : 0.0;
+    }
+  }
+  // ---- QR: reflectors below the diagonal of their columns, R on and above it
+  for (int cc = 0; cc < ke; ++cc) {
+    if (warp == cc / kOrCpw) {
+      orth_reflector(a, cc % kOrCpw, cc, bj, vs, taus);
+    }
+    __syncthreads();
+    const double tc = taus[cc];
+#pragma unroll
+    for (int j = 0; j < kOrCpw; ++j) {
+      const int col = warp * kOrCpw + j;
+      if (col > cc && col < ke) {
+        double w = 0.0;
+#pragma unroll
+        for (int i = 0; i < kOrRpl; ++i) w = fma(vs[lane + 32 * i], a[j][i], w);
+        w = warp_sum(w) * tc;
+#pragma unroll
+        for (int i = 0; i < kOrRpl; ++i) a[j][i] = fma(-w, vs[lane + 32 * i], a[j][i]);
+      }
+    }
+    __syncthreads();  // vs is rewritten for the next column
+  }
+  // ---- Q = H_0 ... H_{ke-1} [I; 0], backwards
+  for (int cc = ke - 1; cc >= 0; --cc) {
+    const double tc = taus[cc];
+    if (warp == cc / kOrCpw) {
+      orth_publish(a, cc % kOrCpw, cc, bj, vs);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kOrCpw; ++j) {
+      const int col = warp * kOrCpw + j;
+      if (col > cc && col < ke && tc != 0.0) {
+        double w = 0.0;
+#pragma unroll
+        for (int i = 0; i < kOrRpl; ++i) w = fma(vs[lane + 32 * i], a[j][i], w);
+        w = warp_sum(w) * tc;
+#pragma unroll
+        for (int i = 0; i < kOrRpl; ++i) a[j][i] = fma(-w, vs[lane + 32 * i], a[j][i]);
+      }
+      if (col == cc) {
+#pragma unroll
+        for (int i = 0; i < kOrRpl; ++i) {
+          const int row = lane + 32 * i;
+          a[j][i] = row < cc || row >= bj ? 0.0 : (row == cc ? 1.0 - tc : -tc * vs[row]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < kOrCpw; ++j) {
+    const int col = warp * kOrCpw + j;
+#pragma unroll
+    for (int i = 0; i < kOrRpl; ++i) {
+      const int row = lane + 32 * i;
+      if (row < bj) Z[pbase + (size_t)col * b + row] = col < ke ? a[j][i] : 0.0;
+    }
   }
 }
 
@@ -448,14 +597,28 @@ __global__ void __launch_bounds__(256) k_resid(const double* TLR_RESTRICT T, int
     }
     __syncthreads();
     if (col < qn) {
-      for (int r = rsub; r < hrows; r += 4) {
-        const double tv = Tc[(size_t)(a0 + r) * b + q0 + col];
-        double s = tv;
-        const double* cr = Cs + r * (k + 1);
-        const double* pr = Pb + col * (k + 1);
-        for (int q = 0; q < k; ++q) s = fma(-cr[q], pr[q], s);
-        acc = fma(s, s, acc);
-        facc = fma(tv, tv, facc);
+      // rows rsub, rsub + 4, rsub + 8, rsub + 12 of the strip as four independent chains (each
+      // element is still T - sum_q C P in q order; rows past the strip contribute nothing)
+      double tv[4], sv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int r = rsub + 4 * u;
+        tv[u] = r < hrows ? Tc[(size_t)(a0 + r) * b + q0 + col] : 0.0;
+        sv[u] = tv[u];
+      }
+      const double* pr = Pb + col * (k + 1);
+#pragma unroll 4
+      for (int q = 0; q < k; ++q) {
+        const double pq = pr[q];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) sv[u] = fma(-Cs[(rsub + 4 * u) * (k + 1) + q], pq, sv[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (rsub + 4 * u < hrows) {
+          acc = fma(sv[u], sv[u], acc);
+          facc = fma(tv[u], tv[u], facc);
+        }
       }
     }
   }
@@ -466,7 +629,7 @@ __global__ void __launch_bounds__(256) k_resid(const double* TLR_RESTRICT T, int
 
 // ----------------------------------------------------------------------------------------
 // Rank decision and output of the truncated pair for every tile still in need.
-__global__ void __launch_bounds__(256) k_finalize(int n, int b, int k, int ldp, int cap, int margin,
+__global__ void __launch_bounds__(1024) k_finalize(int n, int b, int k, int ldp, int cap, int margin,
                                                  int rule_fixed, double thr_rel, double thr_abs,
                                                  int tile_base, const int* TLR_RESTRICT ti,
                                                  const int* TLR_RESTRICT tj, int* TLR_RESTRICT need,
@@ -476,7 +639,7 @@ __global__ void __launch_bounds__(256) k_finalize(int n, int b, int k, int ldp, 
                                                  double* TLR_RESTRICT gscratch, double* TLR_RESTRICT gsv,
                                                  double* TLR_RESTRICT Uo,
                                                  double* TLR_RESTRICT Vo, int* TLR_RESTRICT rank,
-                                                 int last_level, int* TLR_RESTRICT status) {
+                                                 int last_level, int w_in_smem, int* TLR_RESTRICT status) {
   if (*status != 0) return;
   const int c = blockIdx.x;
   if (!need[c]) return;
@@ -493,15 +656,17 @@ __global__ void __launch_bounds__(256) k_finalize(int n, int b, int k, int ldp, 
   double* M = (k <= 64) ? smem + 40 + 136 * 3 + 8 : gsv + (size_t)c * 2 * k * k;  // k x k
   double* Vw = M + k * k;                                                             // k x k
   const size_t pbase = (size_t)c * b * ldp;
-  double* W = gscratch + pbase;  // bi x k copy of C (ld b)
+  // bi x k copy of C for the QR: in shared memory (ld bi) when it fits, else global scratch (ld b)
+  double* W = w_in_smem ? smem + 40 + 136 * 3 + 8 + 2 * (size_t)k * k : gscratch + pbase;
+  const int ldw = w_in_smem ? bi : b;
   for (int e = threadIdx.x; e < bi * k; e += blockDim.x) {
     const int row = e % bi, q = e / bi;
-    W[(size_t)q * b + row] = C[pbase + (size_t)q * b + row];
+    W[(size_t)q * ldw + row] = C[pbase + (size_t)q * b + row];
   }
   __syncthreads();
   const int kk = min(k, bi);
-  cta_geqr2(W, b, bi, k, tau, red);
-  cta_copy_r(W, b, bi, k, M, k);
+  cta_geqr2(W, ldw, bi, k, tau, red);
+  cta_copy_r(W, ldw, bi, k, M, k);
   cta_jacobi_svd(M, k, k, k, Vw, k, sig, perm, iflag);
   if (threadIdx.x == 0) {
     double rho2 = 0.0, fro2 = 0.0;
@@ -600,11 +765,21 @@ int launch_project_resid(const double* T, int n, int b, int tile_base, const int
 
 int launch_orth(double* Z, int n, int b, int k, int ldp, int tile_base, const int* tj, const int* need,
                 double* gscratch, int nchunk, const int* status, cudaStream_t s) {
+  if (k == 16 && b <= 32 * kOrRpl) {  // panel in registers
+    k_orth_reg<8><<<nchunk, 256, 0, s>>>(Z, n, b, ldp, tile_base, tj, need, status);
+    return (int)cudaGetLastError();
+  }
+  if (k == 32 && b <= 32 * kOrRpl) {
+    k_orth_reg<16><<<nchunk, 512, 0, s>>>(Z, n, b, ldp, tile_base, tj, need, status);
+    return (int)cudaGetLastError();
+  }
   size_t sm = (40 + 136) * 8;
   const int in_smem = (size_t)b * k * 8 <= 160 * 1024;
   if (in_smem) sm += (size_t)b * k * 8;
   cudaFuncSetAttribute(k_orth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_orth<<<nchunk, 256, sm, s>>>(Z, n, b, k, ldp, tile_base, tj, need, gscratch, in_smem, status);
+  // the wide levels hold few tiles, each a long chain of column steps: four times the warps per
+  // step there
+  k_orth<<<nchunk, k >= 32 ? 1024 : 256, sm, s>>>(Z, n, b, k, ldp, tile_base, tj, need, gscratch, in_smem, status);
   return (int)cudaGetLastError();
 }
 
@@ -623,10 +798,13 @@ int launch_finalize(int n, int b, int k, int ldp, int cap, int margin, int rule_
                     const double* C, const double* parts, const double* fparts, int nblk, double* gscratch,
                     double* gsv, double* U, double* V, int* rank, int last_level, int nchunk, int* status,
                     cudaStream_t s) {
-  const size_t sm = (40 + 136 * 3 + 8 + (k <= 64 ? 2 * (size_t)k * k : 0)) * 8;
+  size_t sm = (40 + 136 * 3 + 8 + (k <= 64 ? 2 * (size_t)k * k : 0)) * 8;
+  const int w_in_smem = k <= 64 && (size_t)b * k * 8 <= 160 * 1024;
+  if (w_in_smem) sm += (size_t)b * k * 8;
   cudaFuncSetAttribute(k_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_finalize<<<nchunk, 256, sm, s>>>(n, b, k, ldp, cap, margin, rule_fixed, thr_rel, thr_abs, tile_base, ti, tj, need,
-                                     P, C, parts, fparts, nblk, gscratch, gsv, U, V, rank, last_level, status);
+  k_finalize<<<nchunk, k >= 32 ? 1024 : 256, sm, s>>>(n, b, k, ldp, cap, margin, rule_fixed, thr_rel, thr_abs, tile_base, ti, tj, need,
+                                     P, C, parts, fparts, nblk, gscratch, gsv, U, V, rank, last_level, w_in_smem,
+                                     status);
   return (int)cudaGetLastError();
 }
 
