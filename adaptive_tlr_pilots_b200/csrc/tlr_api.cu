@@ -83,6 +83,7 @@ struct tlr_plan {
   int precision = TLR_PRECISION_FP64;
   // launch accounting and optional per-kernel event timing
   bool prof = false;
+  int prof_kind = -1;  // -1: every kind
   std::vector<cudaEvent_t> ev_pool;
   size_t ev_used = 0;
   std::vector<int> ev_kind;
@@ -149,12 +150,13 @@ cudaEvent_t next_event(tlr_plan* p) {
 // launch one kernel of kind `kind` on stream `st`; with profiling on, bracket it by two events
 #define LAUNCH_ON(st, kind, x)                                                      \
   do {                                                                              \
-    if (p->prof) {                                                                  \
+    const bool _ev = p->prof && (p->prof_kind < 0 || p->prof_kind == (kind));      \
+    if (_ev) {                                                                      \
       cudaEventRecord(next_event(p), st);                                           \
       p->ev_kind.push_back(kind);                                                   \
     }                                                                               \
     const int _rc = (x);                                                            \
-    if (p->prof) cudaEventRecord(next_event(p), st);                                \
+    if (_ev) cudaEventRecord(next_event(p), st);                                    \
     p->klaunch[kind] += 1;                                                          \
     if (_rc != 0) return fail(TLR_ERR_CUDA, std::string("kernel launch failed: ") + \
                                                 cudaGetErrorString((cudaError_t)_rc)); \
@@ -852,6 +854,7 @@ int tlr_plan_set_precision(tlr_plan* p, int mode) {
 int tlr_plan_set_profiling(tlr_plan* p, int on) {
   if (!p) return fail(TLR_ERR_ARG, "plan is NULL");
   p->prof = on != 0;
+  p->prof_kind = on < 0 ? -on - 1 : -1;  // on < 0: only the launches of kind -on - 1
   return 0;
 }
 

@@ -165,9 +165,11 @@ class Plan:
         _lib.check(self.lib.tlr_plan_set_precision(self.handle, _lib.PRECISIONS[mode]))
         self.precision = mode
 
-    def set_profiling(self, on=True):
-        """Bracket every launch with CUDA events (per-kernel device time; results unchanged)."""
-        _lib.check(self.lib.tlr_plan_set_profiling(self.handle, 1 if on else 0))
+    def set_profiling(self, on=True, kind=None):
+        """Bracket every launch with CUDA events (per-kernel device time; results unchanged), or
+        only the launches of one kernel kind (a key of kernel_stats) when `kind` is given."""
+        code = (-(_lib.KERNEL_KINDS.index(kind) + 1) if kind is not None else 1) if on else 0
+        _lib.check(self.lib.tlr_plan_set_profiling(self.handle, code))
 
     def kernel_stats(self, reset=False):
         """{kernel kind: dict(ms, launches, flops, bytes)} accumulated since the last reset

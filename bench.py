@@ -237,9 +237,22 @@ def main():
     free_b, total_b = torch.cuda.mem_get_info(local)
     for _ in range(a.warmup):
         out = pb.evaluate(thetas, "adaptive", a.tau)
+    # one untimed step with every launch bracketed by events: the per-kernel table and the
+    # dominant kernel; the timed steps then bracket only that kernel's launches (its roofline)
     for p in pb.plans:
         p.set_profiling(True)
         p.kernel_stats(reset=True)
+    out = pb.evaluate(thetas, "adaptive", a.tau)
+    torch.cuda.synchronize()
+    prof_stats = {}
+    for p in pb.plans:
+        for k, v in p.kernel_stats(reset=True).items():
+            acc = prof_stats.setdefault(k, dict(ms=0.0, launches=0, flops=0.0, bytes=0.0))
+            for f in acc:
+                acc[f] += v[f]
+    top = max(prof_stats, key=lambda k: prof_stats[k]["ms"])
+    for p in pb.plans:
+        p.set_profiling(True, kind=top)
     sampler = ClockSampler(local)
     sampler.start()
     barrier()
@@ -282,7 +295,6 @@ def main():
     if rank == 0:
         pk, pk_kind = peaks()
         launches = int(sum(v["launches"] for v in stats.values()))
-        top = max(stats, key=lambda k: stats[k]["ms"])
         st = stats[top]
         per_launch_ms = st["ms"] / max(st["launches"], 1)
         achieved_gbs = st["bytes"] / max(st["launches"], 1) / (per_launch_ms * 1e-3) / 1e9
@@ -290,11 +302,12 @@ def main():
                 "frac": achieved_gbs / pk["hbm_gbs"], "traffic": None, "peak_kind": pk_kind,
                 "fp64_tflops": st["flops"] / max(st["launches"], 1) / (per_launch_ms * 1e-3) / 1e12,
                 "fp64_peak_nominal_tflops": 37.0,
-                "share": st["ms"] / sum(v["ms"] for v in stats.values()),
+                "share": prof_stats[top]["ms"] / sum(v["ms"] for v in prof_stats.values()),
                 "per_launch_ms": per_launch_ms, "launches_per_step": st["launches"] / a.steps}
-        kern = {k: {"ms_per_step": v["ms"] / a.steps, "launches_per_step": v["launches"] / a.steps,
-                    "gflop_per_step": v["flops"] / a.steps / 1e9, "gb_per_step": v["bytes"] / a.steps / 1e9}
-                for k, v in stats.items() if v["launches"]}
+        # per-kernel table of the profiled step (event intervals of concurrent plans overlap)
+        kern = {k: {"ms_per_step": v["ms"], "launches_per_step": v["launches"],
+                    "gflop_per_step": v["flops"] / 1e9, "gb_per_step": v["bytes"] / 1e9}
+                for k, v in prof_stats.items() if v["launches"]}
         value = world * a.steps * B / (ms_max / 1e3)
         line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True,

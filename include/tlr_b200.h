@@ -167,7 +167,8 @@ int tlr_plan_set_precision(tlr_plan* plan, int mode);
 #define TLR_NKINDS 18
 
 /* Profiling: when on, every launch is bracketed by CUDA events on the plan's stream and the
- * per-kind device time is accumulated (no effect on results).  No reference counterpart. */
+ * per-kind device time is accumulated (no effect on results); on < 0 brackets only the launches
+ * of kernel kind -on - 1 (the order of tlr_plan_kernel_stats).  No reference counterpart. */
 int tlr_plan_set_profiling(tlr_plan* plan, int on);
 /* Per-kind accumulated device milliseconds (profiling on), launch counts and algorithmic work
  * (FP64 flops and HBM bytes the kernels count for themselves) since the last reset.  Any output
