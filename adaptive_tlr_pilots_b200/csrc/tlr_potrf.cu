@@ -11,8 +11,9 @@
 //   the panel rows below are split across the cluster, four threads per row: X = A21 L11^{-T} as
 //   independent dot products (no substitution chain), and rhs_rows -= X z_p with
 //   z_p = L11^{-1} rhs_p (the fused forward solve);
-//   cluster barrier; the lower-triangular 32 x 32 blocks of the trailing matrix are split across
-//   the cluster (A22 -= X X^T); cluster barrier.
+//   cluster barrier; every CTA stages the whole panel X in shared memory once, and the
+//   lower-triangular 32 x 32 blocks of the trailing matrix are split across the cluster
+//   (A22 -= X X^T, no block barrier between blocks); cluster barrier.
 // Several tiles (one per parameter vector of a batch) are factored by independent clusters of
 // one launch.  The status word is read once by rank 0 and shared through distributed shared
 // memory, so every CTA of a cluster takes the same branch even when another stream writes the
@@ -46,8 +47,7 @@ __global__ void __cluster_dims__(kPC, 1, 1) __launch_bounds__(256)
   __shared__ double Li[kPB][kPB + 1];  // L11^{-1}
   __shared__ double dinv[kPB];
   __shared__ double zp[kPB];
-  __shared__ double Pa[kPB][kPB + 1];
-  __shared__ double Pc[kPB][kPB + 1];
+  extern __shared__ double Ps[];  // the panel below the diagonal block, b x (kPB + 1)
   __shared__ int go, fail;
   __shared__ double logdet_acc, quad_acc;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -178,7 +178,13 @@ __global__ void __cluster_dims__(kPC, 1, 1) __launch_bounds__(256)
         quad_acc = q;
       }
     }
-    // trailing update of the lower triangle in 32 x 32 blocks
+    // trailing update of the lower triangle in 32 x 32 blocks, from the whole panel staged once in
+    // shared memory (rows below the diagonal block, ld kPB + 1)
+    for (int e = tid; e < m * kPB; e += blockDim.x) {
+      const int row = e % m, t = e / m;
+      Ps[(size_t)row * (kPB + 1) + t] = t < pw ? A[(size_t)(p0 + t) * b + p0 + pw + row] : 0.0;
+    }
+    __syncthreads();
     const int mb = (m + 31) / 32;
     const int nblk = mb * (mb + 1) / 2;
     for (int blk = g; blk < nblk; blk += G) {
@@ -187,28 +193,28 @@ __global__ void __cluster_dims__(kPC, 1, 1) __launch_bounds__(256)
       while ((rb + 1) * (rb + 2) / 2 <= blk) ++rb;
       const int cb = blk - rb * (rb + 1) / 2;
       const int a0 = rb * 32, c0 = cb * 32;
-      __syncthreads();
-      for (int t = warp; t < kPB; t += 8) {
-        const double* col = A + (size_t)(p0 + t) * b + p0 + pw;
-        Pa[lane][t] = (t < pw && a0 + lane < m) ? col[a0 + lane] : 0.0;
-        Pc[lane][t] = (t < pw && c0 + lane < m) ? col[c0 + lane] : 0.0;
-      }
-      __syncthreads();
       const int cl = tid & 31, rl = tid >> 5;  // column cl, rows rl + 8q
+      const int cg2 = c0 + cl;
+      double* colp = A + (size_t)(p0 + pw + min(cg2, m - 1)) * b + p0 + pw;
+      double old[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {  // the block's current values, loaded before the products
+        const int ag = a0 + rl + 8 * q;
+        old[q] = (cg2 < m && ag < m && ag >= cg2) ? colp[ag] : 0.0;
+      }
+      const double* pcr = Ps + (size_t)min(cg2, m - 1) * (kPB + 1);
       double acc[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll 8
       for (int t = 0; t < kPB; ++t) {
-        const double pc = Pc[cl][t];
+        const double pc = pcr[t];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) acc[q] = fma(Pa[rl + 8 * q][t], pc, acc[q]);
+        for (int q = 0; q < 4; ++q) acc[q] = fma(Ps[(size_t)min(a0 + rl + 8 * q, m - 1) * (kPB + 1) + t], pc, acc[q]);
       }
-      const int cg2 = c0 + cl;
       if (cg2 < m) {
-        double* colp = A + (size_t)(p0 + pw + cg2) * b + p0 + pw;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const int ag = a0 + rl + 8 * q;
-          if (ag < m && ag >= cg2) colp[ag] -= acc[q];
+          if (ag < m && ag >= cg2) colp[ag] = old[q] - acc[q];
         }
       }
     }
@@ -227,7 +233,9 @@ int launch_potrf(double* D, int n, int b, int k, double* rhs, double* z, double*
 
 int launch_potrf_batched(double* D, int n, int b, int k, double* rhs, double* z, double* ldpart, double* qpart,
                          int* status, int nbatch, size_t sD, size_t sV, int sS, cudaStream_t s) {
-  k_potrf_cluster<<<kPC * nbatch, 256, 0, s>>>(D, n, b, k, rhs, z, ldpart, qpart, status, sD, sV, sS);
+  const size_t sm = (size_t)b * (kPB + 1) * sizeof(double);
+  cudaFuncSetAttribute(k_potrf_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_potrf_cluster<<<kPC * nbatch, 256, sm, s>>>(D, n, b, k, rhs, z, ldpart, qpart, status, sD, sV, sS);
   return (int)cudaGetLastError();
 }
 
