@@ -168,11 +168,23 @@ __global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int 
         double l[32];
 #pragma unroll
         for (int c = 0; c < 32; ++c) l[c] = (c < pw) ? L[(size_t)(p0 + c) * b + row] : 0.0;
-        for (int q = 0; q < rq; ++q) {
-          double s = 0.0;
+        // eight columns of V at a time: their current values are loaded together, then the dots
+        for (int q1 = 0; q1 < rq; q1 += 8) {
+          double old[8], sv[8];
 #pragma unroll
-          for (int c = 0; c < 32; ++c) s = fma(l[c], Xp[c][q], s);
-          Vt[(size_t)(q0 + q) * b + row] -= s;
+          for (int u = 0; u < 8; ++u) {
+            old[u] = q1 + u < rq ? Vt[(size_t)(q0 + q1 + u) * b + row] : 0.0;
+            sv[u] = 0.0;
+          }
+#pragma unroll
+          for (int c = 0; c < 32; ++c) {
+            const double lc = l[c];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) sv[u] = fma(lc, Xp[c][min(q1 + u, 63)], sv[u]);
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            if (q1 + u < rq) Vt[(size_t)(q0 + q1 + u) * b + row] = old[u] - sv[u];
         }
       }
     }
@@ -205,10 +217,18 @@ __global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int 
   // Y_ik = U_ik W_ik, the factor of the deferred diagonal update of tile i
   double* Yt = Y + (size_t)t * b * cap;
   for (int a = tid; a < bi; a += 256)
-    for (int q = 0; q < r; ++q) {
-      double s = 0.0;
-      for (int p = 0; p < r; ++p) s = fma(Ut[(size_t)p * b + a], W[(size_t)q * cap + p], s);
-      Yt[(size_t)q * b + a] = s;
+    for (int q1 = 0; q1 < r; q1 += 8) {  // eight output columns per pass over the row of U
+      double sv[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) sv[u] = 0.0;
+      for (int p = 0; p < r; ++p) {
+        const double up = Ut[(size_t)p * b + a];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) sv[u] = fma(up, W[(size_t)min(q1 + u, r - 1) * cap + p], sv[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (q1 + u < r) Yt[(size_t)(q1 + u) * b + a] = sv[u];
     }
   double* ri = rhs + (size_t)i * b;
   if (r <= 64) {

@@ -74,6 +74,7 @@ __global__ void __cluster_dims__(kPC, 1, 1) __launch_bounds__(256)
       for (int j = 0; j < kPB; ++j)
         row[j] = (lane < pw && j <= lane) ? A[(size_t)(p0 + j) * b + p0 + lane] : 0.0;
       int bad = 0;
+      double dl = 0.0;  // 1 / L11[lane][lane]
 #pragma unroll
       for (int c = 0; c < kPB; ++c) {
         if (c < pw && !bad) {
@@ -81,8 +82,13 @@ __global__ void __cluster_dims__(kPC, 1, 1) __launch_bounds__(256)
           if (!(d > 0.0)) {
             bad = 1;  // the same pivot in every lane: the whole warp stops here
           } else {
-            const double sd = sqrt(d), rsd = 1.0 / sd;
-            if (lane == c) row[c] = sd;
+            // one reciprocal square root per pivot on the column chain (sqrt d = d / sqrt d);
+            // an IEEE square root followed by a division costs several times as long here
+            const double rsd = rsqrt(d), sd = d * rsd;
+            if (lane == c) {
+              row[c] = sd;
+              dl = rsd;
+            }
             if (lane > c) row[c] *= rsd;
 #pragma unroll
             for (int j = c + 1; j < kPB; ++j) {
@@ -96,7 +102,7 @@ __global__ void __cluster_dims__(kPC, 1, 1) __launch_bounds__(256)
       for (int j = 0; j < kPB; ++j) L11[lane][j] = (j <= lane && lane < pw && j < pw) ? row[j] : 0.0;
       if (lane == 0) fail = bad;
       __syncwarp();
-      dinv[lane] = (!bad && lane < pw) ? 1.0 / L11[lane][lane] : 0.0;
+      dinv[lane] = (!bad && lane < pw) ? dl : 0.0;
       __syncwarp();
       if (!bad) {
         // column `lane` of L11^{-1} by forward substitution
