@@ -12,7 +12,8 @@
 // apart, the two 16-byte K halves of one MMA 2048 B apart for A), fences the generic-proxy writes
 // for the async proxy, and thread 0 issues 4 K-steps x 3 tcgen05.mma.kind::tf32 and commits them
 // to the stage's mbarrier.  Two stages alternate, so the conversion of slice s+1 overlaps the MMAs
-// of slice s.  Waits on the mbarriers are bounded: on timeout the kernel sets an error status,
+// of slice s, and the global loads of slice s+1 are issued (into a second register set) before
+// slice s is converted, so their latency overlaps that work.  Waits on the mbarriers are bounded: on timeout the kernel sets an error status,
 // frees its tensor memory and returns.
 #include <stdint.h>
 
@@ -116,41 +117,40 @@ __global__ void __launch_bounds__(256) k_gemm_tc3(const GemmJob* TLR_RESTRICT jo
   const uint32_t idesc = umma_idesc_tf32(kTcM, kTcN);
   const int nk = (jb.K + kTcBK - 1) / kTcBK;
   int fail = 0;
-  for (int it = 0; it < nk; ++it) {
+  // global -> registers for slice `it`: thread -> (row r = tid / 2, K groups (tid & 1) * 4 .. + 3
+  // of 4 consecutive k each), all 16 loads of A and of B issued before any of them is used
+  auto gload = [&](int it, double (&va)[16], double (&vb)[16]) {
+    const int k0 = it * kTcBK;
+    const int r = tid >> 1, gh = (tid & 1) * 4;
+    const int gma = m0 + r, gnb = n0 + r;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int gk = k0 + gh * 4 + q;
+      va[q] = (gma < jb.M && gk < jb.K)
+                  ? (jb.transA ? jb.A[(size_t)gma * jb.lda + gk] : jb.A[(size_t)gk * jb.lda + gma])
+                  : 0.0;
+      vb[q] = (gnb < jb.N && gk < jb.K)
+                  ? (jb.transB ? jb.B[(size_t)gk * jb.ldb + gnb] : jb.B[(size_t)gnb * jb.ldb + gk])
+                  : 0.0;
+    }
+  };
+  // registers of slice `it` -> its shared-memory stage (split TF32, each group of 4 as one 16-byte
+  // store), then thread 0 issues the slice's MMAs; false (in every thread) on a timed-out wait
+  auto stage_in = [&](int it, const double (&va)[16], const double (&vb)[16]) -> bool {
     const int st = it & 1;
     unsigned char* sbase = tc_smem + st * kTcStageBytes;
     float* Ahi = reinterpret_cast<float*>(sbase);
     float* Alo = Ahi + kTcM * kTcBK;
     float* Bhi = Alo + kTcM * kTcBK;
     float* Blo = Bhi + kTcN * kTcBK;
+    int bad = 0;
     if (it >= kTcStages) {
       // the MMAs that read this stage two slices ago must be done before it is overwritten
-      if (!mbar_wait(smem_u32(&mbar[st]), (uint32_t)(((it - kTcStages) >> 1) & 1))) {
-        fail = 1;
-      }
+      if (!mbar_wait(smem_u32(&mbar[st]), (uint32_t)(((it - kTcStages) >> 1) & 1))) bad = 1;
     }
-    if (__syncthreads_or(fail)) {
-      fail = 1;
-      break;
-    }
-    const int k0 = it * kTcBK;
-    // thread -> (row r = tid / 2, K groups (tid & 1) * 4 .. + 3 of 4 consecutive k each): all 16
-    // loads of A and of B are issued before any of them is used, then each group of 4 goes to
-    // shared memory as one 16-byte store (hi and lo)
+    if (__syncthreads_or(bad)) return false;
     {
       const int r = tid >> 1, gh = (tid & 1) * 4;
-      double va[16], vb[16];
-      const int gma = m0 + r, gnb = n0 + r;
-#pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const int gk = k0 + gh * 4 + q;
-        va[q] = (gma < jb.M && gk < jb.K)
-                    ? (jb.transA ? jb.A[(size_t)gma * jb.lda + gk] : jb.A[(size_t)gk * jb.lda + gma])
-                    : 0.0;
-        vb[q] = (gnb < jb.N && gk < jb.K)
-                    ? (jb.transB ? jb.B[(size_t)gk * jb.ldb + gnb] : jb.B[(size_t)gnb * jb.ldb + gk])
-                    : 0.0;
-      }
 #pragma unroll
       for (int g = 0; g < 4; ++g) {
         float4 ah, al, bh, bl;
@@ -188,6 +188,23 @@ __global__ void __launch_bounds__(256) k_gemm_tc3(const GemmJob* TLR_RESTRICT jo
         mma_tf32(tmem_d, dAl, dBh, idesc, 1u);
       }
       mma_commit(smem_u32(&mbar[st]));
+    }
+    return true;
+  };
+  // two register sets: the loads of slice it + 1 are in flight while slice it is converted
+  double a0[16], b0[16], a1[16], b1[16];
+  if (nk > 0) gload(0, a0, b0);
+  for (int it = 0; it < nk; it += 2) {
+    if (it + 1 < nk) gload(it + 1, a1, b1);
+    if (!stage_in(it, a0, b0)) {
+      fail = 1;
+      break;
+    }
+    if (it + 1 >= nk) break;
+    if (it + 2 < nk) gload(it + 2, a0, b0);
+    if (!stage_in(it + 1, a1, b1)) {
+      fail = 1;
+      break;
     }
   }
   // wait for the last commit (it covers every MMA issued before it)
