@@ -33,7 +33,7 @@ constexpr int kPC = 8;   // CTAs per cluster (one cluster per tile)
 __global__ void __cluster_dims__(kPC, 1, 1) __launch_bounds__(256)
     k_potrf_cluster(double* TLR_RESTRICT D, int n, int b, int k, double* TLR_RESTRICT rhs, double* TLR_RESTRICT z,
                     double* TLR_RESTRICT ldpart, double* TLR_RESTRICT qpart, int* TLR_RESTRICT status,
-                    size_t sD, size_t sV, int sS) {
+                    size_t sD, size_t sV, int sS, int staged) {
   cg::cluster_group cluster = cg::this_cluster();
   const int g = (int)cluster.block_rank(), G = kPC;
   const int bz = blockIdx.x / kPC;  // which tile of the batch
@@ -47,7 +47,9 @@ __global__ void __cluster_dims__(kPC, 1, 1) __launch_bounds__(256)
   __shared__ double Li[kPB][kPB + 1];  // L11^{-1}
   __shared__ double dinv[kPB];
   __shared__ double zp[kPB];
-  extern __shared__ double Ps[];  // the panel below the diagonal block, b x (kPB + 1)
+  extern __shared__ double Ps[];  // the panel below the diagonal block, b x (kPB + 1), when staged
+  __shared__ double Pa[kPB][kPB + 1];
+  __shared__ double Pc[kPB][kPB + 1];
   __shared__ int go, fail;
   __shared__ double logdet_acc, quad_acc;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -184,16 +186,51 @@ __global__ void __cluster_dims__(kPC, 1, 1) __launch_bounds__(256)
         quad_acc = q;
       }
     }
-    // trailing update of the lower triangle in 32 x 32 blocks, from the whole panel staged once in
-    // shared memory (rows below the diagonal block, ld kPB + 1)
-    for (int e = tid; e < m * kPB; e += blockDim.x) {
-      const int row = e % m, t = e / m;
-      Ps[(size_t)row * (kPB + 1) + t] = t < pw ? A[(size_t)(p0 + t) * b + p0 + pw + row] : 0.0;
+    // trailing update of the lower triangle in 32 x 32 blocks.  staged: from the whole panel put in
+    // shared memory once (rows below the diagonal block, ld kPB + 1); otherwise (tiles too tall for
+    // that) each block's two 32 x 32 panel pieces are loaded from L2 in turn
+    if (staged) {
+      for (int e = tid; e < m * kPB; e += blockDim.x) {
+        const int row = e % m, t = e / m;
+        Ps[(size_t)row * (kPB + 1) + t] = t < pw ? A[(size_t)(p0 + t) * b + p0 + pw + row] : 0.0;
+      }
+      __syncthreads();
     }
-    __syncthreads();
     const int mb = (m + 31) / 32;
     const int nblk = mb * (mb + 1) / 2;
     for (int blk = g; blk < nblk; blk += G) {
+      if (!staged) {
+        int rb = (int)((sqrt(8.0 * blk + 1.0) - 1.0) * 0.5);
+        while (rb * (rb + 1) / 2 > blk) --rb;
+        while ((rb + 1) * (rb + 2) / 2 <= blk) ++rb;
+        const int cb = blk - rb * (rb + 1) / 2;
+        const int a0 = rb * 32, c0 = cb * 32;
+        __syncthreads();
+        for (int t = warp; t < kPB; t += 8) {
+          const double* col = A + (size_t)(p0 + t) * b + p0 + pw;
+          Pa[lane][t] = (t < pw && a0 + lane < m) ? col[a0 + lane] : 0.0;
+          Pc[lane][t] = (t < pw && c0 + lane < m) ? col[c0 + lane] : 0.0;
+        }
+        __syncthreads();
+        const int cl = tid & 31, rl = tid >> 5;  // column cl, rows rl + 8q
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+        for (int t = 0; t < kPB; ++t) {
+          const double pc = Pc[cl][t];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[q] = fma(Pa[rl + 8 * q][t], pc, acc[q]);
+        }
+        const int cg2 = c0 + cl;
+        if (cg2 < m) {
+          double* colp = A + (size_t)(p0 + pw + cg2) * b + p0 + pw;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int ag = a0 + rl + 8 * q;
+            if (ag < m && ag >= cg2) colp[ag] -= acc[q];
+          }
+        }
+        continue;
+      }
       int rb = (int)((sqrt(8.0 * blk + 1.0) - 1.0) * 0.5);
       while (rb * (rb + 1) / 2 > blk) --rb;
       while ((rb + 1) * (rb + 2) / 2 <= blk) ++rb;
@@ -239,9 +276,12 @@ int launch_potrf(double* D, int n, int b, int k, double* rhs, double* z, double*
 
 int launch_potrf_batched(double* D, int n, int b, int k, double* rhs, double* z, double* ldpart, double* qpart,
                          int* status, int nbatch, size_t sD, size_t sV, int sS, cudaStream_t s) {
-  const size_t sm = (size_t)b * (kPB + 1) * sizeof(double);
+  // the staged panel needs b (kPB + 1) doubles beside the 34 KB of static shared memory
+  const size_t sm_staged = (size_t)b * (kPB + 1) * sizeof(double);
+  const int staged = sm_staged <= 190 * 1024;
+  const size_t sm = staged ? sm_staged : 0;
   cudaFuncSetAttribute(k_potrf_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_potrf_cluster<<<kPC * nbatch, 256, sm, s>>>(D, n, b, k, rhs, z, ldpart, qpart, status, sD, sV, sS);
+  k_potrf_cluster<<<kPC * nbatch, 256, sm, s>>>(D, n, b, k, rhs, z, ldpart, qpart, status, sD, sV, sS, staged);
   return (int)cudaGetLastError();
 }
 

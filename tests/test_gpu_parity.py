@@ -91,3 +91,30 @@ def test_factor_tiles_match_oracle(tlr):
         Ug, Vg = Lo_gpu[key]
         assert Ug.shape == U.shape
         np.testing.assert_allclose(Ug @ Vg.T, U @ V.T, rtol=0, atol=1e-11)
+
+
+@pytest.mark.parametrize("data,n,b,rule,value,tol", [
+    ("n1030_b100_data.npz", 1030, 103, "adaptive", 0.9, REL_TOL),  # odd tile size: CUDA-core sketch and residual
+    ("n1030_b100_data.npz", 1030, 103, "fixed", 1e-6, REL_TOL),
+    ("n2000_b200_r1.0_e0.005_data.npz", 2000, 650, "adaptive", 0.9, REL_TOL),  # tiles wider than 512
+    # POTRF panel too tall to stage; the one 1000 x 1000 off-diagonal tile has rank 24, accepted at
+    # k = 32 exactly at the margin, so the sketch's subspace error shows at 2.6e-10 relative
+    ("n2000_b200_r1.0_e0.005_data.npz", 2000, 1000, "adaptive", 0.9, 1e-9),
+])
+def test_tile_sizes_outside_tensor_core_forms(tlr, data, n, b, rule, value, tol):
+    """The sketch, residual and orthonormalisation have tensor-core / register forms for even tile
+    sizes up to 512 and general forms otherwise, and POTRF stages its panel in shared memory only
+    up to about 740 rows; the general forms keep the oracle's ranks and log-likelihood (the oracle
+    is the reference's algorithm run here)."""
+    d = np.load(os.path.join(GOLD, data))
+    S, y = d["S"], d["y"]
+    theta = (1.0, 0.3, 0.05) if "r1.0" not in data else (1.0, 1.0, 0.005)
+    bounds = O.tile_bounds(n, b)
+    ll_o, _, info_o = O.tlr_loglik(S, y, theta, bounds, rule, value)
+    plan = tlr.get_plan(n, b)
+    ev = plan.evaluate(theta, rule, value, host_S=S, host_y=y)
+    assert list(ev.sigma_ranks) == list(info_o["sigma_ranks"])
+    assert ev.info["completed"] == info_o["completed"]
+    if info_o["completed"]:
+        assert list(ev.factor_ranks) == list(info_o["factor_ranks"])
+        assert abs(ev.loglik - ll_o) <= tol * abs(ll_o)
