@@ -496,7 +496,9 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     for (int c = 0; c < s; ++c)
       for (int a = tid; a < s; a += kRcT) Zc[(size_t)c * lc + a] = (a >= c) ? Mc[(size_t)a * lc + c] : 0.0;
     __syncthreads();
-    cta_jacobi_svd(Zc, lc, s, s, Vc, lc, sig, perm, &iflag);
+    // columns below 1e-14 of the largest singular value (the projections' rounding noise) are not
+    // rotated: their relative orthogonality test would otherwise run to the sweep limit
+    cta_jacobi_svd(Zc, lc, s, s, Vc, lc, sig, perm, &iflag, 40, 1e-28);
     // Vc <- normalised Z (right singular vectors of M), in place of the rotation matrix
     for (int c = warp; c < s; c += kRcW) {
       const double inv = sig[c] > 0.0 ? 1.0 / sig[c] : 0.0;
