@@ -49,6 +49,10 @@ def parse():
     return ap.parse_args()
 
 
+# k_recompress DRAM traffic per launch at N = 50,000, b = 500, adaptive tau = 0.9 (bytes): the mean of
+# dram__bytes_read.sum + dram__bytes_write.sum over the 98 launches of one evaluation, from an ncu
+# capture of `bench.py --steps 1 --warmup 1 --cpu-sample 0 --plain-steps 0 --batch 1 --dense 0`
+RC_TRAFFIC_N50K = 283.5e6
 METRIC = "TLR loglik+grad evals/s at N=50k vs plain FP64 on B200; |dl| vs FP64 dense"
 
 
@@ -299,7 +303,12 @@ def main():
         per_launch_ms = st["ms"] / max(st["launches"], 1)
         achieved_gbs = st["bytes"] / max(st["launches"], 1) / (per_launch_ms * 1e-3) / 1e9
         roof = {"kernel": top, "bound": "hbm", "achieved": achieved_gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved_gbs / pk["hbm_gbs"], "traffic": None, "peak_kind": pk_kind,
+                "frac": achieved_gbs / pk["hbm_gbs"], "peak_kind": pk_kind,
+                # DRAM bytes per launch from one ncu capture of this kernel on this workload
+                "traffic": (RC_TRAFFIC_N50K if top == "recompress" and (a.n, a.b, a.tau) == (50000, 500, 0.9)
+                            and a.precision == "mixed" else None),
+                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum, mean over the 98 "
+                                   "k_recompress launches of one evaluation (batch 1, same workload, 1-pass capture)"),
                 "fp64_tflops": st["flops"] / max(st["launches"], 1) / (per_launch_ms * 1e-3) / 1e12,
                 "fp64_peak_nominal_tflops": 37.0,
                 "share": prof_stats[top]["ms"] / sum(v["ms"] for v in prof_stats.values()),
