@@ -175,28 +175,17 @@ def main():
         return
     import numpy as np
     import torch
-    import torch.distributed as dist
 
     import adaptive_tlr_pilots_b200 as tlr
     from adaptive_tlr_pilots_b200 import synth
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    from adaptive_tlr_pilots_b200.replicas import Replicas
+
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(ms):
-        t = torch.tensor([ms], device="cuda")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    rep = Replicas("nccl")  # one replica per GPU: independent evaluations, no data-path exchange
+    world, rank = rep.world, rep.rank
+    barrier, max_over_ranks = rep.barrier, rep.max_over_ranks
 
     if a.sim == "dense":
         S, y, _, _ = synth.simulate_field(a.n, THETA, device=local)
@@ -348,8 +337,7 @@ def main():
             line["cpu_baseline"] = cpu_baseline(S, y, a)
         print(json.dumps(line), flush=True)
     tlr.release_plans()
-    if world > 1:
-        dist.destroy_process_group()
+    rep.close()
 
 
 if __name__ == "__main__":
