@@ -310,7 +310,8 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f64+tf32x3",
-                "data": "synthetic (seeded reference protocol, y = L z with the dense FP64 Cholesky)",
+                "data": ("synthetic (seeded reference protocol, y = L z with the dense FP64 Cholesky)" if a.sim == "dense"
+                         else "synthetic (seeded reference protocol, y = L z with a tight TLR factor: no dense factor fits)"),
                 "config": dict(workload(a), parallelism=f"replicas x{world}"),
                 "loglik": ll0, "dense_loglik": dense,
                 "abs_dloglik_vs_dense": None if (dense is None or ll0 is None) else abs(ll0 - dense),
