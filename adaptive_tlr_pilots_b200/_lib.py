@@ -71,6 +71,8 @@ SIGNATURES = {
     "tlr_plan_kernel_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int]),
+    "tlr_selftest_bounded_wait": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                                 ctypes.POINTER(ctypes.c_longlong)]),
     "tlr_last_error": (ctypes.c_char_p, []),
 }
 

@@ -851,6 +851,38 @@ int tlr_plan_set_precision(tlr_plan* p, int mode) {
   return 0;
 }
 
+int tlr_selftest_bounded_wait(long long iterations, int device, double* elapsed_ms, long long* limit) {
+  if (limit) *limit = tlr::tc_wait_limit();
+  if (iterations <= 0 || iterations > tlr::tc_wait_limit()) return fail(TLR_ERR_ARG, "iterations out of range");
+  int rc = cuda_check(cudaSetDevice(device), "set device");
+  if (rc) return rc;
+  int* d = nullptr;
+  cudaStream_t s = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int h = 1;
+  rc = cuda_check(cudaMalloc(&d, sizeof(int)), "status word");
+  if (!rc) rc = cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+  if (!rc) rc = cuda_check(cudaEventCreate(&e0), "event");
+  if (!rc) rc = cuda_check(cudaEventCreate(&e1), "event");
+  if (!rc) rc = cuda_check(cudaEventRecord(e0, s), "event");
+  if (!rc) rc = cuda_check((cudaError_t)tlr::launch_wait_selftest(iterations, d, s), "self-test launch");
+  if (!rc) rc = cuda_check(cudaEventRecord(e1, s), "event");
+  if (!rc) rc = cuda_check(cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, s), "status copy");
+  if (!rc) rc = cuda_check(cudaStreamSynchronize(s), "self-test");
+  float ms = 0.f;
+  if (!rc && elapsed_ms) {
+    cudaEventElapsedTime(&ms, e0, e1);
+    *elapsed_ms = ms;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (s) cudaStreamDestroy(s);
+  if (d) cudaFree(d);
+  if (rc) return rc;
+  if (h == TLR_ERR_TIMEOUT) return fail(TLR_ERR_TIMEOUT, "a device wait ran out of its iteration limit");
+  return h;
+}
+
 int tlr_plan_set_profiling(tlr_plan* p, int on) {
   if (!p) return fail(TLR_ERR_ARG, "plan is NULL");
   p->prof = on != 0;

@@ -71,6 +71,9 @@ struct CopyJob {
 int launch_dgemm_batched(const GemmJob* jobs, int njobs, int max_m, int max_n, const int* status, int kind,
                          cudaStream_t s);
 int launch_gemm_tc3(const GemmJob* jobs, int njobs, int max_m, int max_n, int* status, int kind, cudaStream_t s);
+// the bounded-wait self-test (tlr_tc.cu) and the iteration limit of the GEMM's waits
+int launch_wait_selftest(long long limit, int* status, cudaStream_t s);
+long long tc_wait_limit();
 int launch_tri_inv(const double* D, double* Li, int n, int b, int nB, const int* status, cudaStream_t s);
 int launch_copy_cols(const CopyJob* jobs, int njobs, const int* status, cudaStream_t s);
 int launch_alpha_step(int n, int b, int m, int nB, const double* U, const double* V, const int* rank, int cap,

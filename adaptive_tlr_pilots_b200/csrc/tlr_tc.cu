@@ -28,7 +28,7 @@ constexpr int kTcBK = 32;
 constexpr int kTcStages = 2;
 // bytes per stage: A_hi, A_lo (128 x 32 x 4), B_hi, B_lo (128 x 32 x 4)
 constexpr int kTcStageBytes = 4 * kTcM * kTcBK * 4;
-constexpr long long kTcWaitLimit = 1ll << 26;
+constexpr long long kTcWaitLimit = 1ll << 23;  // polls of about 140 ns on B200: about 1.2 s
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -82,10 +82,40 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity) {
 }
 
 // bounded wait; false on timeout
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-  for (long long it = 0; it < kTcWaitLimit; ++it)
+__device__ __forceinline__ bool mbar_wait_n(uint32_t mbar, uint32_t parity, long long limit) {
+  for (long long it = 0; it < limit; ++it)
     if (mbar_try_wait(mbar, parity)) return true;
   return false;
+}
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  return mbar_wait_n(mbar, parity, kTcWaitLimit);
+}
+
+// Self-test of the timeout path: the GEMM's set-up (tensor memory allocated, an mbarrier
+// initialised), then a bounded wait on a phase that nothing completes; when the wait runs out
+// the kernel frees its tensor memory and reports TLR_ERR_TIMEOUT (-7), as k_gemm_tc3 does.
+__global__ void k_wait_selftest(long long limit, int* status) {
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_base_sh;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                 "r"(32));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  bool ok = true;
+  if (tid == 0) ok = mbar_wait_n(smem_u32(&mbar), 0u, limit);  // no arrival: runs out
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base_sh), "r"(32));
+  if (tid == 0) *status = ok ? 0 : -7;
 }
 
 __global__ void __launch_bounds__(256) k_gemm_tc3(const GemmJob* TLR_RESTRICT jobs, int* TLR_RESTRICT status,
@@ -253,6 +283,13 @@ __global__ void __launch_bounds__(256) k_gemm_tc3(const GemmJob* TLR_RESTRICT jo
     }
   }
 }
+
+int launch_wait_selftest(long long limit, int* status, cudaStream_t s) {
+  k_wait_selftest<<<1, 64, 0, s>>>(limit, status);
+  return (int)cudaGetLastError();
+}
+
+long long tc_wait_limit() { return kTcWaitLimit; }
 
 int launch_gemm_tc3(const GemmJob* jobs, int njobs, int max_m, int max_n, int* status, int kind, cudaStream_t s) {
   if (njobs <= 0) return 0;

@@ -176,6 +176,14 @@ int tlr_plan_set_profiling(tlr_plan* plan, int on);
 int tlr_plan_kernel_stats(tlr_plan* plan, double* ms, long long* launches, double* flops, double* bytes, int nkinds,
                           int reset);
 
+/* Self-test of the failure path of the tensor-core kernels' bounded waits (no reference
+ * counterpart): one CTA allocates tensor memory and waits, at most `iterations` polls, on an
+ * mbarrier phase that nothing completes; it then frees the tensor memory and reports.  Returns
+ * TLR_ERR_TIMEOUT when the wait ran out (the expected outcome; the context stays usable), 0 if
+ * it did not, < 0 on other errors.  *elapsed_ms (optional): device time of the launch; *limit
+ * (optional): the poll limit of the production waits.  Allocates one int on `device`. */
+int tlr_selftest_bounded_wait(long long iterations, int device, double* elapsed_ms, long long* limit);
+
 /* Message of the last error on this thread. */
 const char* tlr_last_error(void);
 
