@@ -4,10 +4,10 @@ Drop-in for the TLR log-likelihood path of marysalvana/adaptive-tlr-pilots
 (codes/17_tlr_cholesky_pilot.py tlr_loglik and its callers), computed by hand-written sm_100a
 CUDA kernels behind the C ABI of include/tlr_b200.h.
 """
-from .tlr import (Likelihood, Plan, PlanBatch, TLRFactor, TLRLogLik, dense_loglik, get_plan,  # noqa: F401
-                  loglik, morton_order, neg_loglik_tlr, release_plans, skill, tile_bounds, tlr_loglik,
-                  tlr_loglik_grad, tlr_predict)
+from .tlr import (Likelihood, Plan, PlanBatch, TLRFactor, TLRLogLik, dense_loglik, get_kernel,  # noqa: F401
+                  get_plan, loglik, morton_order, neg_loglik_tlr, release_plans, set_kernel, skill, tile_bounds,
+                  tlr_loglik, tlr_loglik_grad, tlr_predict)
 
-__all__ = ["Likelihood", "Plan", "PlanBatch", "TLRFactor", "TLRLogLik", "dense_loglik", "get_plan", "loglik",
-           "morton_order", "neg_loglik_tlr", "release_plans", "skill", "tile_bounds", "tlr_loglik",
-           "tlr_loglik_grad", "tlr_predict"]
+__all__ = ["Likelihood", "Plan", "PlanBatch", "TLRFactor", "TLRLogLik", "dense_loglik", "get_kernel", "get_plan",
+           "loglik", "morton_order", "neg_loglik_tlr", "release_plans", "set_kernel", "skill", "tile_bounds",
+           "tlr_loglik", "tlr_loglik_grad", "tlr_predict"]

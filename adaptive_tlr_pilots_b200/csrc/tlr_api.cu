@@ -83,6 +83,7 @@ struct tlr_plan {
   int precision = TLR_PRECISION_FP64;
   // launch accounting and optional per-kernel event timing
   bool prof = false;
+  int nu5 = 0;  // covariance: 0 Matern 3/2, 1 Matern 5/2
   int prof_kind = -1;  // -1: every kind
   std::vector<cudaEvent_t> ev_pool;
   size_t ev_used = 0;
@@ -170,7 +171,7 @@ int run_compression(tlr_plan* p, double sigma2, double inv_range, int rule_fixed
   for (int base = 0; base < p->ntiles; base += p->chunk) {
     const int nc = std::min(p->chunk, p->ntiles - base);
     LAUNCH(TLR_K_FILL, tlr::launch_fill_int(p->need, 1, nc, s));
-    LAUNCH(TLR_K_GEN, tlr::launch_gen_offdiag(p->xy, p->n, p->b, base, p->ti, p->tj, p->T, nc, sigma2, inv_range, p->status, s));
+    LAUNCH(TLR_K_GEN, tlr::launch_gen_offdiag(p->xy, p->n, p->b, base, p->ti, p->tj, p->T, nc, sigma2, inv_range, p->nu5, p->status, s));
     for (int lev = 0; lev < kLevels; ++lev) {
       const int k = 16 << lev;
       double* Pp = p->P;
@@ -203,7 +204,7 @@ int run_compression(tlr_plan* p, double sigma2, double inv_range, int rule_fixed
 int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugget, int rule_fixed, double thr_rel,
                       double thr_abs) {
   cudaStream_t s = p->stream, sd = p->side;
-  LAUNCH(TLR_K_DIAG, tlr::launch_diag_build(p->xy, p->n, p->b, 0, sigma2, inv_range, nugget, p->U, p->Yd, p->rank,
+  LAUNCH(TLR_K_DIAG, tlr::launch_diag_build(p->xy, p->n, p->b, 0, sigma2, inv_range, p->nu5, nugget, p->U, p->Yd, p->rank,
                                             p->cap, p->D, p->status, s));
   LAUNCH(TLR_K_POTRF, tlr::launch_potrf(p->D, p->n, p->b, 0, p->rhs, p->z, p->ldpart, p->qpart, p->status, s));
   for (int k = 0; k < p->nB; ++k) {
@@ -215,7 +216,7 @@ int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugge
       // done; step k's recompression touches tiles (i, j) with j > k + 1 only.
       TRY(cuda_check(cudaEventRecord(p->ev_panel, s), "event"));
       TRY(cuda_check(cudaStreamWaitEvent(sd, p->ev_panel, 0), "wait"));
-      LAUNCH_ON(sd, TLR_K_DIAG, tlr::launch_diag_build(p->xy, p->n, p->b, k + 1, sigma2, inv_range, nugget, p->U,
+      LAUNCH_ON(sd, TLR_K_DIAG, tlr::launch_diag_build(p->xy, p->n, p->b, k + 1, sigma2, inv_range, p->nu5, nugget, p->U,
                                                        p->Yd, p->rank, p->cap, p->D, p->status, sd));
       LAUNCH_ON(sd, TLR_K_POTRF, tlr::launch_potrf(p->D, p->n, p->b, k + 1, p->rhs, p->z, p->ldpart, p->qpart,
                                                    p->status, sd));
@@ -450,7 +451,7 @@ int run_backward(tlr_plan* p, double sigma2, double inv_range, double eta) {
     } else if (L.kind == 2) {
       TRY(cuda_check(cudaStreamWaitEvent(s, p->ev_alpha[L.m], 0), "wait"));
     } else {
-      LAUNCH(TLR_K_DTRACE, tlr::launch_dtrace_step(p->xy, n, b, L.m, nB, sigma2, inv_range, eta, Zb, base + oAl,
+      LAUNCH(TLR_K_DTRACE, tlr::launch_dtrace_step(p->xy, n, b, L.m, nB, sigma2, inv_range, p->nu5, eta, Zb, base + oAl,
                                                    base + oPart + 3 * L.part_off, p->status, s));
     }
   }
@@ -881,6 +882,13 @@ int tlr_selftest_bounded_wait(long long iterations, int device, double* elapsed_
   if (rc) return rc;
   if (h == TLR_ERR_TIMEOUT) return fail(TLR_ERR_TIMEOUT, "a device wait ran out of its iteration limit");
   return h;
+}
+
+int tlr_plan_set_kernel(tlr_plan* p, double nu) {
+  if (!p) return fail(TLR_ERR_ARG, "plan is NULL");
+  if (nu != 1.5 && nu != 2.5) return fail(TLR_ERR_ARG, "nu must be 1.5 or 2.5");
+  p->nu5 = nu == 2.5 ? 1 : 0;
+  return 0;
 }
 
 int tlr_plan_set_profiling(tlr_plan* p, int on) {

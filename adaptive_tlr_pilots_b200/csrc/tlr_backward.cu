@@ -311,7 +311,7 @@ int launch_alpha_step(int n, int b, int m, int nB, const double* U, const double
 // (i, m), i >= m, of block column m; weight 2 for off-diagonal tiles.  One CTA per 32 x 32 block;
 // partial sums [3] per CTA into part (fixed slots: deterministic final reduction).
 __global__ void __launch_bounds__(256) k_dtrace_step(const double* TLR_RESTRICT xy, int n, int b, int m, int nB,
-                                                    double sigma2, double inv_range, double eta,
+                                                    double sigma2, double inv_range, int nu5, double eta,
                                                     const double* TLR_RESTRICT Zbuf,
                                                     const double* TLR_RESTRICT alpha, double* TLR_RESTRICT part,
                                                     const int* TLR_RESTRICT status) {
@@ -341,11 +341,14 @@ __global__ void __launch_bounds__(256) k_dtrace_step(const double* TLR_RESTRICT 
         if (a >= bi) continue;
         const double2 pa = p2[(size_t)i * b + a];
         const double dx = pa.x - pc.x, dy = pa.y - pc.y;
-        const double x = kSqrt3 * sqrt(fmax(dx * dx + dy * dy, 0.0)) * inv_range;
+        // dk/d sigma2 = k; dk/d range = sigma2 x^2 e^{-x} / range (nu 3/2) or
+        // sigma2 x^2 (1 + x) e^{-x} / (3 range) (nu 5/2)
+        const double h = sqrt(fmax(dx * dx + dy * dy, 0.0));
+        const double x = (nu5 ? kSqrt5 : kSqrt3) * h * inv_range;
         const double e = exp(-x);
         const double sbar = 0.5 * (ai[a] * amc - Z[(size_t)c * b + a]);
-        double ds = (1.0 + x) * e;
-        const double dr = sigma2 * x * x * e * inv_range;
+        double ds = (nu5 ? 1.0 + x + x * x / 3.0 : 1.0 + x) * e;
+        const double dr = nu5 ? sigma2 * x * x * (1.0 + x) / 3.0 * e * inv_range : sigma2 * x * x * e * inv_range;
         double de = 0.0;
         if (i == m && a == c) {
           ds += eta;
@@ -369,11 +372,12 @@ __global__ void __launch_bounds__(256) k_dtrace_step(const double* TLR_RESTRICT 
   }
 }
 
-int launch_dtrace_step(const double* xy, int n, int b, int m, int nB, double sigma2, double inv_range, double eta,
-                       const double* Zbuf, const double* alpha, double* part, const int* status, cudaStream_t s) {
+int launch_dtrace_step(const double* xy, int n, int b, int m, int nB, double sigma2, double inv_range, int nu5,
+                       double eta, const double* Zbuf, const double* alpha, double* part, const int* status,
+                       cudaStream_t s) {
   const int nb32 = (b + 31) / 32;
   const int ntile = nB - m;
-  k_dtrace_step<<<ntile * nb32 * nb32, 256, 0, s>>>(xy, n, b, m, nB, sigma2, inv_range, eta, Zbuf, alpha, part,
+  k_dtrace_step<<<ntile * nb32 * nb32, 256, 0, s>>>(xy, n, b, m, nB, sigma2, inv_range, nu5, eta, Zbuf, alpha, part,
                                                     status);
   return (int)cudaGetLastError();
 }

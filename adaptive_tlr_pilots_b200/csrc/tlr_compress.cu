@@ -34,7 +34,7 @@ __device__ __forceinline__ double omega_entry(uint32_t tile, uint32_t row, uint3
 // T[c] = sigma2 * matern32(dist(S_i, S_j)), row-major with leading dimension b.
 __global__ void k_gen_offdiag(const double* TLR_RESTRICT xy, int n, int b, int tile_base,
                               const int* TLR_RESTRICT ti, const int* TLR_RESTRICT tj, double* TLR_RESTRICT T,
-                              double sigma2, double inv_range, const int* TLR_RESTRICT status) {
+                              double sigma2, double inv_range, int nu5, const int* TLR_RESTRICT status) {
   if (*status != 0) return;
   const int c = blockIdx.y;
   const int t = (tile_base + c);
@@ -48,7 +48,7 @@ __global__ void k_gen_offdiag(const double* TLR_RESTRICT xy, int n, int b, int t
     const int a = e / bj, q = e - a * bj;
     const double2 pa = reinterpret_cast<const double2*>(xy)[i0 + a];
     const double2 pq = reinterpret_cast<const double2*>(xy)[j0 + q];
-    Tc[(size_t)a * b + q] = matern32_cov(pa.x, pa.y, pq.x, pq.y, sigma2, inv_range);
+    Tc[(size_t)a * b + q] = matern_cov(pa.x, pa.y, pq.x, pq.y, sigma2, inv_range, nu5);
   }
 }
 
@@ -714,10 +714,10 @@ __global__ void __launch_bounds__(1024) k_finalize(int n, int b, int k, int ldp,
 // ----------------------------------------------------------------------------------------
 // launchers
 int launch_gen_offdiag(const double* xy, int n, int b, int tile_base, const int* ti, const int* tj,
-                       double* T, int nchunk, double sigma2, double inv_range, const int* status,
+                       double* T, int nchunk, double sigma2, double inv_range, int nu5, const int* status,
                        cudaStream_t s) {
   dim3 grid((unsigned)((b * b + 1023) / 1024), (unsigned)nchunk);
-  k_gen_offdiag<<<grid, 256, 0, s>>>(xy, n, b, tile_base, ti, tj, T, sigma2, inv_range, status);
+  k_gen_offdiag<<<grid, 256, 0, s>>>(xy, n, b, tile_base, ti, tj, T, sigma2, inv_range, nu5, status);
   return (int)cudaGetLastError();
 }
 

@@ -15,6 +15,7 @@
 namespace tlr {
 
 constexpr double kSqrt3 = 1.7320508075688772935;
+constexpr double kSqrt5 = 2.2360679774997896964;
 
 // ---------------------------------------------------------------- FP64 tensor cores, async copies
 // D = A B + D on the FP64 tensor cores, one 8 x 8 x 4 step per warp (g = lane / 4, t = lane % 4):
@@ -73,12 +74,18 @@ __device__ __forceinline__ void add_work(const int* status, int kind, double flo
 }
 
 // ---------------------------------------------------------------- covariance model
-// Matern nu=3/2 kernel sigma2 (1 + x) e^{-x}, x = sqrt(3) h / range
-// (codes/11_tlr_rank_rules.py:35-37 with the sigma2 scaling of codes/17_tlr_cholesky_pilot.py:161).
-__device__ __forceinline__ double matern32_cov(double ax, double ay, double bx, double by,
-                                               double sigma2, double inv_range) {
+// Matern kernel sigma2 k(h): nu = 3/2, k = (1 + x) e^{-x}, x = sqrt(3) h / range
+// (codes/11_tlr_rank_rules.py:35-37 with the sigma2 scaling of codes/17_tlr_cholesky_pilot.py:161);
+// nu = 5/2 (nu5 != 0), k = (1 + x + x^2 / 3) e^{-x}, x = sqrt(5) h / range
+// (codes/24_screening_stress.py:30-43, the kernel it patches in for the regime sweeps).
+__device__ __forceinline__ double matern_cov(double ax, double ay, double bx, double by, double sigma2,
+                                             double inv_range, int nu5) {
   const double dx = ax - bx, dy = ay - by;
   const double h = sqrt(fmax(dx * dx + dy * dy, 0.0));
+  if (nu5) {
+    const double x = kSqrt5 * h * inv_range;
+    return sigma2 * ((1.0 + x + x * x / 3.0) * exp(-x));
+  }
   const double x = kSqrt3 * h * inv_range;
   return sigma2 * ((1.0 + x) * exp(-x));
 }

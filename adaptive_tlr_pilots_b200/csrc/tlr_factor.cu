@@ -25,7 +25,7 @@ __device__ __forceinline__ int tidx(int i, int j) { return i * (i - 1) / 2 + j; 
 // lower-triangular 32 x 32 block; the inner index runs over (m, q) in ascending order, 32 at a
 // time through shared memory.
 __global__ void __launch_bounds__(256) k_diag_build(const double* TLR_RESTRICT xy, int n, int b, int k,
-                                                   double sigma2, double inv_range, double nugget,
+                                                   double sigma2, double inv_range, int nu5, double nugget,
                                                    const double* TLR_RESTRICT U, const double* TLR_RESTRICT Y,
                                                    const int* TLR_RESTRICT rank, int cap, double* TLR_RESTRICT D,
                                                    const int* TLR_RESTRICT status) {
@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(256) k_diag_build(const double* TLR_RESTRICT x
   for (int q = 0; q < 4; ++q) {
     const int ag = r0 + rl + 8 * q;
     const double2 pa = p2[k * b + min(ag, bk - 1)];
-    acc[q] = matern32_cov(pa.x, pa.y, pc.x, pc.y, sigma2, inv_range) + (ag == cg ? nugget : 0.0);
+    acc[q] = matern_cov(pa.x, pa.y, pc.x, pc.y, sigma2, inv_range, nu5) + (ag == cg ? nugget : 0.0);
   }
   __syncthreads();
   const int R = off[k];
@@ -585,12 +585,12 @@ __global__ void k_finish(int nB, int n, const double* ldpart, const double* qpar
 }
 
 // ----------------------------------------------------------------------------------------
-int launch_diag_build(const double* xy, int n, int b, int k, double sigma2, double inv_range, double nugget,
-                      const double* U, const double* Y, const int* rank, int cap, double* D, const int* status,
-                      cudaStream_t s) {
+int launch_diag_build(const double* xy, int n, int b, int k, double sigma2, double inv_range, int nu5,
+                      double nugget, const double* U, const double* Y, const int* rank, int cap, double* D,
+                      const int* status, cudaStream_t s) {
   const int bk = std::min(b, n - k * b);
   const int nb = (bk + 31) / 32;
-  k_diag_build<<<nb * (nb + 1) / 2, 256, 0, s>>>(xy, n, b, k, sigma2, inv_range, nugget, U, Y, rank, cap, D,
+  k_diag_build<<<nb * (nb + 1) / 2, 256, 0, s>>>(xy, n, b, k, sigma2, inv_range, nu5, nugget, U, Y, rank, cap, D,
                                                  status);
   return (int)cudaGetLastError();
 }

@@ -14,7 +14,7 @@ int launch_gather_sites(const double* xy_in, const double* y_in, const long long
 
 // initial compression
 int launch_gen_offdiag(const double* xy, int n, int b, int tile_base, const int* ti, const int* tj, double* T,
-                       int nchunk, double sigma2, double inv_range, const int* status, cudaStream_t s);
+                       int nchunk, double sigma2, double inv_range, int nu5, const int* status, cudaStream_t s);
 int launch_sketch(const double* T, int n, int b, int k, int tile_base, const int* ti, const int* tj, const int* need,
                   const double* P, double* out, int ldp, int omega, int mode, int nchunk, const int* status,
                   cudaStream_t s);
@@ -36,9 +36,9 @@ int launch_finalize(int n, int b, int k, int ldp, int cap, int margin, int rule_
                     cudaStream_t s);
 
 // factorization
-int launch_diag_build(const double* xy, int n, int b, int k, double sigma2, double inv_range, double nugget,
-                      const double* U, const double* Y, const int* rank, int cap, double* D, const int* status,
-                      cudaStream_t s);
+int launch_diag_build(const double* xy, int n, int b, int k, double sigma2, double inv_range, int nu5,
+                      double nugget, const double* U, const double* Y, const int* rank, int cap, double* D,
+                      const int* status, cudaStream_t s);
 int launch_potrf(double* D, int n, int b, int k, double* rhs, double* z, double* ldpart, double* qpart,
                  int* status, cudaStream_t s);
 // nbatch tiles, tile q at D + q sD, rhs / z + q sV, ldpart / qpart / status + q sS
@@ -79,8 +79,9 @@ int launch_copy_cols(const CopyJob* jobs, int njobs, const int* status, cudaStre
 int launch_alpha_step(int n, int b, int m, int nB, const double* U, const double* V, const int* rank, int cap,
                       const double* Li, const double* z, double* alpha, double* work, const int* status,
                       cudaStream_t s);
-int launch_dtrace_step(const double* xy, int n, int b, int m, int nB, double sigma2, double inv_range, double eta,
-                       const double* Zbuf, const double* alpha, double* part, const int* status, cudaStream_t s);
+int launch_dtrace_step(const double* xy, int n, int b, int m, int nB, double sigma2, double inv_range, int nu5,
+                       double eta, const double* Zbuf, const double* alpha, double* part, const int* status,
+                       cudaStream_t s);
 int launch_grad_finish(const double* part, long nparts, double* grad, const int* status, cudaStream_t s);
 
 // solves and products with the factor (tlr_solve.cu); column-major n x m, ld n

@@ -23,6 +23,22 @@ import numpy as np
 from . import _lib
 
 RULES = {"fixed": _lib.TLR_RULE_FIXED, "adaptive": _lib.TLR_RULE_ADAPTIVE}
+KERNELS = (1.5, 2.5)  # Matern smoothness nu
+_NU = 1.5
+
+
+def set_kernel(nu):
+    """Covariance smoothness for every later evaluation of plans that have none of their own:
+    nu = 1.5 (Matern 3/2, the default) or 2.5 (Matern 5/2).  The counterpart of
+    codes/24_screening_stress.py:46-47 set_kernel, which patches the kernel of 17 globally."""
+    global _NU
+    if float(nu) not in KERNELS:
+        raise ValueError(f"nu must be one of {KERNELS}")
+    _NU = float(nu)
+
+
+def get_kernel():
+    return _NU
 
 
 def _torch():
@@ -95,6 +111,21 @@ class Plan:
         self.handle = h
         self.generation = 0
         self._data = None
+        self.nu = None          # None: follow set_kernel; else this plan's own smoothness
+        self._nu_applied = 1.5  # the C plan starts with Matern 3/2
+
+    def set_kernel(self, nu):
+        """This plan's covariance smoothness (1.5 or 2.5), independent of set_kernel."""
+        if float(nu) not in KERNELS:
+            raise ValueError(f"nu must be one of {KERNELS}")
+        self.nu = float(nu)
+        self._apply_kernel()
+
+    def _apply_kernel(self):
+        nu = self.nu if self.nu is not None else _NU
+        if nu != self._nu_applied:
+            _lib.check(self.lib.tlr_plan_set_kernel(self.handle, ctypes.c_double(nu)))
+            self._nu_applied = nu
 
     def close(self):
         if self.handle is not None and self.handle.value:
@@ -122,6 +153,7 @@ class Plan:
         """One log-likelihood evaluation (and its gradient when grad=True) on the device."""
         if rule not in RULES:
             raise ValueError(f"rule must be one of {sorted(RULES)}, got {rule!r}")
+        self._apply_kernel()
         th = (ctypes.c_double * 3)(*[float(v) for v in theta])
         ll = ctypes.c_double(0.0)
         info = _lib.TlrInfo()
@@ -269,6 +301,8 @@ class PlanBatch:
         m = th.shape[0]
         if m > self.count or th.shape[1] != 3:
             raise ValueError(f"thetas must be at most {self.count} x 3")
+        for p in self.plans[:m]:
+            p._apply_kernel()
         handles = (ctypes.c_void_p * m)(*[p.handle.value for p in self.plans[:m]])
         ll = np.full(m, np.nan)
         g = np.zeros((m, 3))
@@ -415,12 +449,16 @@ def tlr_loglik(S, y, theta, bounds, rule, value, cap=64, device=0):
     return ev.loglik, TLRFactor(plan), ev.info
 
 
-def _cross_cov(Sp, S, theta, device=0):
-    """sigma2 * matern32(dist(Sp, S)) on the device (np x n), codes/17_tlr_cholesky_pilot.py:270."""
+def _cross_cov(Sp, S, theta, device=0, nu=1.5):
+    """sigma2 * matern(dist(Sp, S)) on the device (np x n), codes/17_tlr_cholesky_pilot.py:270
+    (nu = 2.5: the kernel of codes/24_screening_stress.py:38-42)."""
     torch = _torch()
     dev = torch.device("cuda", device)
     A = torch.as_tensor(np.asarray(Sp, dtype=np.float64), device=dev)
     B = torch.as_tensor(np.asarray(S, dtype=np.float64), device=dev)
+    if nu == 2.5:
+        x = torch.cdist(A, B) * ((5.0 ** 0.5) / float(theta[1]))
+        return float(theta[0]) * (1.0 + x + x * x / 3.0) * torch.exp(-x)
     x = torch.cdist(A, B) * ((3.0 ** 0.5) / float(theta[1]))
     return float(theta[0]) * (1.0 + x) * torch.exp(-x)
 
@@ -432,7 +470,7 @@ def tlr_predict(S, y, Sp, theta, bounds, fac):
     torch = _torch()
     fac._check()
     plan = fac.plan
-    Kp = _cross_cov(Sp, S, theta, plan.device)
+    Kp = _cross_cov(Sp, S, theta, plan.device, plan._nu_applied)
     yt = torch.as_tensor(np.asarray(y, dtype=np.float64), device=plan.dev)
     alpha = fac.backward(fac.forward(yt))
     mu = Kp @ alpha
@@ -470,7 +508,8 @@ def neg_loglik_tlr(logth, S, y, bounds, rule, value, trace):
 def dense_loglik(S, y, theta, device=0):
     """Dense FP64 log-likelihood on the GPU (cuSOLVER Cholesky through torch); None if not PD.
 
-    The 'dense' rule of codes/17_tlr_cholesky_pilot.py:282-284 (rules.loglik_dense, 11:112-120)."""
+    The 'dense' rule of codes/17_tlr_cholesky_pilot.py:282-284 (rules.loglik_dense, 11:112-120),
+    with the kernel chosen by set_kernel."""
     torch = _torch()
     dev = torch.device("cuda", device)
     St = torch.as_tensor(np.asarray(S, dtype=np.float64), device=dev)
@@ -478,9 +517,14 @@ def dense_loglik(S, y, theta, device=0):
     sigma2, rng, eta = [float(v) for v in theta]
     with torch.no_grad():
         K = torch.cdist(St, St)
-        K.mul_((3.0 ** 0.5) / rng)
-        E = torch.exp(-K)
-        K.add_(1.0).mul_(E).mul_(sigma2)
+        if _NU == 2.5:  # (1 + x + x^2 / 3) e^{-x}, x = sqrt(5) h / range
+            K.mul_((5.0 ** 0.5) / rng)
+            E = torch.exp(-K)
+            K.mul_(K.div(3.0).add_(1.0)).add_(1.0).mul_(E).mul_(sigma2)
+        else:
+            K.mul_((3.0 ** 0.5) / rng)
+            E = torch.exp(-K)
+            K.add_(1.0).mul_(E).mul_(sigma2)
         del E
         K.diagonal().add_(sigma2 * eta)
         L, info = torch.linalg.cholesky_ex(K)

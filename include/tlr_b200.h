@@ -166,6 +166,13 @@ int tlr_plan_set_precision(tlr_plan* plan, int mode);
 #define TLR_K_GRAD_FINISH 17
 #define TLR_NKINDS 18
 
+/* Covariance smoothness for the plan's next evaluations: nu = 1.5 (Matern 3/2, the default,
+ * codes/11_tlr_rank_rules.py:35-37) or 2.5 (Matern 5/2, (1 + x + x^2/3) e^{-x}, x = sqrt(5) h /
+ * range: codes/24_screening_stress.py:30-47, which patches it into the TLR Cholesky of 17).
+ * Other values: TLR_ERR_ARG.  Applies to tile generation, the diagonal tiles and dSigma of the
+ * gradient. */
+int tlr_plan_set_kernel(tlr_plan* plan, double nu);
+
 /* Profiling: when on, every launch is bracketed by CUDA events on the plan's stream and the
  * per-kind device time is accumulated (no effect on results); on < 0 brackets only the launches
  * of kernel kind -on - 1 (the order of tlr_plan_kernel_stats).  No reference counterpart. */

@@ -36,6 +36,42 @@ def matern32(h, rng):
     return (1.0 + x) * np.exp(-x)
 
 
+SQRT5 = np.sqrt(5.0)
+NU = 1.5  # smoothness of the kernel every covariance below uses (set_kernel)
+
+
+def matern52(h, rng):
+    """Matern nu=5/2 correlation (1 + x + x^2/3) exp(-x), x = sqrt(5) h / range.
+
+    Follows codes/24_screening_stress.py:38-42."""
+    x = SQRT5 * h / rng
+    return (1.0 + x + x * x / 3.0) * np.exp(-x)
+
+
+def set_kernel(nu):
+    """Select nu = 1.5 or 2.5 for every later covariance: the counterpart of
+    codes/24_screening_stress.py:46-47, which patches the kernel of 17 globally."""
+    global NU
+    if nu not in (1.5, 2.5):
+        raise ValueError("nu must be 1.5 or 2.5")
+    NU = float(nu)
+
+
+def matern(h, rng):
+    """The selected kernel (set_kernel): matern32 or matern52."""
+    return matern52(h, rng) if NU == 2.5 else matern32(h, rng)
+
+
+def matern_drange(h, rng):
+    """d/drange of the selected correlation: x^2 e^{-x} / range (3/2), x^2 (1 + x) e^{-x} / (3 range)
+    (5/2).  No counterpart in the reference (it has no gradient code)."""
+    if NU == 2.5:
+        x = SQRT5 * h / rng
+        return x * x * (1.0 + x) * np.exp(-x) / (3.0 * rng)
+    x = SQRT3 * h / rng
+    return x * x * np.exp(-x) / rng
+
+
 def morton_order(xy, order=10):
     """Z-order permutation of points in the unit square.
 
@@ -65,7 +101,7 @@ def pairwise_dist(A, B):
 def cov_dense(S, theta):
     """Dense covariance sigma2 * M + sigma2 * eta * I.  codes/11_tlr_rank_rules.py:61-65."""
     sigma2, rng, eta = theta
-    K = sigma2 * matern32(pairwise_dist(S, S), rng)
+    K = sigma2 * matern(pairwise_dist(S, S), rng)
     K[np.diag_indices_from(K)] += sigma2 * eta
     return K
 
@@ -166,12 +202,12 @@ def tlr_cholesky(S, theta, bounds, rule, value, rank_log=None, frozen=None):
     A_off = {}
     stored0 = 0
     for i, (i0, i1) in enumerate(bounds):
-        D = sigma2 * matern32(pairwise_dist(S[i0:i1], S[i0:i1]), rng)
+        D = sigma2 * matern(pairwise_dist(S[i0:i1], S[i0:i1]), rng)
         D[np.diag_indices_from(D)] += nugget
         A_diag.append(D)
         stored0 += (i1 - i0) ** 2
         for j, (j0, j1) in enumerate(bounds[:i]):
-            T = sigma2 * matern32(pairwise_dist(S[i0:i1], S[j0:j1]), rng)
+            T = sigma2 * matern(pairwise_dist(S[i0:i1], S[j0:j1]), rng)
             U, V, _, r = truncate_svd(T, rule, thr_rel, thr_abs, pick(("init", i, j)))
             if rank_log is not None:
                 rank_log[("init", i, j)] = r
@@ -269,7 +305,7 @@ def tlr_backward(L_diag, L_off, bounds, Z):
 def tlr_predict(S, y, Sp, theta, bounds, fac):
     """Kriging mean and standard deviation with the tile factor.  codes/17_tlr_cholesky_pilot.py:269-276."""
     L_diag, L_off = fac
-    Kp = theta[0] * matern32(pairwise_dist(Sp, S), theta[1])
+    Kp = theta[0] * matern(pairwise_dist(Sp, S), theta[1])
     alpha = tlr_backward(L_diag, L_off, bounds, tlr_forward(L_diag, L_off, bounds, y[:, None]))[:, 0]
     mu = Kp @ alpha
     W = tlr_forward(L_diag, L_off, bounds, Kp.T)
@@ -303,15 +339,14 @@ def tlr_loglik(S, y, theta, bounds, rule, value, rank_log=None, frozen=None):
 
 
 def matern32_dtheta(S, bounds, theta, i, j):
-    """(dSigma/dsigma2, dSigma/drange, dSigma/deta) of tile (i, j): Sigma/sigma2 (+ eta I on the
-    diagonal), sigma2 x^2 e^{-x} / range with x = sqrt(3) h / range, and sigma2 I on the diagonal.
-    No counterpart in the reference (it has no gradient code)."""
+    """(dSigma/dsigma2, dSigma/drange, dSigma/deta) of tile (i, j) for the selected kernel:
+    Sigma/sigma2 (+ eta I on the diagonal), sigma2 dk/drange (matern_drange), and sigma2 I on the
+    diagonal.  No counterpart in the reference (it has no gradient code)."""
     sigma2, rng, eta = theta
     (i0, i1), (j0, j1) = bounds[i], bounds[j]
-    x = SQRT3 * pairwise_dist(S[i0:i1], S[j0:j1]) / rng
-    e = np.exp(-x)
-    ds = (1.0 + x) * e
-    dr = sigma2 * x * x * e / rng
+    h = pairwise_dist(S[i0:i1], S[j0:j1])
+    ds = matern(h, rng)
+    dr = sigma2 * matern_drange(h, rng)
     de = np.zeros_like(ds)
     if i == j:
         ds[np.diag_indices_from(ds)] += eta
@@ -400,12 +435,11 @@ def dense_loglik_and_grad(S, y, theta):
     """Dense FP64 log-likelihood and its gradient in (sigma2, range, eta).
 
     dl/dtheta = 1/2 alpha^T dK alpha - 1/2 tr(K^{-1} dK), alpha = K^{-1} y, with
-    dK/dsigma2 = K/sigma2, dK/drange = sigma2 x^2 e^{-x} / range (x = sqrt3 h/range),
+    dK/dsigma2 = K/sigma2, dK/drange = sigma2 dk/drange of the selected kernel (matern_drange),
     dK/deta = sigma2 I.  No counterpart in the reference (it has no gradient code)."""
     sigma2, rng, eta = theta
     H = pairwise_dist(S, S)
-    x = SQRT3 * H / rng
-    M = (1.0 + x) * np.exp(-x)
+    M = matern(H, rng)
     K = sigma2 * M
     K[np.diag_indices_from(K)] += sigma2 * eta
     c = cholesky(K, lower=True, check_finite=False)
@@ -415,7 +449,7 @@ def dense_loglik_and_grad(S, y, theta):
     Kinv = Ci.T @ Ci
     ll = -0.5 * (z @ z + 2.0 * np.log(np.diag(c)).sum() + len(y) * LOG2PI)
     dKs = M + eta * np.eye(len(y))
-    dKr = sigma2 * x * x * np.exp(-x) / rng
+    dKr = sigma2 * matern_drange(H, rng)
     grads = []
     for dK in (dKs, dKr, None):
         if dK is None:

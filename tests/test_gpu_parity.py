@@ -118,3 +118,41 @@ def test_tile_sizes_outside_tensor_core_forms(tlr, data, n, b, rule, value, tol)
     if info_o["completed"]:
         assert list(ev.factor_ranks) == list(info_o["factor_ranks"])
         assert abs(ev.loglik - ll_o) <= tol * abs(ll_o)
+
+
+@pytest.mark.parametrize("case", ["n1030_b100", "n4000_b250"])
+def test_matern52_matches_reference(tlr, case):
+    """nu = 2.5 (codes/24_screening_stress.py's kernel inside 17's TLR Cholesky): the reference's
+    ranks, stored values and log-likelihoods (golden_nu52.json); gradient and kriging against the
+    oracle with the same kernel."""
+    gold = {c["name"]: c for c in json.load(open(os.path.join(GOLD, "golden_nu52.json")))["cases"]}[case]
+    d = np.load(os.path.join(GOLD, gold["data"]))
+    S, y = d["S"], d["y"]
+    bounds = tlr.tile_bounds(gold["n"], gold["b"])
+    plan = tlr.get_plan(gold["n"], gold["b"])
+    tlr.set_kernel(2.5)
+    O.set_kernel(2.5)
+    try:
+        for rec in gold["rules"]:
+            ev = plan.evaluate(gold["theta"], rec["rule"], rec["value"], host_S=S, host_y=y)
+            assert list(ev.sigma_ranks) == rec["sigma_ranks"], (rec["rule"], rec["value"])
+            assert ev.info["completed"] == rec["completed"]
+            assert list(ev.factor_ranks) == rec["factor_ranks"]
+            assert ev.info["stored_factor"] == rec["stored_factor"]
+            assert abs(ev.loglik - rec["loglik"]) <= REL_TOL * abs(rec["loglik"]), (ev.loglik, rec["loglik"])
+        rule, value = "adaptive", 0.9
+        ll, g, _ = tlr.tlr_loglik_grad(S, y, gold["theta"], bounds, rule, value)
+        ll_o, g_o, _ = O.tlr_loglik_grad(S, y, gold["theta"], bounds, rule, value)
+        assert abs(ll - ll_o) <= REL_TOL * abs(ll_o)
+        np.testing.assert_allclose(g, g_o, rtol=1e-8, atol=1e-8 * np.abs(g_o).max())
+        if case == "n1030_b100":
+            Sp = np.random.default_rng(7).random((50, 2))
+            _, fac, _ = tlr.tlr_loglik(S, y, gold["theta"], bounds, rule, value)
+            mu, sd = tlr.tlr_predict(S, y, Sp, gold["theta"], bounds, fac)
+            _, fac_o, _ = O.tlr_loglik(S, y, gold["theta"], bounds, rule, value)
+            mu_o, sd_o = O.tlr_predict(S, y, Sp, gold["theta"], bounds, fac_o)
+            np.testing.assert_allclose(mu, mu_o, rtol=1e-9, atol=1e-10)
+            np.testing.assert_allclose(sd, sd_o, rtol=1e-9, atol=1e-10)
+    finally:
+        tlr.set_kernel(1.5)
+        O.set_kernel(1.5)

@@ -117,3 +117,26 @@ def test_oracle_prediction_matches_reference():
     sk = O.skill(f["yp"], f["mu"], f["sd"])
     assert abs(sk["rmse"] - float(f["rmse"])) <= 1e-12 and abs(sk["crps"] - float(f["crps"])) <= 1e-12
     assert sk["cover90"] == float(f["cover90"])
+
+
+@pytest.mark.parametrize("case", ["n1030_b100", "n4000_b250"])
+def test_oracle_matern52_matches_reference(case):
+    """With nu = 2.5 (the kernel codes/24_screening_stress.py patches into 17) the oracle gives the
+    reference's ranks, stored values, TLR and dense log-likelihoods (golden_nu52.json)."""
+    gold = {c["name"]: c for c in json.load(open(os.path.join(GOLD, "golden_nu52.json")))["cases"]}[case]
+    d = np.load(os.path.join(GOLD, gold["data"]))
+    S, y = d["S"], d["y"]
+    bounds = O.tile_bounds(gold["n"], gold["b"])
+    O.set_kernel(2.5)
+    try:
+        for rec in gold["rules"]:
+            ll, _, info = O.tlr_loglik(S, y, gold["theta"], bounds, rec["rule"], rec["value"])
+            assert info["sigma_ranks"] == rec["sigma_ranks"]
+            assert info["completed"] == rec["completed"]
+            assert info["factor_ranks"] == rec["factor_ranks"]
+            assert info["stored_factor"] == rec["stored_factor"]
+            assert abs(ll - rec["loglik"]) <= 1e-10 * abs(rec["loglik"])
+        ll_d, _ = O.loglik_dense(O.cov_dense(S, gold["theta"]), y)
+        assert abs(ll_d - gold["dense_loglik"]) <= 1e-10 * abs(gold["dense_loglik"])
+    finally:
+        O.set_kernel(1.5)
