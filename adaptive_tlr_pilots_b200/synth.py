@@ -2,7 +2,8 @@
 
 codes/17_tlr_cholesky_pilot.py:313-325: S_all uniform on the unit square, y_all = L z with L the
 dense FP64 Cholesky of Sigma(S_all; theta), a random split into N observed and n_pred held-out
-sites, Morton order of the observed sites.  The random numbers come from numpy's
+sites, Morton order of the observed sites (the kernel chosen by tlr.set_kernel, as the reference's
+sweeps simulate with the kernel they patch in, codes/24_screening_stress.py:58-59).  The random numbers come from numpy's
 default_rng(seed) in the same order as the reference; the dense Cholesky and the product L z run
 on the GPU in FP64 (cuSOLVER/cuBLAS through torch), which lets N go past the size where a CPU
 LAPACK Cholesky of the (N + n_pred)^2 matrix fails (more than 2^31 entries).  This is data
@@ -11,6 +12,22 @@ generation, not part of the likelihood path.
 from __future__ import annotations
 
 import numpy as np
+
+
+def _matern_inplace(K, rg, sigma2):
+    """K (distances) <- sigma2 k(K / range) in place for the kernel chosen by tlr.set_kernel."""
+    import torch
+
+    from .tlr import get_kernel
+    if get_kernel() == 2.5:  # (1 + x + x^2 / 3) e^{-x}, x = sqrt(5) h / range (24:38-42)
+        K.mul_((5.0 ** 0.5) / rg)
+        E = torch.exp(-K)
+        K.mul_(K.div(3.0).add_(1.0)).add_(1.0).mul_(E).mul_(sigma2)
+    else:
+        K.mul_((3.0 ** 0.5) / rg)
+        E = torch.exp(-K)
+        K.add_(1.0).mul_(E).mul_(sigma2)
+    del E
 
 
 def simulate_field(n, theta=(1.0, 0.3, 0.05), n_pred=300, seed=20261020, device=0, order_fn=None):
@@ -32,10 +49,7 @@ def simulate_field(n, theta=(1.0, 0.3, 0.05), n_pred=300, seed=20261020, device=
     with torch.no_grad():
         St = torch.as_tensor(S_all, device=dev)
         K = torch.cdist(St, St)
-        K.mul_((3.0 ** 0.5) / rg)
-        E = torch.exp(-K)
-        K.add_(1.0).mul_(E).mul_(sigma2)
-        del E
+        _matern_inplace(K, rg, sigma2)
         K.diagonal().add_(sigma2 * eta)
         L, info = torch.linalg.cholesky_ex(K)
         del K
@@ -62,6 +76,8 @@ def dense_loglik_grad_gpu(S, y, theta, device=0, chunk=4096):
     (cuSOLVER Cholesky and inverse through torch; dSigma in row blocks): the dense oracle for the
     gradient at sizes where a CPU Cholesky fails.  Returns (ll, grad) or (None, None)."""
     import torch
+
+    from .tlr import get_kernel
     dev = torch.device("cuda", device)
     sigma2, rg, eta = [float(v) for v in theta]
     with torch.no_grad():
@@ -69,10 +85,7 @@ def dense_loglik_grad_gpu(S, y, theta, device=0, chunk=4096):
         yt = torch.as_tensor(np.asarray(y, dtype=np.float64), device=dev)
         n = St.shape[0]
         K = torch.cdist(St, St)
-        K.mul_((3.0 ** 0.5) / rg)
-        E = torch.exp(-K)
-        K.add_(1.0).mul_(E).mul_(sigma2)
-        del E
+        _matern_inplace(K, rg, sigma2)
         K.diagonal().add_(sigma2 * eta)
         L, info = torch.linalg.cholesky_ex(K)
         del K
@@ -86,11 +99,16 @@ def dense_loglik_grad_gpu(S, y, theta, device=0, chunk=4096):
         g = np.zeros(3)
         for r0 in range(0, n, chunk):
             r1 = min(n, r0 + chunk)
-            x = torch.cdist(St[r0:r1], St) * ((3.0 ** 0.5) / rg)
+            nu5 = get_kernel() == 2.5
+            x = torch.cdist(St[r0:r1], St) * (((5.0 if nu5 else 3.0) ** 0.5) / rg)
             e = torch.exp(-x)
             W = 0.5 * (alpha[r0:r1, None] * alpha[None, :] - Kinv[r0:r1])
-            g[0] += float(((1.0 + x) * e * W).sum())
-            g[1] += float((sigma2 * x * x * e / rg * W).sum())
+            if nu5:
+                g[0] += float(((1.0 + x + x * x / 3.0) * e * W).sum())
+                g[1] += float((sigma2 * x * x * (1.0 + x) / 3.0 * e / rg * W).sum())
+            else:
+                g[0] += float(((1.0 + x) * e * W).sum())
+                g[1] += float((sigma2 * x * x * e / rg * W).sum())
             del x, e
             idx = torch.arange(r0, r1, device=dev)
             wd = W[idx - r0, idx]

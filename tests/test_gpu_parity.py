@@ -156,3 +156,25 @@ def test_matern52_matches_reference(tlr, case):
     finally:
         tlr.set_kernel(1.5)
         O.set_kernel(1.5)
+
+
+def test_matern52_dense_helpers_match_oracle(tlr):
+    """The GPU dense log-likelihood and gradient (the dense oracle at large N) follow the kernel
+    switch: against the CPU dense FP64 formula with nu = 2.5."""
+    from adaptive_tlr_pilots_b200 import synth
+    d = np.load(os.path.join(GOLD, "n1030_b100_data.npz"))
+    S, y = d["S"], d["y"]
+    theta = (1.0, 0.3, 0.05)
+    tlr.set_kernel(2.5)
+    O.set_kernel(2.5)
+    try:
+        ll_o, g_o = O.dense_loglik_and_grad(S, y, theta)
+        ll = tlr.dense_loglik(S, y, theta)
+        ll2, g = synth.dense_loglik_grad_gpu(S, y, theta)
+        assert abs(ll - ll_o) <= 1e-10 * abs(ll_o) and abs(ll2 - ll_o) <= 1e-10 * abs(ll_o)
+        np.testing.assert_allclose(g, g_o, rtol=1e-8, atol=1e-8 * np.abs(g_o).max())
+        S2, y2, _, _ = synth.simulate_field(600, theta)   # simulation with the same kernel runs
+        assert np.isfinite(y2).all() and S2.shape == (600, 2)
+    finally:
+        tlr.set_kernel(1.5)
+        O.set_kernel(1.5)
