@@ -5,7 +5,8 @@
 // the selected-inversion gradient within ~1e-5 of the FP64 one (single-pass TF32 loses ~1e-2 on
 // the range component).
 //
-// One CTA of 256 threads computes a 128 x N_TILE output tile (N_TILE = 128): the accumulator is
+// One CTA of 512 threads (four per row of the tile, so that sixteen warps share the conversion
+// latency) computes a 128 x N_TILE output tile (N_TILE = 128): the accumulator is
 // 128 TMEM lanes x 128 columns.  K advances in slices of 32: every thread converts and splits its
 // share of the FP64 slice into shared memory in the canonical K-major, no-swizzle UMMA layout
 // (core matrices of 8 rows x 16 bytes; rows of a core matrix 16 B apart, 8-row groups 128 B
@@ -26,6 +27,8 @@ constexpr int kTcM = 128;
 constexpr int kTcN = 128;
 constexpr int kTcBK = 32;
 constexpr int kTcStages = 2;
+constexpr int kTcThreads = 512;                   // 4 threads per row of a 128-row slice
+constexpr int kTcPerThread = kTcBK * 2 / (kTcThreads / kTcM) / 2;  // k values of A (and of B) per thread: 8
 // bytes per stage: A_hi, A_lo (128 x 32 x 4), B_hi, B_lo (128 x 32 x 4)
 constexpr int kTcStageBytes = 4 * kTcM * kTcBK * 4;
 constexpr long long kTcWaitLimit = 1ll << 23;  // polls of about 140 ns on B200: about 1.2 s
@@ -118,7 +121,7 @@ __global__ void k_wait_selftest(long long limit, int* status) {
   if (tid == 0) *status = ok ? 0 : -7;
 }
 
-__global__ void __launch_bounds__(256) k_gemm_tc3(const GemmJob* TLR_RESTRICT jobs, int* TLR_RESTRICT status,
+__global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc3(const GemmJob* TLR_RESTRICT jobs, int* TLR_RESTRICT status,
                                                  int kind) {
   if (*status != 0) return;
   const GemmJob jb = jobs[blockIdx.z];
@@ -147,14 +150,14 @@ __global__ void __launch_bounds__(256) k_gemm_tc3(const GemmJob* TLR_RESTRICT jo
   const uint32_t idesc = umma_idesc_tf32(kTcM, kTcN);
   const int nk = (jb.K + kTcBK - 1) / kTcBK;
   int fail = 0;
-  // global -> registers for slice `it`: thread -> (row r = tid / 2, K groups (tid & 1) * 4 .. + 3
-  // of 4 consecutive k each), all 16 loads of A and of B issued before any of them is used
-  auto gload = [&](int it, double (&va)[16], double (&vb)[16]) {
+  // global -> registers for slice `it`: thread -> (row r = tid / 4, K groups (tid & 3) * 2 .. + 1
+  // of 4 consecutive k each), all 8 loads of A and of B issued before any of them is used
+  auto gload = [&](int it, double (&va)[kTcPerThread], double (&vb)[kTcPerThread]) {
     const int k0 = it * kTcBK;
-    const int r = tid >> 1, gh = (tid & 1) * 4;
+    const int r = tid >> 2, gh = (tid & 3) * 2;
     const int gma = m0 + r, gnb = n0 + r;
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
+    for (int q = 0; q < kTcPerThread; ++q) {
       const int gk = k0 + gh * 4 + q;
       va[q] = (gma < jb.M && gk < jb.K)
                   ? (jb.transA ? jb.A[(size_t)gma * jb.lda + gk] : jb.A[(size_t)gk * jb.lda + gma])
@@ -166,7 +169,7 @@ __global__ void __launch_bounds__(256) k_gemm_tc3(const GemmJob* TLR_RESTRICT jo
   };
   // registers of slice `it` -> its shared-memory stage (split TF32, each group of 4 as one 16-byte
   // store), then thread 0 issues the slice's MMAs; false (in every thread) on a timed-out wait
-  auto stage_in = [&](int it, const double (&va)[16], const double (&vb)[16]) -> bool {
+  auto stage_in = [&](int it, const double (&va)[kTcPerThread], const double (&vb)[kTcPerThread]) -> bool {
     const int st = it & 1;
     unsigned char* sbase = tc_smem + st * kTcStageBytes;
     float* Ahi = reinterpret_cast<float*>(sbase);
@@ -180,9 +183,9 @@ __global__ void __launch_bounds__(256) k_gemm_tc3(const GemmJob* TLR_RESTRICT jo
     }
     if (__syncthreads_or(bad)) return false;
     {
-      const int r = tid >> 1, gh = (tid & 1) * 4;
+      const int r = tid >> 2, gh = (tid & 3) * 2;
 #pragma unroll
-      for (int g = 0; g < 4; ++g) {
+      for (int g = 0; g < kTcPerThread / 4; ++g) {
         float4 ah, al, bh, bl;
         float* pah = &ah.x; float* pal = &al.x; float* pbh = &bh.x; float* pbl = &bl.x;
 #pragma unroll
@@ -222,7 +225,7 @@ __global__ void __launch_bounds__(256) k_gemm_tc3(const GemmJob* TLR_RESTRICT jo
     return true;
   };
   // two register sets: the loads of slice it + 1 are in flight while slice it is converted
-  double a0[16], b0[16], a1[16], b1[16];
+  double a0[kTcPerThread], b0[kTcPerThread], a1[kTcPerThread], b1[kTcPerThread];
   if (nk > 0) gload(0, a0, b0);
   for (int it = 0; it < nk; it += 2) {
     if (it + 1 < nk) gload(it + 1, a1, b1);
@@ -247,10 +250,11 @@ __global__ void __launch_bounds__(256) k_gemm_tc3(const GemmJob* TLR_RESTRICT jo
   asm volatile("tcgen05.fence::after_thread_sync;");
   const bool ok = !timed_out;
   if (ok) {
-    const int quarter = warp & 3, half = warp >> 2;
+    // warp w reads TMEM lane quarter w % 4 (the lanes a warp may access) and column quarter w / 4
+    const int quarter = warp & 3, part = warp >> 2, nparts = kTcThreads / 128;
     const int row = quarter * 32 + lane;
     const int gm = m0 + row;
-    for (int c0 = half * (kTcN / 2); c0 < (half + 1) * (kTcN / 2); c0 += 8) {
+    for (int c0 = part * (kTcN / nparts); c0 < (part + 1) * (kTcN / nparts); c0 += 8) {
       uint32_t r[8];
       const uint32_t taddr = tmem_d + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0;
       asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
@@ -296,7 +300,7 @@ int launch_gemm_tc3(const GemmJob* jobs, int njobs, int max_m, int max_n, int* s
   const size_t sm = (size_t)kTcStages * kTcStageBytes + 1024;
   cudaFuncSetAttribute(k_gemm_tc3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   dim3 grid((unsigned)((max_n + kTcN - 1) / kTcN), (unsigned)((max_m + kTcM - 1) / kTcM), (unsigned)njobs);
-  k_gemm_tc3<<<grid, 256, sm, s>>>(jobs, status, kind);
+  k_gemm_tc3<<<grid, kTcThreads, sm, s>>>(jobs, status, kind);
   return (int)cudaGetLastError();
 }
 
