@@ -74,6 +74,10 @@ SIGNATURES = {
                                              ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int]),
     "tlr_selftest_bounded_wait": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                                  ctypes.POINTER(ctypes.c_longlong)]),
+    "tlr_selftest_gemm": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_int,
+                                         ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_void_p,
+                                         ctypes.c_int, ctypes.c_int]),
     "tlr_last_error": (ctypes.c_char_p, []),
 }
 

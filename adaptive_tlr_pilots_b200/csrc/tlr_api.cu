@@ -7,6 +7,7 @@
 #include "../../include/tlr_b200.h"
 #include "tlr_kernels.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -256,6 +257,16 @@ int grow(T** ptr, size_t* cap, size_t need) {
   return 0;
 }
 
+// 1 when every job's A and B start on 16 bytes and have even leading dimensions, so that the
+// tensor-core GEMM may copy its operands two doubles at a time
+static int tc_aligned16(const tlr::GemmJob* j, int count) {
+  for (int q = 0; q < count; ++q)
+    if ((reinterpret_cast<uintptr_t>(j[q].A) & 15) || (reinterpret_cast<uintptr_t>(j[q].B) & 15) || (j[q].lda & 1) ||
+        (j[q].ldb & 1))
+      return 0;
+  return 1;
+}
+
 struct LaunchRange {
   int kind;      // 0 gemm, 1 copy, 2 alpha, 3 dtrace, 4 gemm that stays FP64 in mixed mode
   size_t first;  // index of the first job
@@ -440,9 +451,11 @@ int run_backward(tlr_plan* p, double sigma2, double inv_range, double eta) {
       LAUNCH(TLR_K_BWD_GEMM, tlr::launch_dgemm_batched(p->d_jobs + L.first, L.count, L.max_m, L.max_n, p->status,
                                                         TLR_K_BWD_GEMM, s));
     } else if (L.kind == 0) {
-      if (p->precision == TLR_PRECISION_MIXED)
-        LAUNCH(TLR_K_BWD_GEMM, tlr::launch_gemm_tc3(p->d_jobs + L.first, L.count, L.max_m, L.max_n, p->status,
+      if (p->precision == TLR_PRECISION_MIXED) {
+        const int al = tc_aligned16(jobs.data() + L.first, L.count);
+        LAUNCH(TLR_K_BWD_GEMM, tlr::launch_gemm_tc3(p->d_jobs + L.first, L.count, L.max_m, L.max_n, al, p->status,
                                                      TLR_K_BWD_GEMM, s));
+      }
       else
         LAUNCH(TLR_K_BWD_GEMM, tlr::launch_dgemm_batched(p->d_jobs + L.first, L.count, L.max_m, L.max_n, p->status,
                                                           TLR_K_BWD_GEMM, s));
@@ -877,6 +890,41 @@ int tlr_selftest_bounded_wait(long long iterations, int device, double* elapsed_
   }
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
+  if (s) cudaStreamDestroy(s);
+  if (d) cudaFree(d);
+  if (rc) return rc;
+  if (h == TLR_ERR_TIMEOUT) return fail(TLR_ERR_TIMEOUT, "a device wait ran out of its iteration limit");
+  return h;
+}
+
+int tlr_selftest_gemm(int precision, int transA, int transB, int M, int N, int K, double alpha, const double* A,
+                      int lda, const double* B, int ldb, double beta, double* C, int ldc, int device) {
+  if (precision != TLR_PRECISION_FP64 && precision != TLR_PRECISION_MIXED) return fail(TLR_ERR_ARG, "unknown precision");
+  if (M < 0 || N < 0 || K < 0) return fail(TLR_ERR_ARG, "negative size");
+  if (lda < std::max(1, transA ? K : M) || ldb < std::max(1, transB ? N : K) || ldc < std::max(1, M))
+    return fail(TLR_ERR_ARG, "leading dimension too small");
+  if ((M && N && !C) || (M && N && K && (!A || !B))) return fail(TLR_ERR_ARG, "NULL matrix");
+  if (M == 0 || N == 0) return 0;
+  int rc = cuda_check(cudaSetDevice(device), "set device");
+  if (rc) return rc;
+  const size_t status_bytes = sizeof(int) * (4 + 4 * TLR_NKINDS);
+  unsigned char* d = nullptr;
+  cudaStream_t s = nullptr;
+  int h = 0;
+  tlr::GemmJob j{A, B, C, nullptr, lda, ldb, ldc, M, N, K, transA ? 1 : 0, transB ? 1 : 0, alpha, beta};
+  rc = cuda_check(cudaMalloc(&d, 256 + status_bytes), "self-test buffers");
+  tlr::GemmJob* dj = reinterpret_cast<tlr::GemmJob*>(d);
+  int* st = reinterpret_cast<int*>(d + 256);
+  if (!rc) rc = cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+  if (!rc) rc = cuda_check(cudaMemsetAsync(st, 0, status_bytes, s), "status");
+  if (!rc) rc = cuda_check(cudaMemcpyAsync(dj, &j, sizeof(j), cudaMemcpyHostToDevice, s), "job");
+  if (!rc)
+    rc = cuda_check((cudaError_t)(precision == TLR_PRECISION_MIXED
+                                      ? tlr::launch_gemm_tc3(dj, 1, M, N, tc_aligned16(&j, 1), st, TLR_K_BWD_GEMM, s)
+                                      : tlr::launch_dgemm_batched(dj, 1, M, N, st, TLR_K_BWD_GEMM, s)),
+                    "self-test launch");
+  if (!rc) rc = cuda_check(cudaMemcpyAsync(&h, st, sizeof(int), cudaMemcpyDeviceToHost, s), "status copy");
+  if (!rc) rc = cuda_check(cudaStreamSynchronize(s), "self-test");
   if (s) cudaStreamDestroy(s);
   if (d) cudaFree(d);
   if (rc) return rc;

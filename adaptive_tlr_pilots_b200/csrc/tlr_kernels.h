@@ -70,7 +70,9 @@ struct CopyJob {
 };
 int launch_dgemm_batched(const GemmJob* jobs, int njobs, int max_m, int max_n, const int* status, int kind,
                          cudaStream_t s);
-int launch_gemm_tc3(const GemmJob* jobs, int njobs, int max_m, int max_n, int* status, int kind, cudaStream_t s);
+// aligned16: every job's A and B start 16-byte aligned with even lda and ldb (16-byte copies)
+int launch_gemm_tc3(const GemmJob* jobs, int njobs, int max_m, int max_n, int aligned16, int* status, int kind,
+                    cudaStream_t s);
 // the bounded-wait self-test (tlr_tc.cu) and the iteration limit of the GEMM's waits
 int launch_wait_selftest(long long limit, int* status, cudaStream_t s);
 long long tc_wait_limit();

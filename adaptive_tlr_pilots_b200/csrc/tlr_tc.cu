@@ -5,17 +5,22 @@
 // the selected-inversion gradient within ~1e-5 of the FP64 one (single-pass TF32 loses ~1e-2 on
 // the range component).
 //
-// One CTA of 512 threads (four per row of the tile, so that sixteen warps share the conversion
-// latency) computes a 128 x N_TILE output tile (N_TILE = 128): the accumulator is
-// 128 TMEM lanes x 128 columns.  K advances in slices of 32: every thread converts and splits its
-// share of the FP64 slice into shared memory in the canonical K-major, no-swizzle UMMA layout
-// (core matrices of 8 rows x 16 bytes; rows of a core matrix 16 B apart, 8-row groups 128 B
-// apart, the two 16-byte K halves of one MMA 2048 B apart for A), fences the generic-proxy writes
-// for the async proxy, and thread 0 issues 4 K-steps x 3 tcgen05.mma.kind::tf32 and commits them
-// to the stage's mbarrier.  Two stages alternate, so the conversion of slice s+1 overlaps the MMAs
-// of slice s, and the global loads of slice s+1 are issued (into a second register set) before
-// slice s is converted, so their latency overlaps that work.  Waits on the mbarriers are bounded: on timeout the kernel sets an error status,
-// frees its tensor memory and returns.
+// One CTA of 512 threads computes a 128 x N_TILE output tile (N_TILE = 128): the accumulator is
+// 128 TMEM lanes x 128 columns.  K advances in slices of 16 through a ring of six shared-memory
+// stages.  Each stage first receives the raw FP64 slice of A and of B by cp.async (16-byte copies
+// when every row start is 16-byte aligned, else 8-byte; rows and k beyond the matrix arrive as
+// zeros), five slices ahead of the one being converted, so the copies' latency hides behind the
+// conversion and the MMAs of the slices before.  The threads then read their four k values of
+// one tile row (thread = row + 128 x k-group), and, after a block barrier, overwrite the same
+// stage with the split TF32 values in the canonical K-major, no-swizzle UMMA layout (core
+// matrices of 8 rows x 16 bytes; rows of a core matrix 16 B apart, 8-row groups 128 B apart, the
+// two 16-byte K halves of one MMA 2048 B apart): a double and its (hi, lo) pair take the same 8
+// bytes, so the conversion fits in place.  After a fence for the async proxy and a barrier,
+// thread 0 issues 2 K-steps x 3 tcgen05.mma.kind::tf32 and commits them to the stage's mbarrier;
+// the stage is refilled once that commit completes.  The MMA sequence (K-steps of 8 in order,
+// three products each) is the same for any slice length, so results do not depend on it.
+// Waits on the mbarriers are bounded: on timeout the kernel sets an error status, lets its copies
+// land, frees its tensor memory and returns.
 #include <stdint.h>
 
 #include "tlr_device.cuh"
@@ -25,12 +30,14 @@ namespace tlr {
 
 constexpr int kTcM = 128;
 constexpr int kTcN = 128;
-constexpr int kTcBK = 32;
-constexpr int kTcStages = 2;
-constexpr int kTcThreads = 512;                   // 4 threads per row of a 128-row slice
-constexpr int kTcPerThread = kTcBK * 2 / (kTcThreads / kTcM) / 2;  // k values of A (and of B) per thread: 8
-// bytes per stage: A_hi, A_lo (128 x 32 x 4), B_hi, B_lo (128 x 32 x 4)
-constexpr int kTcStageBytes = 4 * kTcM * kTcBK * 4;
+constexpr int kTcBK = 16;                          // k per slice: two MMA K-steps
+constexpr int kTcStages = 6;
+constexpr int kTcThreads = 512;                    // thread = tile row (0..127) + 128 x k-group (0..3)
+constexpr int kTcRawKS = kTcBK + 2;                // row stride (doubles) of a k-contiguous raw slice
+constexpr int kTcOpBytes = kTcM * kTcRawKS * 8;    // one operand's region: 18,432 B >= 16 KB of hi + lo
+constexpr int kTcStageBytes = 2 * kTcOpBytes;      // A region, then B region
+static_assert(kTcM == kTcN && kTcThreads == 4 * kTcM && kTcBK == 16, "thread map assumes 128 x 128 x 16");
+static_assert(kTcStageBytes * kTcStages + 1024 <= 227 * 1024, "stages exceed shared memory");
 constexpr long long kTcWaitLimit = 1ll << 23;  // polls of about 140 ns on B200: about 1.2 s
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -121,6 +128,74 @@ __global__ void k_wait_selftest(long long limit, int* status) {
   if (tid == 0) *status = ok ? 0 : -7;
 }
 
+// One operand's raw FP64 slice global -> shared by cp.async: 128 tile rows x 16 k from row0 and
+// k0, zeros beyond `rows` and K.  kcont: k is the contiguous index in global memory (element
+// (row, k) at X[row * ld + k]); the slice is then stored [row][kTcRawKS], else [k][128] (element
+// at X[k * ld + row]).  VEC doubles per copy (2: X and ld keep every copy 16-byte aligned).
+template <int VEC>
+__device__ __forceinline__ void tc_load_slice(double* raw, const double* X, int ld, int rows, int row0, int K, int k0,
+                                              int kcont, int tid) {
+  constexpr int kChunks = kTcM * kTcBK / VEC;
+#pragma unroll
+  for (int i = 0; i < kChunks / kTcThreads; ++i) {
+    const int q = tid + i * kTcThreads;
+    int row, k, nv;
+    const double* src;
+    double* dst;
+    if (kcont) {
+      row = q / (kTcBK / VEC);
+      k = (q % (kTcBK / VEC)) * VEC;
+      nv = row0 + row < rows ? min(VEC, K - (k0 + k)) : 0;
+      src = X + (size_t)(row0 + row) * ld + (k0 + k);
+      dst = raw + row * kTcRawKS + k;
+    } else {
+      k = q / (kTcM / VEC);
+      row = (q % (kTcM / VEC)) * VEC;
+      nv = k0 + k < K ? min(VEC, rows - (row0 + row)) : 0;
+      src = X + (size_t)(k0 + k) * ld + (row0 + row);
+      dst = raw + k * kTcM + row;
+    }
+    if (nv <= 0) {  // nothing to read: zeros, from a valid address
+      nv = 0;
+      src = X;
+    }
+    if (VEC == 2) cp_async16(dst, src, nv * 8);
+    else cp_async8(dst, src, nv * 8);
+  }
+}
+
+// k values 4g .. 4g + 3 of tile row r from a raw slice
+__device__ __forceinline__ void tc_read4(const double* raw, int kcont, int r, int g, double (&x)[4]) {
+  if (kcont) {
+    const double2 u = *reinterpret_cast<const double2*>(raw + r * kTcRawKS + 4 * g);
+    const double2 v = *reinterpret_cast<const double2*>(raw + r * kTcRawKS + 4 * g + 2);
+    x[0] = u.x;
+    x[1] = u.y;
+    x[2] = v.x;
+    x[3] = v.y;
+  } else {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) x[c] = raw[(4 * g + c) * kTcM + r];
+  }
+}
+
+// split x = hi + lo (both TF32) and store them in the UMMA layout: hi at `out`, lo 8 KB after
+__device__ __forceinline__ void tc_write4(float* out, const double (&x)[4], int r, int g) {
+  float4 h, l;
+  float* ph = &h.x;
+  float* pl = &l.x;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const float f = (float)x[c];
+    const float fh = __uint_as_float(to_tf32(f));
+    ph[c] = fh;
+    pl[c] = __uint_as_float(to_tf32(f - fh));
+  }
+  *reinterpret_cast<float4*>(out + g * (kTcM * 4) + r * 4) = h;
+  *reinterpret_cast<float4*>(out + kTcM * kTcBK + g * (kTcM * 4) + r * 4) = l;
+}
+
+template <int VEC>
 __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc3(const GemmJob* TLR_RESTRICT jobs, int* TLR_RESTRICT status,
                                                  int kind) {
   if (*status != 0) return;
@@ -149,101 +224,71 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc3(const GemmJob* TLR_R
   const uint32_t tmem_d = tmem_base_sh;
   const uint32_t idesc = umma_idesc_tf32(kTcM, kTcN);
   const int nk = (jb.K + kTcBK - 1) / kTcBK;
-  int fail = 0;
-  // global -> registers for slice `it`: thread -> (row r = tid / 4, K groups (tid & 3) * 2 .. + 1
-  // of 4 consecutive k each), all 8 loads of A and of B issued before any of them is used
-  auto gload = [&](int it, double (&va)[kTcPerThread], double (&vb)[kTcPerThread]) {
-    const int k0 = it * kTcBK;
-    const int r = tid >> 2, gh = (tid & 3) * 2;
-    const int gma = m0 + r, gnb = n0 + r;
-#pragma unroll
-    for (int q = 0; q < kTcPerThread; ++q) {
-      const int gk = k0 + gh * 4 + q;
-      va[q] = (gma < jb.M && gk < jb.K)
-                  ? (jb.transA ? jb.A[(size_t)gma * jb.lda + gk] : jb.A[(size_t)gk * jb.lda + gma])
-                  : 0.0;
-      vb[q] = (gnb < jb.N && gk < jb.K)
-                  ? (jb.transB ? jb.B[(size_t)gk * jb.ldb + gnb] : jb.B[(size_t)gnb * jb.ldb + gk])
-                  : 0.0;
+  const int kcA = jb.transA ? 1 : 0, kcB = jb.transB ? 0 : 1;
+  const int trow = tid & (kTcM - 1), kg = tid >> 7;
+  // copies of slice s into its stage, committed as one group (an empty group past the end keeps
+  // the count of groups per slice uniform)
+  auto issue = [&](int s) {
+    if (s < nk) {
+      double* raw = reinterpret_cast<double*>(tc_smem + (s % kTcStages) * kTcStageBytes);
+      tc_load_slice<VEC>(raw, jb.A, jb.lda, jb.M, m0, jb.K, s * kTcBK, kcA, tid);
+      tc_load_slice<VEC>(raw + kTcOpBytes / 8, jb.B, jb.ldb, jb.N, n0, jb.K, s * kTcBK, kcB, tid);
     }
+    cp_async_commit();
   };
-  // registers of slice `it` -> its shared-memory stage (split TF32, each group of 4 as one 16-byte
-  // store), then thread 0 issues the slice's MMAs; false (in every thread) on a timed-out wait
-  auto stage_in = [&](int it, const double (&va)[kTcPerThread], const double (&vb)[kTcPerThread]) -> bool {
-    const int st = it & 1;
-    unsigned char* sbase = tc_smem + st * kTcStageBytes;
-    float* Ahi = reinterpret_cast<float*>(sbase);
-    float* Alo = Ahi + kTcM * kTcBK;
-    float* Bhi = Alo + kTcM * kTcBK;
-    float* Blo = Bhi + kTcN * kTcBK;
-    int bad = 0;
-    if (it >= kTcStages) {
-      // the MMAs that read this stage two slices ago must be done before it is overwritten
-      if (!mbar_wait(smem_u32(&mbar[st]), (uint32_t)(((it - kTcStages) >> 1) & 1))) bad = 1;
+#pragma unroll 1
+  for (int s = 0; s < kTcStages - 1; ++s) issue(s);
+  cp_async_wait<kTcStages - 2>();  // slice 0 landed
+  __syncthreads();
+  int fail = 0, bad = 0;
+#pragma unroll 1
+  for (int s = 0; s < nk; ++s) {
+    const int st = s % kTcStages;
+    unsigned char* base = tc_smem + st * kTcStageBytes;
+    double xa[4], xb[4];
+    tc_read4(reinterpret_cast<const double*>(base), kcA, trow, kg, xa);
+    tc_read4(reinterpret_cast<const double*>(base + kTcOpBytes), kcB, trow, kg, xb);
+    if (__syncthreads_or(bad)) {  // every raw read of the stage is done (or a wait ran out)
+      fail = 1;
+      break;
     }
-    if (__syncthreads_or(bad)) return false;
-    {
-      const int r = tid >> 2, gh = (tid & 3) * 2;
-#pragma unroll
-      for (int g = 0; g < kTcPerThread / 4; ++g) {
-        float4 ah, al, bh, bl;
-        float* pah = &ah.x; float* pal = &al.x; float* pbh = &bh.x; float* pbl = &bl.x;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const float fa = (float)va[4 * g + c], fb = (float)vb[4 * g + c];
-          const uint32_t ha = to_tf32(fa), hb = to_tf32(fb);
-          pah[c] = __uint_as_float(ha);
-          pal[c] = __uint_as_float(to_tf32(fa - __uint_as_float(ha)));
-          pbh[c] = __uint_as_float(hb);
-          pbl[c] = __uint_as_float(to_tf32(fb - __uint_as_float(hb)));
-        }
-        const int chunk = gh + g;
-        *reinterpret_cast<float4*>(Ahi + chunk * (kTcM * 4) + r * 4) = ah;
-        *reinterpret_cast<float4*>(Alo + chunk * (kTcM * 4) + r * 4) = al;
-        *reinterpret_cast<float4*>(Bhi + chunk * (kTcN * 4) + r * 4) = bh;
-        *reinterpret_cast<float4*>(Blo + chunk * (kTcN * 4) + r * 4) = bl;
-      }
-    }
+    tc_write4(reinterpret_cast<float*>(base), xa, trow, kg);
+    tc_write4(reinterpret_cast<float*>(base + kTcOpBytes), xb, trow, kg);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    cp_async_wait<kTcStages - 3>();  // slice s + 1 landed; the barrier publishes it with this stage
     __syncthreads();
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;");
-      const uint32_t aH = smem_u32(Ahi), aL = smem_u32(Alo), bH = smem_u32(Bhi), bL = smem_u32(Blo);
+      const uint32_t aH = smem_u32(base), aL = aH + kTcM * kTcBK * 4;
+      const uint32_t bH = smem_u32(base + kTcOpBytes), bL = bH + kTcN * kTcBK * 4;
       const uint32_t lboA = kTcM * 16, lboB = kTcN * 16, sbo = 128;
 #pragma unroll
       for (int ks = 0; ks < kTcBK / 8; ++ks) {
         const uint32_t oa = ks * 2 * kTcM * 16, ob = ks * 2 * kTcN * 16;
         const uint64_t dAh = umma_desc(aH + oa, lboA, sbo), dAl = umma_desc(aL + oa, lboA, sbo);
         const uint64_t dBh = umma_desc(bH + ob, lboB, sbo), dBl = umma_desc(bL + ob, lboB, sbo);
-        const uint32_t first = (it == 0 && ks == 0) ? 0u : 1u;
+        const uint32_t first = (s == 0 && ks == 0) ? 0u : 1u;
         mma_tf32(tmem_d, dAh, dBh, idesc, first);
         mma_tf32(tmem_d, dAh, dBl, idesc, 1u);
         mma_tf32(tmem_d, dAl, dBh, idesc, 1u);
       }
       mma_commit(smem_u32(&mbar[st]));
     }
-    return true;
-  };
-  // two register sets: the loads of slice it + 1 are in flight while slice it is converted
-  double a0[kTcPerThread], b0[kTcPerThread], a1[kTcPerThread], b1[kTcPerThread];
-  if (nk > 0) gload(0, a0, b0);
-  for (int it = 0; it < nk; it += 2) {
-    if (it + 1 < nk) gload(it + 1, a1, b1);
-    if (!stage_in(it, a0, b0)) {
-      fail = 1;
-      break;
+    // slice s + 5 refills the stage of slice s - 1 once the MMAs that read it are done
+    const int nxt = s + kTcStages - 1;
+    if (s >= 1 && nxt < nk && !bad) {
+      const int prev = s - 1;
+      if (!mbar_wait(smem_u32(&mbar[prev % kTcStages]), (uint32_t)((prev / kTcStages) & 1))) bad = 1;
     }
-    if (it + 1 >= nk) break;
-    if (it + 2 < nk) gload(it + 2, a0, b0);
-    if (!stage_in(it + 1, a1, b1)) {
-      fail = 1;
-      break;
-    }
+    if (!bad) issue(nxt);
+    else cp_async_commit();
   }
+  cp_async_wait<0>();  // no copy in flight when the kernel leaves
+  if (__syncthreads_or(bad | fail)) fail = 1;
   // wait for the last commit (it covers every MMA issued before it)
   if (!fail && nk > 0 && tid == 0) {
     const int last = nk - 1;
-    if (!mbar_wait(smem_u32(&mbar[last & 1]), (uint32_t)((last >> 1) & 1))) timed_out = 1;
+    if (!mbar_wait(smem_u32(&mbar[last % kTcStages]), (uint32_t)((last / kTcStages) & 1))) timed_out = 1;
   }
   if (fail && tid == 0) timed_out = 1;
   __syncthreads();
@@ -295,12 +340,18 @@ int launch_wait_selftest(long long limit, int* status, cudaStream_t s) {
 
 long long tc_wait_limit() { return kTcWaitLimit; }
 
-int launch_gemm_tc3(const GemmJob* jobs, int njobs, int max_m, int max_n, int* status, int kind, cudaStream_t s) {
+int launch_gemm_tc3(const GemmJob* jobs, int njobs, int max_m, int max_n, int aligned16, int* status, int kind,
+                    cudaStream_t s) {
   if (njobs <= 0) return 0;
   const size_t sm = (size_t)kTcStages * kTcStageBytes + 1024;
-  cudaFuncSetAttribute(k_gemm_tc3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   dim3 grid((unsigned)((max_n + kTcN - 1) / kTcN), (unsigned)((max_m + kTcM - 1) / kTcM), (unsigned)njobs);
-  k_gemm_tc3<<<grid, kTcThreads, sm, s>>>(jobs, status, kind);
+  if (aligned16) {
+    cudaFuncSetAttribute(k_gemm_tc3<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_gemm_tc3<2><<<grid, kTcThreads, sm, s>>>(jobs, status, kind);
+  } else {
+    cudaFuncSetAttribute(k_gemm_tc3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_gemm_tc3<1><<<grid, kTcThreads, sm, s>>>(jobs, status, kind);
+  }
   return (int)cudaGetLastError();
 }
 

@@ -191,6 +191,13 @@ int tlr_plan_kernel_stats(tlr_plan* plan, double* ms, long long* launches, doubl
  * (optional): the poll limit of the production waits.  Allocates one int on `device`. */
 int tlr_selftest_bounded_wait(long long iterations, int device, double* elapsed_ms, long long* limit);
 
+/* Self-test of the backward pass's GEMM kernels (no reference counterpart):
+ * C = alpha op(A) op(B) + beta C, column-major, op(X) = X^T when trans != 0, on device pointers
+ * of `device`, on the FP64 tensor cores (precision TLR_PRECISION_FP64) or as split TF32 on the
+ * tcgen05 tensor cores (TLR_PRECISION_MIXED).  Synchronous; 0 on success, < 0 on errors. */
+int tlr_selftest_gemm(int precision, int transA, int transB, int M, int N, int K, double alpha, const double* A,
+                      int lda, const double* B, int ldb, double beta, double* C, int ldc, int device);
+
 /* Message of the last error on this thread. */
 const char* tlr_last_error(void);
 
