@@ -12,7 +12,9 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
+#include <tuple>
 #include <vector>
 
 namespace {
@@ -103,6 +105,13 @@ struct tlr_plan {
   size_t d_ccol_cap = 0;
   tlr::CopyJob* d_copy = nullptr;
   size_t d_copy_cap = 0;
+  // mixed precision: the GEMM operands split to TF32 blocks (one launch at a time) and their tables
+  float* tc_area = nullptr;
+  size_t tc_area_cap = 0;
+  tlr::SplitJob* d_split = nullptr;
+  size_t d_split_cap = 0;
+  tlr::TcOperands* d_tcops = nullptr;
+  size_t d_tcops_cap = 0;
 };
 
 namespace {
@@ -128,6 +137,12 @@ void free_all(tlr_plan* p) {
   if (p->d_jobs) cudaFree(p->d_jobs);
   if (p->d_ccol) cudaFree(p->d_ccol);
   if (p->d_copy) cudaFree(p->d_copy);
+  if (p->tc_area) cudaFree(p->tc_area);
+  if (p->d_split) cudaFree(p->d_split);
+  if (p->d_tcops) cudaFree(p->d_tcops);
+  p->tc_area = nullptr;
+  p->d_split = nullptr;
+  p->d_tcops = nullptr;
   p->bw = nullptr;
   p->d_jobs = nullptr;
   p->d_ccol = nullptr;
@@ -257,14 +272,39 @@ int grow(T** ptr, size_t* cap, size_t need) {
   return 0;
 }
 
-// 1 when every job's A and B start on 16 bytes and have even leading dimensions, so that the
-// tensor-core GEMM may copy its operands two doubles at a time
-static int tc_aligned16(const tlr::GemmJob* j, int count) {
-  for (int q = 0; q < count; ++q)
-    if ((reinterpret_cast<uintptr_t>(j[q].A) & 15) || (reinterpret_cast<uintptr_t>(j[q].B) & 15) || (j[q].lda & 1) ||
-        (j[q].ldb & 1))
-      return 0;
-  return 1;
+// Split tables of one launch of the tensor-core GEMM: every distinct operand (pointer, leading
+// dimension, layout, rows, K) of the jobs once, at float offsets of a scratch area (the SplitJob's
+// dst stays NULL until the area is known); per job the offsets of its op(A) and op(B)^T blocks,
+// SIZE_MAX for a job without products.
+struct TcSplitPlan {
+  std::vector<tlr::SplitJob> splits;
+  std::vector<size_t> split_off;
+  std::vector<std::pair<size_t, size_t>> job_off;
+  int nblocks = 0;
+  size_t floats = 0;
+};
+
+static void tc_split_plan(const tlr::GemmJob* jobs, int count, TcSplitPlan& out) {
+  std::map<std::tuple<const double*, int, int, int, int>, size_t> seen;
+  auto panel = [&](const double* src, int ld, int kcont, int rows, int K) {
+    const auto key = std::make_tuple(src, ld, kcont, rows, K);
+    const auto it = seen.find(key);
+    if (it != seen.end()) return it->second;
+    const size_t off = out.floats;
+    out.splits.push_back({src, nullptr, ld, kcont, rows, K, out.nblocks});
+    out.split_off.push_back(off);
+    out.nblocks += tlr::tc_panel_blocks(rows, K);
+    out.floats += tlr::tc_panel_floats(rows, K);
+    seen.emplace(key, off);
+    return off;
+  };
+  for (int q = 0; q < count; ++q) {
+    const tlr::GemmJob& j = jobs[q];
+    if (j.M > 0 && j.N > 0 && j.K > 0)
+      out.job_off.push_back({panel(j.A, j.lda, j.transA ? 1 : 0, j.M, j.K), panel(j.B, j.ldb, j.transB ? 0 : 1, j.N, j.K)});
+    else
+      out.job_off.push_back({SIZE_MAX, SIZE_MAX});
+  }
 }
 
 struct LaunchRange {
@@ -430,6 +470,44 @@ int run_backward(tlr_plan* p, double sigma2, double inv_range, double eta) {
     TRY(cuda_check(cudaMemcpyAsync(p->d_copy, copies.data(), copies.size() * sizeof(tlr::CopyJob),
                                    cudaMemcpyHostToDevice, s),
                    "copies"));
+  // mixed precision: split tables of every tensor-core GEMM launch; the launches share one area
+  // (each split runs right before its GEMM on the same stream)
+  std::vector<size_t> split_first(plan.size(), 0);
+  std::vector<int> split_count(plan.size(), 0), split_blocks(plan.size(), 0);
+  if (p->precision == TLR_PRECISION_MIXED) {
+    std::vector<tlr::SplitJob> splits;
+    std::vector<size_t> soff;
+    std::vector<std::pair<size_t, size_t>> joff(jobs.size(), {SIZE_MAX, SIZE_MAX});
+    size_t area = 0;
+    for (size_t li = 0; li < plan.size(); ++li) {
+      const LaunchRange& L = plan[li];
+      if (L.kind != 0 || L.count == 0) continue;
+      TcSplitPlan sp;
+      tc_split_plan(jobs.data() + L.first, L.count, sp);
+      split_first[li] = splits.size();
+      split_count[li] = (int)sp.splits.size();
+      split_blocks[li] = sp.nblocks;
+      splits.insert(splits.end(), sp.splits.begin(), sp.splits.end());
+      soff.insert(soff.end(), sp.split_off.begin(), sp.split_off.end());
+      for (int q = 0; q < L.count; ++q) joff[L.first + q] = sp.job_off[q];
+      area = std::max(area, sp.floats);
+    }
+    TRY(grow(&p->tc_area, &p->tc_area_cap, area));
+    TRY(grow(&p->d_split, &p->d_split_cap, splits.size()));
+    TRY(grow(&p->d_tcops, &p->d_tcops_cap, jobs.size()));
+    for (size_t q = 0; q < splits.size(); ++q) splits[q].dst = p->tc_area + soff[q];
+    std::vector<tlr::TcOperands> ops(jobs.size(), {nullptr, nullptr});
+    for (size_t q = 0; q < jobs.size(); ++q)
+      if (joff[q].first != SIZE_MAX) ops[q] = {p->tc_area + joff[q].first, p->tc_area + joff[q].second};
+    if (!splits.empty())
+      TRY(cuda_check(cudaMemcpyAsync(p->d_split, splits.data(), splits.size() * sizeof(tlr::SplitJob),
+                                     cudaMemcpyHostToDevice, s),
+                     "split table"));
+    if (!ops.empty())
+      TRY(cuda_check(cudaMemcpyAsync(p->d_tcops, ops.data(), ops.size() * sizeof(tlr::TcOperands),
+                                     cudaMemcpyHostToDevice, s),
+                     "operand table"));
+  }
   // launches
   LAUNCH(TLR_K_TRI_INV, tlr::launch_tri_inv(p->D, Li, n, b, nB, p->status, s));
   // alpha = Sigma_t^{-1} y (block rows nB-1 .. 0) needs only the factor, z and the inverses of
@@ -446,15 +524,18 @@ int run_backward(tlr_plan* p, double sigma2, double inv_range, double eta) {
                                                            base + oAl, base + oWk, p->status, p->side));
     TRY(cuda_check(cudaEventRecord(p->ev_alpha[m], p->side), "event"));
   }
-  for (const LaunchRange& L : plan) {
+  for (size_t li = 0; li < plan.size(); ++li) {
+    const LaunchRange& L = plan[li];
     if (L.kind == 4) {
       LAUNCH(TLR_K_BWD_GEMM, tlr::launch_dgemm_batched(p->d_jobs + L.first, L.count, L.max_m, L.max_n, p->status,
                                                         TLR_K_BWD_GEMM, s));
     } else if (L.kind == 0) {
       if (p->precision == TLR_PRECISION_MIXED) {
-        const int al = tc_aligned16(jobs.data() + L.first, L.count);
-        LAUNCH(TLR_K_BWD_GEMM, tlr::launch_gemm_tc3(p->d_jobs + L.first, L.count, L.max_m, L.max_n, al, p->status,
-                                                     TLR_K_BWD_GEMM, s));
+        if (split_count[li])
+          LAUNCH(TLR_K_BWD_GEMM, tlr::launch_split_tf32(p->d_split + split_first[li], split_count[li],
+                                                         split_blocks[li], p->status, TLR_K_BWD_GEMM, s));
+        LAUNCH(TLR_K_BWD_GEMM, tlr::launch_gemm_tc3(p->d_jobs + L.first, p->d_tcops + L.first, L.count, L.max_m,
+                                                     L.max_n, p->status, TLR_K_BWD_GEMM, s));
       }
       else
         LAUNCH(TLR_K_BWD_GEMM, tlr::launch_dgemm_batched(p->d_jobs + L.first, L.count, L.max_m, L.max_n, p->status,
@@ -908,25 +989,45 @@ int tlr_selftest_gemm(int precision, int transA, int transB, int M, int N, int K
   int rc = cuda_check(cudaSetDevice(device), "set device");
   if (rc) return rc;
   const size_t status_bytes = sizeof(int) * (4 + 4 * TLR_NKINDS);
+  tlr::GemmJob j{A, B, C, nullptr, lda, ldb, ldc, M, N, K, transA ? 1 : 0, transB ? 1 : 0, alpha, beta};
+  TcSplitPlan sp;
+  tc_split_plan(&j, 1, sp);
+  // one buffer: job, operand pointers, split table, status, then the split area (16-byte aligned)
+  const size_t oOps = 256, oSplit = 512, oStatus = 1024, oArea = 4096;
   unsigned char* d = nullptr;
   cudaStream_t s = nullptr;
   int h = 0;
-  tlr::GemmJob j{A, B, C, nullptr, lda, ldb, ldc, M, N, K, transA ? 1 : 0, transB ? 1 : 0, alpha, beta};
-  rc = cuda_check(cudaMalloc(&d, 256 + status_bytes), "self-test buffers");
+  rc = cuda_check(cudaMalloc(&d, oArea + sizeof(float) * std::max<size_t>(sp.floats, 4)), "self-test buffers");
+  if (rc) return rc;
   tlr::GemmJob* dj = reinterpret_cast<tlr::GemmJob*>(d);
-  int* st = reinterpret_cast<int*>(d + 256);
-  if (!rc) rc = cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+  tlr::TcOperands* dops = reinterpret_cast<tlr::TcOperands*>(d + oOps);
+  tlr::SplitJob* dsplit = reinterpret_cast<tlr::SplitJob*>(d + oSplit);
+  int* st = reinterpret_cast<int*>(d + oStatus);
+  float* area = reinterpret_cast<float*>(d + oArea);
+  for (size_t q = 0; q < sp.splits.size(); ++q) sp.splits[q].dst = area + sp.split_off[q];
+  tlr::TcOperands op{nullptr, nullptr};
+  if (sp.job_off[0].first != SIZE_MAX) op = {area + sp.job_off[0].first, area + sp.job_off[0].second};
+  rc = cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
   if (!rc) rc = cuda_check(cudaMemsetAsync(st, 0, status_bytes, s), "status");
   if (!rc) rc = cuda_check(cudaMemcpyAsync(dj, &j, sizeof(j), cudaMemcpyHostToDevice, s), "job");
-  if (!rc)
-    rc = cuda_check((cudaError_t)(precision == TLR_PRECISION_MIXED
-                                      ? tlr::launch_gemm_tc3(dj, 1, M, N, tc_aligned16(&j, 1), st, TLR_K_BWD_GEMM, s)
-                                      : tlr::launch_dgemm_batched(dj, 1, M, N, st, TLR_K_BWD_GEMM, s)),
-                    "self-test launch");
+  if (!rc) rc = cuda_check(cudaMemcpyAsync(dops, &op, sizeof(op), cudaMemcpyHostToDevice, s), "operands");
+  if (!rc && !sp.splits.empty())
+    rc = cuda_check(cudaMemcpyAsync(dsplit, sp.splits.data(), sp.splits.size() * sizeof(tlr::SplitJob),
+                                    cudaMemcpyHostToDevice, s),
+                    "split table");
+  if (!rc && precision == TLR_PRECISION_MIXED) {
+    if (!sp.splits.empty())
+      rc = cuda_check((cudaError_t)tlr::launch_split_tf32(dsplit, (int)sp.splits.size(), sp.nblocks, st,
+                                                          TLR_K_BWD_GEMM, s),
+                      "split launch");
+    if (!rc) rc = cuda_check((cudaError_t)tlr::launch_gemm_tc3(dj, dops, 1, M, N, st, TLR_K_BWD_GEMM, s), "gemm launch");
+  } else if (!rc) {
+    rc = cuda_check((cudaError_t)tlr::launch_dgemm_batched(dj, 1, M, N, st, TLR_K_BWD_GEMM, s), "gemm launch");
+  }
   if (!rc) rc = cuda_check(cudaMemcpyAsync(&h, st, sizeof(int), cudaMemcpyDeviceToHost, s), "status copy");
   if (!rc) rc = cuda_check(cudaStreamSynchronize(s), "self-test");
   if (s) cudaStreamDestroy(s);
-  if (d) cudaFree(d);
+  cudaFree(d);
   if (rc) return rc;
   if (h == TLR_ERR_TIMEOUT) return fail(TLR_ERR_TIMEOUT, "a device wait ran out of its iteration limit");
   return h;

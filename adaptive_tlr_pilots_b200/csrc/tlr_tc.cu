@@ -5,22 +5,21 @@
 // the selected-inversion gradient within ~1e-5 of the FP64 one (single-pass TF32 loses ~1e-2 on
 // the range component).
 //
-// One CTA of 512 threads computes a 128 x N_TILE output tile (N_TILE = 128): the accumulator is
-// 128 TMEM lanes x 128 columns.  K advances in slices of 16 through a ring of six shared-memory
-// stages.  Each stage first receives the raw FP64 slice of A and of B by cp.async (16-byte copies
-// when every row start is 16-byte aligned, else 8-byte; rows and k beyond the matrix arrive as
-// zeros), five slices ahead of the one being converted, so the copies' latency hides behind the
-// conversion and the MMAs of the slices before.  The threads then read their four k values of
-// one tile row (thread = row + 128 x k-group), and, after a block barrier, overwrite the same
-// stage with the split TF32 values in the canonical K-major, no-swizzle UMMA layout (core
-// matrices of 8 rows x 16 bytes; rows of a core matrix 16 B apart, 8-row groups 128 B apart, the
-// two 16-byte K halves of one MMA 2048 B apart): a double and its (hi, lo) pair take the same 8
-// bytes, so the conversion fits in place.  After a fence for the async proxy and a barrier,
-// thread 0 issues 2 K-steps x 3 tcgen05.mma.kind::tf32 and commits them to the stage's mbarrier;
-// the stage is refilled once that commit completes.  The MMA sequence (K-steps of 8 in order,
-// three products each) is the same for any slice length, so results do not depend on it.
-// Waits on the mbarriers are bounded: on timeout the kernel sets an error status, lets its copies
-// land, frees its tensor memory and returns.
+// Two kernels per batch of GEMM jobs.  k_split_tf32 converts each distinct operand once: rows x K
+// of FP64 into zero-padded blocks of 128 rows x 16 k, block (row tile t, K slice s) stored
+// contiguously at (t * nks + s) x 16 KB as hi TF32 then lo TF32, each in the canonical K-major,
+// no-swizzle UMMA layout (core matrices of 8 rows x 16 bytes; rows of a core matrix 16 B apart,
+// 8-row groups 128 B apart, the two 16-byte K halves of one MMA 2048 B apart).  A block is then
+// exactly the shared-memory image of one operand's slice.  k_gemm_tc3 computes a 128 x 128 output
+// tile per CTA (accumulator: 128 TMEM lanes x 128 columns) with two single-thread roles over a ring
+// of six 32 KB stages: a producer thread moves each slice's A and B blocks with two bulk async
+// copies (cp.async.bulk, completing on the stage's "full" mbarrier with a byte count), and an MMA
+// thread waits on "full", issues 2 K-steps x 3 tcgen05.mma.kind::tf32 and commits them to the
+// stage's "empty" mbarrier, which releases the stage to the producer.  The other warps join for
+// the epilogue (tcgen05.ld of the accumulator, alpha / beta, column scatter).  The MMA sequence
+// (K-steps of 8 in order, three products each) is fixed, so results do not depend on the staging.
+// Waits are bounded: on timeout the kernel sets an error status, waits (bounded) for its copies
+// in flight, frees its tensor memory and returns.
 #include <stdint.h>
 
 #include "tlr_device.cuh"
@@ -30,13 +29,14 @@ namespace tlr {
 
 constexpr int kTcM = 128;
 constexpr int kTcN = 128;
-constexpr int kTcBK = 16;                          // k per slice: two MMA K-steps
+constexpr int kTcBK = 16;                               // k per slice: two MMA K-steps
 constexpr int kTcStages = 6;
-constexpr int kTcThreads = 512;                    // thread = tile row (0..127) + 128 x k-group (0..3)
-constexpr int kTcRawKS = kTcBK + 2;                // row stride (doubles) of a k-contiguous raw slice
-constexpr int kTcOpBytes = kTcM * kTcRawKS * 8;    // one operand's region: 18,432 B >= 16 KB of hi + lo
-constexpr int kTcStageBytes = 2 * kTcOpBytes;      // A region, then B region
-static_assert(kTcM == kTcN && kTcThreads == 4 * kTcM && kTcBK == 16, "thread map assumes 128 x 128 x 16");
+constexpr int kTcThreads = 256;                         // warp 0: copies, warp 1: MMAs, all: epilogue
+constexpr int kTcBlockFloats = 2 * kTcM * kTcBK;        // one operand block: hi + lo, 16 KB
+constexpr int kTcOpBytes = kTcBlockFloats * 4;
+constexpr int kTcStageBytes = 2 * kTcOpBytes;           // A block, then B block
+constexpr int kSplitThreads = 256;
+static_assert(kTcM == kTcN && kTcBK == 16, "block layout assumes 128-row tiles and 16-k slices");
 static_assert(kTcStageBytes * kTcStages + 1024 <= 227 * 1024, "stages exceed shared memory");
 constexpr long long kTcWaitLimit = 1ll << 23;  // polls of about 140 ns on B200: about 1.2 s
 
@@ -128,57 +128,6 @@ __global__ void k_wait_selftest(long long limit, int* status) {
   if (tid == 0) *status = ok ? 0 : -7;
 }
 
-// One operand's raw FP64 slice global -> shared by cp.async: 128 tile rows x 16 k from row0 and
-// k0, zeros beyond `rows` and K.  kcont: k is the contiguous index in global memory (element
-// (row, k) at X[row * ld + k]); the slice is then stored [row][kTcRawKS], else [k][128] (element
-// at X[k * ld + row]).  VEC doubles per copy (2: X and ld keep every copy 16-byte aligned).
-template <int VEC>
-__device__ __forceinline__ void tc_load_slice(double* raw, const double* X, int ld, int rows, int row0, int K, int k0,
-                                              int kcont, int tid) {
-  constexpr int kChunks = kTcM * kTcBK / VEC;
-#pragma unroll
-  for (int i = 0; i < kChunks / kTcThreads; ++i) {
-    const int q = tid + i * kTcThreads;
-    int row, k, nv;
-    const double* src;
-    double* dst;
-    if (kcont) {
-      row = q / (kTcBK / VEC);
-      k = (q % (kTcBK / VEC)) * VEC;
-      nv = row0 + row < rows ? min(VEC, K - (k0 + k)) : 0;
-      src = X + (size_t)(row0 + row) * ld + (k0 + k);
-      dst = raw + row * kTcRawKS + k;
-    } else {
-      k = q / (kTcM / VEC);
-      row = (q % (kTcM / VEC)) * VEC;
-      nv = k0 + k < K ? min(VEC, rows - (row0 + row)) : 0;
-      src = X + (size_t)(k0 + k) * ld + (row0 + row);
-      dst = raw + k * kTcM + row;
-    }
-    if (nv <= 0) {  // nothing to read: zeros, from a valid address
-      nv = 0;
-      src = X;
-    }
-    if (VEC == 2) cp_async16(dst, src, nv * 8);
-    else cp_async8(dst, src, nv * 8);
-  }
-}
-
-// k values 4g .. 4g + 3 of tile row r from a raw slice
-__device__ __forceinline__ void tc_read4(const double* raw, int kcont, int r, int g, double (&x)[4]) {
-  if (kcont) {
-    const double2 u = *reinterpret_cast<const double2*>(raw + r * kTcRawKS + 4 * g);
-    const double2 v = *reinterpret_cast<const double2*>(raw + r * kTcRawKS + 4 * g + 2);
-    x[0] = u.x;
-    x[1] = u.y;
-    x[2] = v.x;
-    x[3] = v.y;
-  } else {
-#pragma unroll
-    for (int c = 0; c < 4; ++c) x[c] = raw[(4 * g + c) * kTcM + r];
-  }
-}
-
 // split x = hi + lo (both TF32) and store them in the UMMA layout: hi at `out`, lo 8 KB after
 __device__ __forceinline__ void tc_write4(float* out, const double (&x)[4], int r, int g) {
   float4 h, l;
@@ -195,17 +144,64 @@ __device__ __forceinline__ void tc_write4(float* out, const double (&x)[4], int 
   *reinterpret_cast<float4*>(out + kTcM * kTcBK + g * (kTcM * 4) + r * 4) = l;
 }
 
-template <int VEC>
-__global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc3(const GemmJob* TLR_RESTRICT jobs, int* TLR_RESTRICT status,
+// One CTA per block (128 rows x 16 k) of the launch's operands; the block's operand is the last
+// job whose block0 is <= blockIdx.x.  Thread (r = tid % 128, g = tid / 128 + 2i) writes k values
+// 4g .. 4g + 3 of tile row r.
+__global__ void __launch_bounds__(kSplitThreads) k_split_tf32(const SplitJob* TLR_RESTRICT jobs, int njobs,
+                                                            int* TLR_RESTRICT status, int kind) {
+  if (*status != 0) return;
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].block0 <= (int)blockIdx.x) lo = mid;
+    else hi = mid - 1;
+  }
+  const SplitJob j = jobs[lo];
+  const int nks = (j.K + kTcBK - 1) / kTcBK;
+  const int blk = (int)blockIdx.x - j.block0;
+  const int row0 = (blk / nks) * kTcM, k0 = (blk % nks) * kTcBK;
+  float* out = j.dst + (size_t)blk * kTcBlockFloats;
+  const int r = threadIdx.x & (kTcM - 1), gr = row0 + r;
+#pragma unroll
+  for (int g = threadIdx.x >> 7; g < kTcBK / 4; g += kSplitThreads / kTcM) {
+    double x[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int gk = k0 + 4 * g + c;
+      x[c] = (gr < j.rows && gk < j.K) ? (j.kcont ? j.src[(size_t)gr * j.ld + gk] : j.src[(size_t)gk * j.ld + gr])
+                                       : 0.0;
+    }
+    tc_write4(out, x, r, g);
+  }
+  if (threadIdx.x == 0) {
+    const int mt = min(kTcM, j.rows - row0), kt = min(kTcBK, j.K - k0);
+    add_work(status, kind, 0.0, 8.0 * mt * kt + 4.0 * kTcBlockFloats);
+  }
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+// contiguous global -> shared bulk copy (16-byte aligned, size a multiple of 16) that completes
+// `bytes` of the transaction count of `mbar`
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(mbar)
+               : "memory");
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc3(const GemmJob* TLR_RESTRICT jobs,
+                                                 const TcOperands* TLR_RESTRICT ops, int* TLR_RESTRICT status,
                                                  int kind) {
   if (*status != 0) return;
   const GemmJob jb = jobs[blockIdx.z];
   const int m0 = blockIdx.y * kTcM, n0 = blockIdx.x * kTcN;
   if (m0 >= jb.M || n0 >= jb.N) return;
   extern __shared__ __align__(1024) unsigned char tc_smem[];
-  __shared__ __align__(8) uint64_t mbar[kTcStages];
+  __shared__ __align__(8) uint64_t full[kTcStages], empty[kTcStages];
   __shared__ uint32_t tmem_base_sh;
-  __shared__ int timed_out;
+  __shared__ int timed_out, issued;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
@@ -213,89 +209,82 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc3(const GemmJob* TLR_R
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    for (int s = 0; s < kTcStages; ++s)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[s])));
+    for (int s = 0; s < kTcStages; ++s) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[s])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[s])));
+    }
     asm volatile("fence.mbarrier_init.release.cluster;");
     timed_out = 0;
+    issued = 0;
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem_d = tmem_base_sh;
-  const uint32_t idesc = umma_idesc_tf32(kTcM, kTcN);
   const int nk = (jb.K + kTcBK - 1) / kTcBK;
-  const int kcA = jb.transA ? 1 : 0, kcB = jb.transB ? 0 : 1;
-  const int trow = tid & (kTcM - 1), kg = tid >> 7;
-  // copies of slice s into its stage, committed as one group (an empty group past the end keeps
-  // the count of groups per slice uniform)
-  auto issue = [&](int s) {
-    if (s < nk) {
-      double* raw = reinterpret_cast<double*>(tc_smem + (s % kTcStages) * kTcStageBytes);
-      tc_load_slice<VEC>(raw, jb.A, jb.lda, jb.M, m0, jb.K, s * kTcBK, kcA, tid);
-      tc_load_slice<VEC>(raw + kTcOpBytes / 8, jb.B, jb.ldb, jb.N, n0, jb.K, s * kTcBK, kcB, tid);
+  const uint32_t sbase = smem_u32(tc_smem);
+  if (nk > 0 && tid == 0) {
+    // producer: slice s into stage s % 6 once the MMAs of slice s - 6 have released it
+    const TcOperands op = ops[blockIdx.z];
+    const float* pa = op.a + (size_t)(m0 / kTcM) * nk * kTcBlockFloats;
+    const float* pb = op.b + (size_t)(n0 / kTcN) * nk * kTcBlockFloats;
+    int s = 0;
+    for (; s < nk; ++s) {
+      const int st = s % kTcStages;
+      if (s >= kTcStages && !mbar_wait(smem_u32(&empty[st]), (uint32_t)((s / kTcStages - 1) & 1))) {
+        timed_out = 1;
+        break;
+      }
+      const uint32_t fb = smem_u32(&full[st]);
+      mbar_expect_tx(fb, kTcStageBytes);
+      bulk_g2s(sbase + st * kTcStageBytes, pa + (size_t)s * kTcBlockFloats, kTcOpBytes, fb);
+      bulk_g2s(sbase + st * kTcStageBytes + kTcOpBytes, pb + (size_t)s * kTcBlockFloats, kTcOpBytes, fb);
     }
-    cp_async_commit();
-  };
-#pragma unroll 1
-  for (int s = 0; s < kTcStages - 1; ++s) issue(s);
-  cp_async_wait<kTcStages - 2>();  // slice 0 landed
-  __syncthreads();
-  int fail = 0, bad = 0;
-#pragma unroll 1
-  for (int s = 0; s < nk; ++s) {
-    const int st = s % kTcStages;
-    unsigned char* base = tc_smem + st * kTcStageBytes;
-    double xa[4], xb[4];
-    tc_read4(reinterpret_cast<const double*>(base), kcA, trow, kg, xa);
-    tc_read4(reinterpret_cast<const double*>(base + kTcOpBytes), kcB, trow, kg, xb);
-    if (__syncthreads_or(bad)) {  // every raw read of the stage is done (or a wait ran out)
-      fail = 1;
-      break;
-    }
-    tc_write4(reinterpret_cast<float*>(base), xa, trow, kg);
-    tc_write4(reinterpret_cast<float*>(base + kTcOpBytes), xb, trow, kg);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    cp_async_wait<kTcStages - 3>();  // slice s + 1 landed; the barrier publishes it with this stage
-    __syncthreads();
-    if (tid == 0) {
+    issued = s;
+  } else if (nk > 0 && tid == 32) {
+    // MMA issuer
+    const uint32_t idesc = umma_idesc_tf32(kTcM, kTcN);
+    const uint32_t lbo = kTcM * 16, sbo = 128;
+    for (int s = 0; s < nk; ++s) {
+      const int st = s % kTcStages;
+      if (!mbar_wait(smem_u32(&full[st]), (uint32_t)((s / kTcStages) & 1))) {
+        timed_out = 1;
+        break;
+      }
       asm volatile("tcgen05.fence::after_thread_sync;");
-      const uint32_t aH = smem_u32(base), aL = aH + kTcM * kTcBK * 4;
-      const uint32_t bH = smem_u32(base + kTcOpBytes), bL = bH + kTcN * kTcBK * 4;
-      const uint32_t lboA = kTcM * 16, lboB = kTcN * 16, sbo = 128;
+      const uint32_t aH = sbase + st * kTcStageBytes, aL = aH + kTcM * kTcBK * 4;
+      const uint32_t bH = aH + kTcOpBytes, bL = bH + kTcN * kTcBK * 4;
 #pragma unroll
       for (int ks = 0; ks < kTcBK / 8; ++ks) {
-        const uint32_t oa = ks * 2 * kTcM * 16, ob = ks * 2 * kTcN * 16;
-        const uint64_t dAh = umma_desc(aH + oa, lboA, sbo), dAl = umma_desc(aL + oa, lboA, sbo);
-        const uint64_t dBh = umma_desc(bH + ob, lboB, sbo), dBl = umma_desc(bL + ob, lboB, sbo);
+        const uint32_t o = ks * 2 * kTcM * 16;
+        const uint64_t dAh = umma_desc(aH + o, lbo, sbo), dAl = umma_desc(aL + o, lbo, sbo);
+        const uint64_t dBh = umma_desc(bH + o, lbo, sbo), dBl = umma_desc(bL + o, lbo, sbo);
         const uint32_t first = (s == 0 && ks == 0) ? 0u : 1u;
         mma_tf32(tmem_d, dAh, dBh, idesc, first);
         mma_tf32(tmem_d, dAh, dBl, idesc, 1u);
         mma_tf32(tmem_d, dAl, dBh, idesc, 1u);
       }
-      mma_commit(smem_u32(&mbar[st]));
+      mma_commit(smem_u32(&empty[st]));
     }
-    // slice s + 5 refills the stage of slice s - 1 once the MMAs that read it are done
-    const int nxt = s + kTcStages - 1;
-    if (s >= 1 && nxt < nk && !bad) {
-      const int prev = s - 1;
-      if (!mbar_wait(smem_u32(&mbar[prev % kTcStages]), (uint32_t)((prev / kTcStages) & 1))) bad = 1;
+  }
+  __syncwarp();
+  __syncthreads();
+  if (tid == 0 && nk > 0) {
+    if (!timed_out) {
+      // the last commit covers every MMA issued before it
+      const int last = nk - 1;
+      if (!mbar_wait(smem_u32(&empty[last % kTcStages]), (uint32_t)((last / kTcStages) & 1))) timed_out = 1;
+    } else {
+      // failure: let the copies in flight land (the last six slices issued) before leaving
+      for (int q = max(0, issued - kTcStages); q < issued; ++q)
+        mbar_wait(smem_u32(&full[q % kTcStages]), (uint32_t)((q / kTcStages) & 1));
     }
-    if (!bad) issue(nxt);
-    else cp_async_commit();
   }
-  cp_async_wait<0>();  // no copy in flight when the kernel leaves
-  if (__syncthreads_or(bad | fail)) fail = 1;
-  // wait for the last commit (it covers every MMA issued before it)
-  if (!fail && nk > 0 && tid == 0) {
-    const int last = nk - 1;
-    if (!mbar_wait(smem_u32(&mbar[last % kTcStages]), (uint32_t)((last / kTcStages) & 1))) timed_out = 1;
-  }
-  if (fail && tid == 0) timed_out = 1;
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const bool ok = !timed_out;
   if (ok) {
-    // warp w reads TMEM lane quarter w % 4 (the lanes a warp may access) and column quarter w / 4
+    // warp w reads TMEM lane quarter w % 4 (the lanes a warp may access) and column half w / 4
     const int quarter = warp & 3, part = warp >> 2, nparts = kTcThreads / 128;
     const int row = quarter * 32 + lane;
     const int gm = m0 + row;
@@ -340,19 +329,25 @@ int launch_wait_selftest(long long limit, int* status, cudaStream_t s) {
 
 long long tc_wait_limit() { return kTcWaitLimit; }
 
-int launch_gemm_tc3(const GemmJob* jobs, int njobs, int max_m, int max_n, int aligned16, int* status, int kind,
+int launch_split_tf32(const SplitJob* jobs, int njobs, int nblocks, int* status, int kind, cudaStream_t s) {
+  if (njobs <= 0 || nblocks <= 0) return 0;
+  k_split_tf32<<<nblocks, kSplitThreads, 0, s>>>(jobs, njobs, status, kind);
+  return (int)cudaGetLastError();
+}
+
+int launch_gemm_tc3(const GemmJob* jobs, const TcOperands* ops, int njobs, int max_m, int max_n, int* status, int kind,
                     cudaStream_t s) {
   if (njobs <= 0) return 0;
   const size_t sm = (size_t)kTcStages * kTcStageBytes + 1024;
+  cudaFuncSetAttribute(k_gemm_tc3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   dim3 grid((unsigned)((max_n + kTcN - 1) / kTcN), (unsigned)((max_m + kTcM - 1) / kTcM), (unsigned)njobs);
-  if (aligned16) {
-    cudaFuncSetAttribute(k_gemm_tc3<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_gemm_tc3<2><<<grid, kTcThreads, sm, s>>>(jobs, status, kind);
-  } else {
-    cudaFuncSetAttribute(k_gemm_tc3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_gemm_tc3<1><<<grid, kTcThreads, sm, s>>>(jobs, status, kind);
-  }
+  k_gemm_tc3<<<grid, kTcThreads, sm, s>>>(jobs, ops, status, kind);
   return (int)cudaGetLastError();
 }
+
+size_t tc_panel_floats(int rows, int K) {
+  return (size_t)((rows + kTcM - 1) / kTcM) * ((K + kTcBK - 1) / kTcBK) * kTcBlockFloats;
+}
+int tc_panel_blocks(int rows, int K) { return ((rows + kTcM - 1) / kTcM) * ((K + kTcBK - 1) / kTcBK); }
 
 }  // namespace tlr
