@@ -280,7 +280,7 @@ struct TcSplitPlan {
   std::vector<tlr::SplitJob> splits;
   std::vector<size_t> split_off;
   std::vector<std::pair<size_t, size_t>> job_off;
-  int nblocks = 0;
+  int max_blocks = 0;
   size_t floats = 0;
 };
 
@@ -291,9 +291,9 @@ static void tc_split_plan(const tlr::GemmJob* jobs, int count, TcSplitPlan& out)
     const auto it = seen.find(key);
     if (it != seen.end()) return it->second;
     const size_t off = out.floats;
-    out.splits.push_back({src, nullptr, ld, kcont, rows, K, out.nblocks});
+    out.splits.push_back({src, nullptr, ld, kcont, rows, K});
     out.split_off.push_back(off);
-    out.nblocks += tlr::tc_panel_blocks(rows, K);
+    out.max_blocks = std::max(out.max_blocks, tlr::tc_panel_blocks(rows, K));
     out.floats += tlr::tc_panel_floats(rows, K);
     seen.emplace(key, off);
     return off;
@@ -486,7 +486,7 @@ int run_backward(tlr_plan* p, double sigma2, double inv_range, double eta) {
       tc_split_plan(jobs.data() + L.first, L.count, sp);
       split_first[li] = splits.size();
       split_count[li] = (int)sp.splits.size();
-      split_blocks[li] = sp.nblocks;
+      split_blocks[li] = sp.max_blocks;
       splits.insert(splits.end(), sp.splits.begin(), sp.splits.end());
       soff.insert(soff.end(), sp.split_off.begin(), sp.split_off.end());
       for (int q = 0; q < L.count; ++q) joff[L.first + q] = sp.job_off[q];
@@ -1017,7 +1017,7 @@ int tlr_selftest_gemm(int precision, int transA, int transB, int M, int N, int K
                     "split table");
   if (!rc && precision == TLR_PRECISION_MIXED) {
     if (!sp.splits.empty())
-      rc = cuda_check((cudaError_t)tlr::launch_split_tf32(dsplit, (int)sp.splits.size(), sp.nblocks, st,
+      rc = cuda_check((cudaError_t)tlr::launch_split_tf32(dsplit, (int)sp.splits.size(), sp.max_blocks, st,
                                                           TLR_K_BWD_GEMM, s),
                       "split launch");
     if (!rc) rc = cuda_check((cudaError_t)tlr::launch_gemm_tc3(dj, dops, 1, M, N, st, TLR_K_BWD_GEMM, s), "gemm launch");

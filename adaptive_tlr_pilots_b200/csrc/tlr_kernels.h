@@ -73,20 +73,19 @@ int launch_dgemm_batched(const GemmJob* jobs, int njobs, int max_m, int max_n, c
 // Split-TF32 tensor-core GEMM (tlr_tc.cu).  An operand is first converted once into blocks of
 // 128 rows x 16 k (hi then lo TF32 in the UMMA layout, zero-padded), block (row tile t, slice s)
 // at dst + (t * nks + s) * 4096 floats, nks = ceil(K / 16).  kcont: element (row, k) of the
-// operand at src[row * ld + k], else at src[k * ld + row].  block0: index of the operand's first
-// block among the launch's blocks.
+// operand at src[row * ld + k], else at src[k * ld + row].
 struct SplitJob {
   const double* src;
   float* dst;
   int ld, kcont, rows, K;
-  int block0;
 };
 // per GEMM job: the converted op(A) (M rows) and op(B)^T (N rows), both over K
 struct TcOperands {
   const float* a;
   const float* b;
 };
-int launch_split_tf32(const SplitJob* jobs, int njobs, int nblocks, int* status, int kind, cudaStream_t s);
+// max_blocks: the largest operand's block count
+int launch_split_tf32(const SplitJob* jobs, int njobs, int max_blocks, int* status, int kind, cudaStream_t s);
 int launch_gemm_tc3(const GemmJob* jobs, const TcOperands* ops, int njobs, int max_m, int max_n, int* status, int kind,
                     cudaStream_t s);
 size_t tc_panel_floats(int rows, int K);

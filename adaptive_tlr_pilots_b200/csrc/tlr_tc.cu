@@ -11,8 +11,8 @@
 // no-swizzle UMMA layout (core matrices of 8 rows x 16 bytes; rows of a core matrix 16 B apart,
 // 8-row groups 128 B apart, the two 16-byte K halves of one MMA 2048 B apart).  A block is then
 // exactly the shared-memory image of one operand's slice.  k_gemm_tc3 computes a 128 x 128 output
-// tile per CTA (accumulator: 128 TMEM lanes x 128 columns) with two single-thread roles over a ring
-// of six 32 KB stages: a producer thread moves each slice's A and B blocks with two bulk async
+// tile per CTA (accumulator: 128 TMEM lanes x 128 columns; two CTAs per SM) with two single-thread
+// roles over a ring of three 32 KB stages: a producer thread moves each slice's A and B blocks with two bulk async
 // copies (cp.async.bulk, completing on the stage's "full" mbarrier with a byte count), and an MMA
 // thread waits on "full", issues 2 K-steps x 3 tcgen05.mma.kind::tf32 and commits them to the
 // stage's "empty" mbarrier, which releases the stage to the producer.  The other warps join for
@@ -30,14 +30,14 @@ namespace tlr {
 constexpr int kTcM = 128;
 constexpr int kTcN = 128;
 constexpr int kTcBK = 16;                               // k per slice: two MMA K-steps
-constexpr int kTcStages = 6;
+constexpr int kTcStages = 3;                            // two CTAs per SM: one's epilogue overlaps the other's MMAs
 constexpr int kTcThreads = 256;                         // warp 0: copies, warp 1: MMAs, all: epilogue
 constexpr int kTcBlockFloats = 2 * kTcM * kTcBK;        // one operand block: hi + lo, 16 KB
 constexpr int kTcOpBytes = kTcBlockFloats * 4;
 constexpr int kTcStageBytes = 2 * kTcOpBytes;           // A block, then B block
 constexpr int kSplitThreads = 256;
 static_assert(kTcM == kTcN && kTcBK == 16, "block layout assumes 128-row tiles and 16-k slices");
-static_assert(kTcStageBytes * kTcStages + 1024 <= 227 * 1024, "stages exceed shared memory");
+static_assert(2 * (kTcStageBytes * kTcStages + 2048) <= 228 * 1024, "two CTAs per SM exceed shared memory");
 constexpr long long kTcWaitLimit = 1ll << 23;  // polls of about 140 ns on B200: about 1.2 s
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -144,21 +144,15 @@ __device__ __forceinline__ void tc_write4(float* out, const double (&x)[4], int 
   *reinterpret_cast<float4*>(out + kTcM * kTcBK + g * (kTcM * 4) + r * 4) = l;
 }
 
-// One CTA per block (128 rows x 16 k) of the launch's operands; the block's operand is the last
-// job whose block0 is <= blockIdx.x.  Thread (r = tid % 128, g = tid / 128 + 2i) writes k values
-// 4g .. 4g + 3 of tile row r.
-__global__ void __launch_bounds__(kSplitThreads) k_split_tf32(const SplitJob* TLR_RESTRICT jobs, int njobs,
+// One CTA per block (128 rows x 16 k) of an operand: blockIdx.y the operand, blockIdx.x its block.
+// Thread (r = tid % 128, g = tid / 128 + 2i) writes k values 4g .. 4g + 3 of tile row r.
+__global__ void __launch_bounds__(kSplitThreads) k_split_tf32(const SplitJob* TLR_RESTRICT jobs,
                                                             int* TLR_RESTRICT status, int kind) {
   if (*status != 0) return;
-  int lo = 0, hi = njobs - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (jobs[mid].block0 <= (int)blockIdx.x) lo = mid;
-    else hi = mid - 1;
-  }
-  const SplitJob j = jobs[lo];
+  const SplitJob j = jobs[blockIdx.y];
   const int nks = (j.K + kTcBK - 1) / kTcBK;
-  const int blk = (int)blockIdx.x - j.block0;
+  const int blk = (int)blockIdx.x;
+  if (blk >= ((j.rows + kTcM - 1) / kTcM) * nks) return;
   const int row0 = (blk / nks) * kTcM, k0 = (blk % nks) * kTcBK;
   float* out = j.dst + (size_t)blk * kTcBlockFloats;
   const int r = threadIdx.x & (kTcM - 1), gr = row0 + r;
@@ -191,7 +185,7 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
                : "memory");
 }
 
-__global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc3(const GemmJob* TLR_RESTRICT jobs,
+__global__ void __launch_bounds__(kTcThreads, 2) k_gemm_tc3(const GemmJob* TLR_RESTRICT jobs,
                                                  const TcOperands* TLR_RESTRICT ops, int* TLR_RESTRICT status,
                                                  int kind) {
   if (*status != 0) return;
@@ -224,7 +218,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc3(const GemmJob* TLR_R
   const int nk = (jb.K + kTcBK - 1) / kTcBK;
   const uint32_t sbase = smem_u32(tc_smem);
   if (nk > 0 && tid == 0) {
-    // producer: slice s into stage s % 6 once the MMAs of slice s - 6 have released it
+    // producer: slice s into stage s % 3 once the MMAs of slice s - 3 have released it
     const TcOperands op = ops[blockIdx.z];
     const float* pa = op.a + (size_t)(m0 / kTcM) * nk * kTcBlockFloats;
     const float* pb = op.b + (size_t)(n0 / kTcN) * nk * kTcBlockFloats;
@@ -275,7 +269,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc3(const GemmJob* TLR_R
       const int last = nk - 1;
       if (!mbar_wait(smem_u32(&empty[last % kTcStages]), (uint32_t)((last / kTcStages) & 1))) timed_out = 1;
     } else {
-      // failure: let the copies in flight land (the last six slices issued) before leaving
+      // failure: let the copies in flight land (the last slices issued, one per stage) before leaving
       for (int q = max(0, issued - kTcStages); q < issued; ++q)
         mbar_wait(smem_u32(&full[q % kTcStages]), (uint32_t)((q / kTcStages) & 1));
     }
@@ -329,9 +323,9 @@ int launch_wait_selftest(long long limit, int* status, cudaStream_t s) {
 
 long long tc_wait_limit() { return kTcWaitLimit; }
 
-int launch_split_tf32(const SplitJob* jobs, int njobs, int nblocks, int* status, int kind, cudaStream_t s) {
-  if (njobs <= 0 || nblocks <= 0) return 0;
-  k_split_tf32<<<nblocks, kSplitThreads, 0, s>>>(jobs, njobs, status, kind);
+int launch_split_tf32(const SplitJob* jobs, int njobs, int max_blocks, int* status, int kind, cudaStream_t s) {
+  if (njobs <= 0 || max_blocks <= 0) return 0;
+  k_split_tf32<<<dim3((unsigned)max_blocks, (unsigned)njobs), kSplitThreads, 0, s>>>(jobs, status, kind);
   return (int)cudaGetLastError();
 }
 
