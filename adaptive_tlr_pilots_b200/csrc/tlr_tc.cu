@@ -36,6 +36,7 @@ constexpr int kTcBlockFloats = 2 * kTcM * kTcBK;        // one operand block: hi
 constexpr int kTcOpBytes = kTcBlockFloats * 4;
 constexpr int kTcStageBytes = 2 * kTcOpBytes;           // A block, then B block
 constexpr int kSplitThreads = 256;
+constexpr int kSplitPer = 4;                            // blocks per CTA of the split
 static_assert(kTcM == kTcN && kTcBK == 16, "block layout assumes 128-row tiles and 16-k slices");
 static_assert(2 * (kTcStageBytes * kTcStages + 2048) <= 228 * 1024, "two CTAs per SM exceed shared memory");
 constexpr long long kTcWaitLimit = 1ll << 23;  // polls of about 140 ns on B200: about 1.2 s
@@ -144,32 +145,50 @@ __device__ __forceinline__ void tc_write4(float* out, const double (&x)[4], int 
   *reinterpret_cast<float4*>(out + kTcM * kTcBK + g * (kTcM * 4) + r * 4) = l;
 }
 
-// One CTA per block (128 rows x 16 k) of an operand: blockIdx.y the operand, blockIdx.x its block.
-// Thread (r = tid % 128, g = tid / 128 + 2i) writes k values 4g .. 4g + 3 of tile row r.
+// One CTA per kSplitPer consecutive blocks (128 rows x 16 k) of an operand: blockIdx.y the
+// operand, blockIdx.x the group of blocks.  Thread (r = tid % 128, g = tid / 128 + 2i) handles k
+// values 4g .. 4g + 3 of tile row r in each block; every load of the group is issued before the
+// first conversion, so a thread keeps 32 loads in flight.
 __global__ void __launch_bounds__(kSplitThreads) k_split_tf32(const SplitJob* TLR_RESTRICT jobs,
                                                             int* TLR_RESTRICT status, int kind) {
   if (*status != 0) return;
   const SplitJob j = jobs[blockIdx.y];
   const int nks = (j.K + kTcBK - 1) / kTcBK;
-  const int blk = (int)blockIdx.x;
-  if (blk >= ((j.rows + kTcM - 1) / kTcM) * nks) return;
-  const int row0 = (blk / nks) * kTcM, k0 = (blk % nks) * kTcBK;
-  float* out = j.dst + (size_t)blk * kTcBlockFloats;
-  const int r = threadIdx.x & (kTcM - 1), gr = row0 + r;
+  const int nblk = ((j.rows + kTcM - 1) / kTcM) * nks;
+  const int blk0 = (int)blockIdx.x * kSplitPer;
+  if (blk0 >= nblk) return;
+  const int r = threadIdx.x & (kTcM - 1), g0 = threadIdx.x >> 7;
+  constexpr int kG = kTcBK / 4 / (kSplitThreads / kTcM);  // k groups per thread and block: 2
+  double x[kSplitPer][kG][4];
 #pragma unroll
-  for (int g = threadIdx.x >> 7; g < kTcBK / 4; g += kSplitThreads / kTcM) {
-    double x[4];
+  for (int b = 0; b < kSplitPer; ++b) {
+    const int blk = blk0 + b;
+    const int gr = (blk / nks) * kTcM + r, k0 = (blk % nks) * kTcBK;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const int gk = k0 + 4 * g + c;
-      x[c] = (gr < j.rows && gk < j.K) ? (j.kcont ? j.src[(size_t)gr * j.ld + gk] : j.src[(size_t)gk * j.ld + gr])
-                                       : 0.0;
-    }
-    tc_write4(out, x, r, g);
+    for (int i = 0; i < kG; ++i)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int gk = k0 + 4 * (g0 + 2 * i) + c;
+        x[b][i][c] = (blk < nblk && gr < j.rows && gk < j.K)
+                         ? (j.kcont ? j.src[(size_t)gr * j.ld + gk] : j.src[(size_t)gk * j.ld + gr])
+                         : 0.0;
+      }
+  }
+#pragma unroll
+  for (int b = 0; b < kSplitPer; ++b) {
+    if (blk0 + b >= nblk) break;
+    float* out = j.dst + (size_t)(blk0 + b) * kTcBlockFloats;
+#pragma unroll
+    for (int i = 0; i < kG; ++i) tc_write4(out, x[b][i], r, g0 + 2 * i);
   }
   if (threadIdx.x == 0) {
-    const int mt = min(kTcM, j.rows - row0), kt = min(kTcBK, j.K - k0);
-    add_work(status, kind, 0.0, 8.0 * mt * kt + 4.0 * kTcBlockFloats);
+    double bytes = 0.0;
+    for (int b = 0; b < kSplitPer && blk0 + b < nblk; ++b) {
+      const int blk = blk0 + b;
+      const int mt = min(kTcM, j.rows - (blk / nks) * kTcM), kt = min(kTcBK, j.K - (blk % nks) * kTcBK);
+      bytes += 8.0 * mt * kt + 4.0 * kTcBlockFloats;
+    }
+    add_work(status, kind, 0.0, bytes);
   }
 }
 
@@ -325,7 +344,8 @@ long long tc_wait_limit() { return kTcWaitLimit; }
 
 int launch_split_tf32(const SplitJob* jobs, int njobs, int max_blocks, int* status, int kind, cudaStream_t s) {
   if (njobs <= 0 || max_blocks <= 0) return 0;
-  k_split_tf32<<<dim3((unsigned)max_blocks, (unsigned)njobs), kSplitThreads, 0, s>>>(jobs, status, kind);
+  const unsigned gx = (unsigned)((max_blocks + kSplitPer - 1) / kSplitPer);
+  k_split_tf32<<<dim3(gx, (unsigned)njobs), kSplitThreads, 0, s>>>(jobs, status, kind);
   return (int)cudaGetLastError();
 }
 
