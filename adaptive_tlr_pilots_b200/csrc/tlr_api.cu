@@ -62,6 +62,7 @@ struct tlr_plan {
   int nslots = 0, nsm = 148;
   size_t slot_doubles = 0;
   double* rcs = nullptr;
+  int* rc_next = nullptr;  // per factorization step: claims of trailing pairs past the grid
   // look-ahead: POTRF(k+1) runs on a second stream while step k's recompression runs
   cudaStream_t side = nullptr;
   cudaEvent_t ev_panel = nullptr, ev_diag = nullptr;
@@ -220,6 +221,7 @@ int run_compression(tlr_plan* p, double sigma2, double inv_range, int rule_fixed
 int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugget, int rule_fixed, double thr_rel,
                       double thr_abs) {
   cudaStream_t s = p->stream, sd = p->side;
+  TRY(cuda_check(cudaMemsetAsync(p->rc_next, 0, sizeof(int) * p->nB, s), "pair counters"));
   LAUNCH(TLR_K_DIAG, tlr::launch_diag_build(p->xy, p->n, p->b, 0, sigma2, inv_range, p->nu5, nugget, p->U, p->Yd, p->rank,
                                             p->cap, p->D, p->status, s));
   LAUNCH(TLR_K_POTRF, tlr::launch_potrf(p->D, p->n, p->b, 0, p->rhs, p->z, p->ldpart, p->qpart, p->status, s));
@@ -240,7 +242,7 @@ int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugge
     }
     LAUNCH(TLR_K_RECOMPRESS, tlr::launch_recompress(p->n, p->b, k, p->nB, p->U, p->V, p->rank, p->cap, rule_fixed,
                                                     thr_rel, thr_abs, p->rcs, p->slot_doubles, p->nslots, nullptr,
-                                                    nullptr, p->status, s));
+                                                    nullptr, p->rc_next + k, p->status, s));
     if (ahead) TRY(cuda_check(cudaStreamWaitEvent(s, p->ev_diag, 0), "wait"));
   }
   LAUNCH(TLR_K_FINISH, tlr::launch_finish(p->nB, p->n, p->ldpart, p->qpart, p->out, p->status, s));
@@ -643,6 +645,7 @@ int tlr_plan_create(tlr_plan** plan, int n, int b, int cap, int device, void* st
   p->nslots = nsm * 4;  // resident recompression CTAs (k_recompress: four per SM)
   p->slot_doubles = tlr::rc_slot_doubles(b, cap);
   A(dalloc(p, &p->rcs, (size_t)p->nslots * p->slot_doubles));
+  A(dalloc(p, &p->rc_next, (size_t)p->nB));
   if (rc == 0) {
     rc = cuda_check(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking), "side stream");
     if (!rc) rc = cuda_check(cudaEventCreateWithFlags(&p->ev_panel, cudaEventDisableTiming), "event");

@@ -310,7 +310,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
                                                    int rule_fixed, double thr_rel, double thr_abs,
                                                    double* TLR_RESTRICT scratch, size_t slot_doubles,
                                                    const int* TLR_RESTRICT list, const int* TLR_RESTRICT list_count,
-                                                   int* TLR_RESTRICT status) {
+                                                   int* TLR_RESTRICT next_pair, int* TLR_RESTRICT status) {
   if (*status != 0) return;
   const int mB = nB - k - 1;  // trailing tiles
   // every pair of the step, or only the listed ones (those the mixed path's warp kernels pass on)
@@ -336,7 +336,17 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     for (int i = k + 1; i < nB; ++i) by += 8.0 * 2.0 * b * rank[tidx(i, k)];
     add_work(status, 10, 0.0, by);
   }
-  for (long qq = blockIdx.x; qq < npairs; qq += gridDim.x) {
+  // pairs are handed out dynamically: each CTA starts on pair blockIdx.x and then takes the next
+  // unclaimed one (*next_pair counts the claims past the grid; zero at launch), so CTAs that drew
+  // low-rank pairs take more of them
+  __shared__ long q_next;
+  auto claim = [&]() -> long {
+    __syncthreads();
+    if (threadIdx.x == 0) q_next = (long)gridDim.x + atomicAdd(next_pair, 1);
+    __syncthreads();
+    return q_next;
+  };
+  for (long qq = blockIdx.x; qq < npairs; qq = claim()) {
     const long pp = list ? (long)list[qq] : qq;
     // decode pp -> (ii, jj), ii > jj >= 0 within the trailing block
     int ii = (int)((1.0 + sqrt(1.0 + 8.0 * (double)pp)) * 0.5);
@@ -604,7 +614,7 @@ int launch_trsm(const double* D, int n, int b, int k, int nB, const double* U, d
 
 int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, int rule_fixed,
                       double thr_rel, double thr_abs, double* scratch, size_t slot_doubles, int nslots,
-                      const int* list, const int* list_count, int* status, cudaStream_t s) {
+                      const int* list, const int* list_count, int* next_pair, int* status, cudaStream_t s) {
   const long mB = nB - k - 1;
   const long npairs = mB * (mB - 1) / 2;
   if (npairs <= 0) return 0;
@@ -612,7 +622,7 @@ int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* ra
   const size_t sm = (size_t)3 * kRcSmemS * kRcSmemS * 8;
   cudaFuncSetAttribute(k_recompress, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   k_recompress<<<grid, kRcT, sm, s>>>(n, b, k, nB, U, V, rank, cap, rule_fixed, thr_rel, thr_abs, scratch,
-                                     slot_doubles, list, list_count, status);
+                                     slot_doubles, list, list_count, next_pair, status);
   return (int)cudaGetLastError();
 }
 

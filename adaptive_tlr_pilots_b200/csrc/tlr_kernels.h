@@ -47,10 +47,11 @@ int launch_potrf_batched(double* D, int n, int b, int k, double* rhs, double* z,
 int launch_trsm(const double* D, int n, int b, int k, int nB, const double* U, double* V, double* Wd, double* Y,
                 const int* rank, int cap, const double* z, double* rhs, const int* status, cudaStream_t s);
 size_t rc_slot_doubles(int b, int cap);
-// every trailing pair of step k, or (list != NULL) the *list_count pairs listed
+// every trailing pair of step k, or (list != NULL) the *list_count pairs listed; next_pair: a
+// counter that is zero at launch (the CTAs claim pairs past the grid through it)
 int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, int rule_fixed,
                       double thr_rel, double thr_abs, double* scratch, size_t slot_doubles, int nslots,
-                      const int* list, const int* list_count, int* status, cudaStream_t s);
+                      const int* list, const int* list_count, int* next_pair, int* status, cudaStream_t s);
 int launch_finish(int nB, int n, const double* ldpart, const double* qpart, double* out, const int* status,
                   cudaStream_t s);
 
