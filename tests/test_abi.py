@@ -44,3 +44,26 @@ def test_kernel_switch_validates_and_restores():
         setter(2.5)
         setter(1.5)
     assert tlr.get_kernel() == 1.5 and O.NU == 1.5
+
+
+def test_gemm_selftest_rejects_bad_arguments_without_a_gpu():
+    """tlr_selftest_gemm checks its arguments before touching a device: unknown precision,
+    negative sizes, leading dimensions below the matrix height and missing matrices are errors."""
+    lib = _lib.load()
+    mixed = _lib.PRECISIONS["mixed"]
+    cases = [
+        (7, 0, 0, 4, 4, 4, 4, 4, 4),          # precision
+        (mixed, 0, 0, -1, 4, 4, 4, 4, 4),     # M < 0
+        (mixed, 0, 0, 4, 4, 4, 2, 4, 4),      # lda < M
+        (mixed, 1, 0, 4, 4, 8, 4, 8, 4),      # lda < K for op(A) = A^T
+        (mixed, 0, 1, 4, 6, 4, 4, 4, 4),      # ldb < N for op(B) = B^T
+        (mixed, 0, 0, 4, 4, 4, 4, 4, 3),      # ldc < M
+    ]
+    for prec, ta, tb, M, N, K, lda, ldb, ldc in cases:
+        rc = lib.tlr_selftest_gemm(prec, ta, tb, M, N, K, 1.0, None, lda, None, ldb, 0.0, None, ldc, 0)
+        assert rc < 0, (prec, ta, tb, M, N, K, lda, ldb, ldc)
+    # sizes are fine but the matrices are missing
+    assert lib.tlr_selftest_gemm(mixed, 0, 0, 4, 4, 4, 1.0, None, 4, None, 4, 0.0, None, 4, 0) < 0
+    assert "NULL" in _lib.last_error()
+    # an empty product is a no-op that needs no device
+    assert lib.tlr_selftest_gemm(mixed, 0, 0, 0, 4, 4, 1.0, None, 1, None, 4, 0.0, None, 1, 0) == 0
