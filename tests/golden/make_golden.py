@@ -97,7 +97,8 @@ def main():
     xy[44:60] = np.round(xy[44:60] * 8) / 8
     np.savez(os.path.join(HERE, "morton_case.npz"), xy=xy, perm=rules.morton_order(xy))
 
-    # 2. dense and TLR log-likelihoods on the BASELINE first config and smaller/ragged cases
+    # 2. dense and TLR log-likelihoods on the N = 4,000, b = 250 field (adaptive tau = 0.9, fixed
+    #    eps = 1e-3 and 1e-4) and on smaller / ragged cases
     configs = [
         dict(name="n4000_b250", n=4000, b=250, theta=theta,
              specs=[("adaptive", 0.9), ("fixed", 1e-3), ("fixed", 1e-4)], save_data=True),
