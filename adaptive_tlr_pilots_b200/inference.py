@@ -282,41 +282,61 @@ def run_chains(obj, starts, iters, burn, seeds, kind="rw", scale0=None, ckpt=Non
 
 
 # ---------------------------------------------------------------------------------- diagnostics
+def _rank_normal_scores(x):
+    """Normal scores of the pooled ranks of x (ties share their average rank), with Blom's
+    offset: Phi^-1((rank - 3/8) / (S + 1/4)), S = x.size (Vehtari et al. 2021, eq. 14)."""
+    from scipy.special import ndtri
+    flat = x.ravel()
+    order = np.argsort(flat, kind="mergesort")
+    srt = flat[order]
+    # average rank of each run of equal values: (first + last) / 2 of its 1-based positions
+    edges = np.flatnonzero(np.diff(srt) != 0) + 1
+    starts = np.concatenate(([0], edges))
+    stops = np.concatenate((edges, [srt.size]))
+    avg = 0.5 * (starts + 1 + stops)
+    ranks = np.empty(flat.size)
+    ranks[order] = np.repeat(avg, stops - starts)
+    return ndtri((ranks - 0.375) / (flat.size + 0.25)).reshape(x.shape)
+
+
 def split_rhat_ess(chains):
-    """Rank-normalised split R-hat and bulk effective sample size (Vehtari, Gelman, Simpson,
-    Carpenter and Buerkner 2021) of draws shaped (M chains, n draws): the chains are split in
-    halves, the pooled draws rank-normalised through the normal quantile function, R-hat from
-    the between/within variances, ESS from the pooled autocorrelation summed over Geyer's
-    initial positive sequence.  Same estimator as codes/35_mcmc_multichain_diagnostics.py:26-59."""
-    from scipy import stats
+    """Rank-normalised split R-hat and bulk effective sample size of draws shaped (M chains,
+    n draws), following Vehtari, Gelman, Simpson, Carpenter and Buerkner (2021), "Rank-
+    normalization, folding, and localization: an improved R-hat", Bayesian Analysis 16:667-718.
+
+    * Every chain is cut into its first and second half (2M sequences of n // 2 draws); all the
+      draws are rank-normalised together (_rank_normal_scores).
+    * R-hat = sqrt(var+ / W), var+ = (h - 1) / h W + B / h, W the mean within-sequence variance,
+      B / h the variance of the sequence means.
+    * The autocovariance of every sequence at every lag comes from one zero-padded FFT over the
+      sequence axis; rho_t = 1 - (W - mean autocovariance_t) / var+ combines the sequences.
+    * ESS = (2M h) / tau with tau = -1 + 2 sum_t P_t over Geyer's (1992, Statistical Science 7:
+      473-483) initial monotone sequence of lag pairs P_t = rho_2t + rho_2t+1: cut at the first
+      negative pair, then made non-increasing; tau is bounded below by 1 / log10(2M h) as the
+      paper does.
+    The reference's codes/35_mcmc_multichain_diagnostics.py reports the same two diagnostics for
+    its chains."""
     x = np.asarray(chains, dtype=np.float64)
     M, n = x.shape
-    half = n // 2
-    x = np.concatenate([x[:, :half], x[:, half:2 * half]], axis=0)
-    r = stats.rankdata(x, method="average").reshape(x.shape)
-    z = stats.norm.ppf((r - 0.375) / (x.size + 0.25))
-    m, nn = z.shape
-    means = z.mean(axis=1)
+    h = n // 2
+    seq = x[:, :2 * h].reshape(2 * M, h)
+    z = _rank_normal_scores(seq)
+    m = z.shape[0]
+    mu = z.mean(axis=1)
     W = z.var(axis=1, ddof=1).mean()
-    B = nn * means.var(ddof=1)
-    var_hat = (nn - 1) / nn * W + B / nn
-    rhat = float(np.sqrt(var_hat / W))
-    acov = np.zeros(nn)
-    for row in z:
-        d = row - row.mean()
-        f = np.fft.rfft(d, 2 * nn)
-        acov += np.fft.irfft(f * np.conj(f))[:nn] / nn
-    acov /= m
-    rho = 1.0 - (W - acov) / var_hat
-    tau, t = -1.0, 0
-    while t + 1 < nn:
-        pair = rho[t] + rho[t + 1]
-        if pair < 0:
-            break
-        tau += 2.0 * pair
-        t += 2
-    ess = m * nn / max(tau, 1e-12)
-    return rhat, float(min(ess, 2.0 * m * nn))
+    var_plus = (h - 1) / h * W + mu.var(ddof=1)
+    rhat = float(np.sqrt(var_plus / W))
+    dev = z - mu[:, None]
+    spec = np.fft.rfft(dev, n=2 * h, axis=1)
+    acov = np.fft.irfft(spec * np.conj(spec), n=2 * h, axis=1)[:, :h] / h
+    rho = 1.0 - (W - acov.mean(axis=0)) / var_plus
+    npair = h // 2
+    pairs = rho[0:2 * npair:2] + rho[1:2 * npair:2]
+    negative = np.flatnonzero(pairs < 0.0)
+    pairs = pairs[:negative[0] if negative.size else npair]
+    pairs = np.minimum.accumulate(pairs)
+    tau = max(-1.0 + 2.0 * float(pairs.sum()), 1.0 / np.log10(m * h))
+    return rhat, float(m * h / tau)
 
 
 def summarize(chains, burn):
