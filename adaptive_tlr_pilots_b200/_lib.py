@@ -15,6 +15,8 @@ LIB_PATH = os.path.join(HERE, "libtlr_b200.so")
 TLR_RULE_FIXED = 0
 TLR_RULE_ADAPTIVE = 1
 PRECISIONS = {"fp64": 0, "mixed": 1}
+RANK_MAP = {"rule": 0, "record": 1, "replay": 2}
+ERR_RANK_CAP = -2  # TLR_ERR_RANK_CAP: a tile rank exceeded the plan's capacity
 
 _lib = None
 
@@ -67,6 +69,7 @@ SIGNATURES = {
     "tlr_get_offdiag_tile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                             ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "tlr_plan_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tlr_plan_rank_map": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tlr_plan_set_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "tlr_plan_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tlr_plan_kernel_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),

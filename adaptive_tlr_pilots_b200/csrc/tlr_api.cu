@@ -85,6 +85,11 @@ struct tlr_plan {
   bool factor_ok = false;  // the last evaluation completed: D, U, V, rank hold its factor
   std::vector<void*> allocs;
   int precision = TLR_PRECISION_FP64;
+  // rank map (tlr_plan_rank_map): ntiles initial ranks, then per step k the ranks of its trailing
+  // pairs from rlog_off[k]
+  int* rlog = nullptr;
+  int rmode = 0;
+  std::vector<size_t> rlog_off;
   // launch accounting and optional per-kernel event timing
   bool prof = false;
   int nu5 = 0;  // covariance: 0 Matern 3/2, 1 Matern 5/2
@@ -212,7 +217,7 @@ int run_compression(tlr_plan* p, double sigma2, double inv_range, int rule_fixed
       }
       LAUNCH(TLR_K_FINALIZE, tlr::launch_finalize(p->n, p->b, k, ldp, p->cap, kMargin, rule_fixed, thr_rel, thr_abs, base, p->ti,
                                 p->tj, p->need, Pp, p->C, p->parts, p->fparts, fused ? 1 : p->nblk, p->gscr, p->gsv, p->U,
-                                p->V, p->rank, lev == kLevels - 1 ? 1 : 0, nc, p->status, s));
+                                p->V, p->rank, lev == kLevels - 1 ? 1 : 0, nc, p->rlog, p->rmode, p->status, s));
     }
   }
   return 0;
@@ -241,8 +246,9 @@ int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugge
       TRY(cuda_check(cudaEventRecord(p->ev_diag, sd), "event"));
     }
     LAUNCH(TLR_K_RECOMPRESS, tlr::launch_recompress(p->n, p->b, k, p->nB, p->U, p->V, p->rank, p->cap, rule_fixed,
-                                                    thr_rel, thr_abs, p->rcs, p->slot_doubles, p->nslots, nullptr,
-                                                    nullptr, p->rc_next + k, p->status, s));
+                                                    thr_rel, thr_abs, p->rcs, p->slot_doubles, p->nslots,
+                                                    p->rc_next + k, p->rlog + p->rlog_off[k], p->rmode, p->status,
+                                                    s));
     if (ahead) TRY(cuda_check(cudaStreamWaitEvent(s, p->ev_diag, 0), "wait"));
   }
   LAUNCH(TLR_K_FINISH, tlr::launch_finish(p->nB, p->n, p->ldpart, p->qpart, p->out, p->status, s));
@@ -646,6 +652,16 @@ int tlr_plan_create(tlr_plan** plan, int n, int b, int cap, int device, void* st
   p->slot_doubles = tlr::rc_slot_doubles(b, cap);
   A(dalloc(p, &p->rcs, (size_t)p->nslots * p->slot_doubles));
   A(dalloc(p, &p->rc_next, (size_t)p->nB));
+  // rank map: the initial ranks, then the trailing pairs of every step
+  p->rlog_off.assign((size_t)p->nB + 1, 0);
+  size_t rl = nt;
+  for (int k = 0; k < p->nB; ++k) {
+    p->rlog_off[k] = rl;
+    const size_t mB = (size_t)(p->nB - k - 1);
+    rl += mB * (mB > 0 ? mB - 1 : 0) / 2;
+  }
+  p->rlog_off[p->nB] = rl;
+  A(dalloc(p, &p->rlog, rl));
   if (rc == 0) {
     rc = cuda_check(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking), "side stream");
     if (!rc) rc = cuda_check(cudaEventCreateWithFlags(&p->ev_panel, cudaEventDisableTiming), "event");
@@ -716,22 +732,15 @@ int tlr_morton_order(const double* xy_dev, int n, int order, long long* perm_dev
   if (n < 1 || !xy_dev || !perm_dev) return fail(TLR_ERR_ARG, "invalid arguments to tlr_morton_order");
   if (order < 1 || order > 12) return fail(TLR_ERR_ARG, "order must be in [1, 12]");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const size_t nbuckets = (size_t)1 << (2 * order);
-  unsigned *keys = nullptr, *cnt = nullptr, *off = nullptr, *cur = nullptr;
-  cudaError_t e = cudaMallocAsync(&keys, sizeof(unsigned) * n, s);
-  if (e == cudaSuccess) e = cudaMallocAsync(&cnt, sizeof(unsigned) * nbuckets, s);
-  if (e == cudaSuccess) e = cudaMallocAsync(&off, sizeof(unsigned) * nbuckets, s);
-  if (e == cudaSuccess) e = cudaMallocAsync(&cur, sizeof(unsigned) * nbuckets, s);
+  unsigned* work = nullptr;
+  const cudaError_t e = cudaMallocAsync(&work, sizeof(unsigned) * tlr::morton_work_words(n, order), s);
   int rc = 0;
   if (e != cudaSuccess) rc = fail(TLR_ERR_NOMEM, std::string("morton scratch: ") + cudaGetErrorString(e));
   if (!rc) {
-    const int lr = tlr::launch_morton(xy_dev, n, order, keys, cnt, off, cur, perm_dev, s);
+    const int lr = tlr::launch_morton(xy_dev, n, order, work, perm_dev, s);
     if (lr) rc = fail(TLR_ERR_CUDA, std::string("morton launch: ") + cudaGetErrorString((cudaError_t)lr));
   }
-  if (keys) cudaFreeAsync(keys, s);
-  if (cnt) cudaFreeAsync(cnt, s);
-  if (off) cudaFreeAsync(off, s);
-  if (cur) cudaFreeAsync(cur, s);
+  if (work) cudaFreeAsync(work, s);
   if (!rc) rc = cuda_check(cudaStreamSynchronize(s), "morton sync");
   return rc;
 }
@@ -946,6 +955,15 @@ int tlr_plan_set_precision(tlr_plan* p, int mode) {
   if (!p) return fail(TLR_ERR_ARG, "plan is NULL");
   if (mode != TLR_PRECISION_FP64 && mode != TLR_PRECISION_MIXED) return fail(TLR_ERR_ARG, "unknown precision mode");
   p->precision = mode;
+  return 0;
+}
+
+int tlr_plan_rank_map(tlr_plan* p, int mode) {
+  if (!p) return fail(TLR_ERR_ARG, "plan is NULL");
+  if (mode != TLR_RANKS_RULE && mode != TLR_RANKS_RECORD && mode != TLR_RANKS_REPLAY)
+    return fail(TLR_ERR_ARG, "rank map mode must be TLR_RANKS_RULE, TLR_RANKS_RECORD or TLR_RANKS_REPLAY");
+  static_assert(TLR_RANKS_RECORD == tlr::kRankRecord && TLR_RANKS_REPLAY == tlr::kRankReplay, "rank map modes");
+  p->rmode = mode;
   return 0;
 }
 

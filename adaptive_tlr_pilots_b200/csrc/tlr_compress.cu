@@ -639,7 +639,8 @@ __global__ void __launch_bounds__(1024) k_finalize(int n, int b, int k, int ldp,
                                                  double* TLR_RESTRICT gscratch, double* TLR_RESTRICT gsv,
                                                  double* TLR_RESTRICT Uo,
                                                  double* TLR_RESTRICT Vo, int* TLR_RESTRICT rank,
-                                                 int last_level, int w_in_smem, int* TLR_RESTRICT status) {
+                                                 int last_level, int w_in_smem, int* TLR_RESTRICT rlog,
+                                                 int rmode, int* TLR_RESTRICT status) {
   if (*status != 0) return;
   const int c = blockIdx.x;
   if (!need[c]) return;
@@ -674,7 +675,8 @@ __global__ void __launch_bounds__(1024) k_finalize(int n, int b, int k, int ldp,
     double sorted[128];
     for (int q = 0; q < k; ++q) sorted[q] = sig[perm[q]];
     const double thr = rule_fixed ? thr_rel * sqrt(fro2) : thr_abs;
-    const int r = select_rank(sorted, k, rho2, thr, nullptr);
+    int r = select_rank(sorted, k, rho2, thr, nullptr);
+    if (rmode == kRankReplay) r = rlog[t];  // frozen: the rank recorded at another theta
     const bool exact = (k >= bj) || (k >= bi);
     int out;
     if (r >= 0 && (r <= k - margin || exact)) out = r;
@@ -708,7 +710,11 @@ __global__ void __launch_bounds__(1024) k_finalize(int n, int b, int k, int ldp,
     for (int u = 0; u < k; ++u) s = fma(P[pbase + (size_t)u * b + row], w[u], s);
     Vt[(size_t)q * b + row] = s;
   }
-  if (threadIdx.x == 0) { rank[t] = r; need[c] = 0; }
+  if (threadIdx.x == 0) {
+    rank[t] = r;
+    need[c] = 0;
+    if (rmode == kRankRecord) rlog[t] = r;
+  }
 }
 
 // ----------------------------------------------------------------------------------------
@@ -796,15 +802,15 @@ int launch_resid(const double* T, int n, int b, int k, int ldp, int tile_base, c
 int launch_finalize(int n, int b, int k, int ldp, int cap, int margin, int rule_fixed, double thr_rel,
                     double thr_abs, int tile_base, const int* ti, const int* tj, int* need, const double* P,
                     const double* C, const double* parts, const double* fparts, int nblk, double* gscratch,
-                    double* gsv, double* U, double* V, int* rank, int last_level, int nchunk, int* status,
-                    cudaStream_t s) {
+                    double* gsv, double* U, double* V, int* rank, int last_level, int nchunk, int* rlog,
+                    int rmode, int* status, cudaStream_t s) {
   size_t sm = (40 + 136 * 3 + 8 + (k <= 64 ? 2 * (size_t)k * k : 0)) * 8;
   const int w_in_smem = k <= 64 && (size_t)b * k * 8 <= 160 * 1024;
   if (w_in_smem) sm += (size_t)b * k * 8;
   cudaFuncSetAttribute(k_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   k_finalize<<<nchunk, k >= 32 ? 1024 : 256, sm, s>>>(n, b, k, ldp, cap, margin, rule_fixed, thr_rel, thr_abs, tile_base, ti, tj, need,
                                      P, C, parts, fparts, nblk, gscratch, gsv, U, V, rank, last_level, w_in_smem,
-                                     status);
+                                     rlog, rmode, status);
   return (int)cudaGetLastError();
 }
 

@@ -129,7 +129,6 @@ __global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int 
   __shared__ double L11[32][33];
   __shared__ double dinv[32];
   __shared__ double Xp[32][65];
-  __shared__ double red[40];
   __shared__ double zt[64];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int q0 = 0; q0 < r; q0 += 64) {
@@ -213,7 +212,6 @@ __global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int 
     }
   }
   __syncthreads();
-  (void)red;
   // Y_ik = U_ik W_ik, the factor of the deferred diagonal update of tile i
   double* Yt = Y + (size_t)t * b * cap;
   for (int a = tid; a < bi; a += 256)
@@ -286,7 +284,7 @@ size_t rc_slot_doubles(int b, int cap) {
 
 // C (p x q, ld p) = A^T B with A (m x p, lda), B (m x q, ldb): one warp per entry.
 __device__ void cta_atb(const double* A, int lda, const double* B, int ldb, int m, int p, int q, double* C,
-                        int ldc, double scale_a_inv_by_norm /*unused*/) {
+                        int ldc) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   for (int e = warp; e < p * q; e += nwarp) {
     const int u = e % p, v = e / p;
@@ -297,7 +295,6 @@ __device__ void cta_atb(const double* A, int lda, const double* B, int ldb, int 
     s = warp_sum(s);
     if (lane == 0) C[(size_t)v * ldc + u] = s;
   }
-  (void)scale_a_inv_by_norm;
 }
 
 constexpr int kRcSmemS = 32;  // cores with s <= 32 are solved in shared memory
@@ -309,12 +306,11 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
                                                    double* TLR_RESTRICT V, int* TLR_RESTRICT rank, int cap,
                                                    int rule_fixed, double thr_rel, double thr_abs,
                                                    double* TLR_RESTRICT scratch, size_t slot_doubles,
-                                                   const int* TLR_RESTRICT list, const int* TLR_RESTRICT list_count,
-                                                   int* TLR_RESTRICT next_pair, int* TLR_RESTRICT status) {
+                                                   int* TLR_RESTRICT next_pair, int* TLR_RESTRICT rlog, int rmode,
+                                                   int* TLR_RESTRICT status) {
   if (*status != 0) return;
   const int mB = nB - k - 1;  // trailing tiles
-  // every pair of the step, or only the listed ones (those the mixed path's warp kernels pass on)
-  const long npairs = list ? (long)*list_count : (long)mB * (mB - 1) / 2;
+  const long npairs = (long)mB * (mB - 1) / 2;  // every trailing pair (i, j), k < j < i
   RcScratch S = rc_slot(scratch + (size_t)blockIdx.x * slot_doubles, b, cap);
   extern __shared__ double rc_smem[];
   double* Msm = rc_smem;                            // kRcSmemS^2
@@ -331,7 +327,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
   __shared__ int rsel;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int ls = 2 * cap;
-  if (blockIdx.x == 0 && tid == 0 && !list) {  // the panel column k is read once per step
+  if (blockIdx.x == 0 && tid == 0) {  // the panel column k is read once per step
     double by = 0.0;
     for (int i = k + 1; i < nB; ++i) by += 8.0 * 2.0 * b * rank[tidx(i, k)];
     add_work(status, 10, 0.0, by);
@@ -347,7 +343,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     return q_next;
   };
   for (long qq = blockIdx.x; qq < npairs; qq = claim()) {
-    const long pp = list ? (long)list[qq] : qq;
+    const long pp = qq;
     // decode pp -> (ii, jj), ii > jj >= 0 within the trailing block
     int ii = (int)((1.0 + sqrt(1.0 + 8.0 * (double)pp)) * 0.5);
     while ((long)ii * (ii - 1) / 2 > pp) --ii;
@@ -372,7 +368,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     const int lc = core_in_smem ? kRcSmemS : ls;
     __syncthreads();
     // W = V_ik^T V_jk (ri x rj); column norms of U_ij
-    cta_atb(Vik, b, Vjk, b, bk, ri, rj, S.W, cap, 0.0);
+    cta_atb(Vik, b, Vjk, b, bk, ri, rj, S.W, cap);
     for (int c = warp; c < r1; c += kRcW) {
       const double* u = Uij + (size_t)c * b;
       const double* v = Vij + (size_t)c * b;
@@ -432,7 +428,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     __syncthreads();
     for (int pass = 0; pass < 2; ++pass) {
       if (r1 > 0) {
-        cta_atb(Vij, b, S.Y, b, bj, r1, rj, S.G, cap, 0.0);
+        cta_atb(Vij, b, S.Y, b, bj, r1, rj, S.G, cap);
         __syncthreads();
         for (int e = tid; e < r1 * rj; e += kRcT) S.G[(size_t)(e / r1) * cap + (e % r1)] *= nvinv[e % r1];
         __syncthreads();
@@ -478,7 +474,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     }
     // re-orthogonalise Q3 against the normalised V_ij once
     if (r1 > 0) {
-      cta_atb(Vij, b, S.Y, b, bj, r1, rj, S.G, cap, 0.0);
+      cta_atb(Vij, b, S.Y, b, bj, r1, rj, S.G, cap);
       __syncthreads();
       for (int v = 0; v < rj; ++v)
         for (int a = tid; a < bj; a += kRcT) {
@@ -523,6 +519,8 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
       const double thr = rule_fixed ? thr_rel * sqrt(fro2) : thr_abs;
       int r = select_rank(srt, s, 0.0, thr, nullptr);
       if (r < 0) r = s;
+      if (rmode == kRankReplay) r = min(rlog[pp], s);  // frozen: the rank recorded at another theta
+      else if (rmode == kRankRecord) rlog[pp] = r;
       if (r > cap) {
         atomicCAS(status, 0, -2);
         r = -1;
@@ -614,7 +612,7 @@ int launch_trsm(const double* D, int n, int b, int k, int nB, const double* U, d
 
 int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, int rule_fixed,
                       double thr_rel, double thr_abs, double* scratch, size_t slot_doubles, int nslots,
-                      const int* list, const int* list_count, int* next_pair, int* status, cudaStream_t s) {
+                      int* next_pair, int* rlog_step, int rmode, int* status, cudaStream_t s) {
   const long mB = nB - k - 1;
   const long npairs = mB * (mB - 1) / 2;
   if (npairs <= 0) return 0;
@@ -622,7 +620,7 @@ int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* ra
   const size_t sm = (size_t)3 * kRcSmemS * kRcSmemS * 8;
   cudaFuncSetAttribute(k_recompress, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   k_recompress<<<grid, kRcT, sm, s>>>(n, b, k, nB, U, V, rank, cap, rule_fixed, thr_rel, thr_abs, scratch,
-                                     slot_doubles, list, list_count, next_pair, status);
+                                     slot_doubles, next_pair, rlog_step, rmode, status);
   return (int)cudaGetLastError();
 }
 

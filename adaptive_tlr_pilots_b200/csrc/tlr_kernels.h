@@ -6,9 +6,15 @@
 
 namespace tlr {
 
-// Morton order (codes/11_tlr_rank_rules.py:40-53)
-int launch_morton(const double* xy, int n, int order, unsigned* keys, unsigned* cnt, unsigned* off,
-                  unsigned* cursor, long long* perm, cudaStream_t s);
+// Rank map: every rank the rule picks (initial compression of tile t at rlog[t], recompression of
+// trailing pair p of step k at rlog[ntiles + off_k + p]) is recorded, or replayed instead of the
+// rule's choice (frozen ranks at another theta).
+constexpr int kRankOff = 0, kRankRecord = 1, kRankReplay = 2;
+
+// Morton order (codes/11_tlr_rank_rules.py:40-53): stable radix sort of the keys.  `work` holds
+// morton_work_words(n, order) unsigned words; perm (n int64) doubles as the sort's second buffer.
+size_t morton_work_words(int n, int order);
+int launch_morton(const double* xy, int n, int order, unsigned* work, long long* perm, cudaStream_t s);
 int launch_gather_sites(const double* xy_in, const double* y_in, const long long* perm, int n, double* xy_out,
                         double* y_out, cudaStream_t s);
 
@@ -32,8 +38,8 @@ int launch_resid(const double* T, int n, int b, int k, int ldp, int tile_base, c
 int launch_finalize(int n, int b, int k, int ldp, int cap, int margin, int rule_fixed, double thr_rel,
                     double thr_abs, int tile_base, const int* ti, const int* tj, int* need, const double* P,
                     const double* C, const double* parts, const double* fparts, int nblk, double* gscratch,
-                    double* gsv, double* U, double* V, int* rank, int last_level, int nchunk, int* status,
-                    cudaStream_t s);
+                    double* gsv, double* U, double* V, int* rank, int last_level, int nchunk, int* rlog,
+                    int rmode, int* status, cudaStream_t s);
 
 // factorization
 int launch_diag_build(const double* xy, int n, int b, int k, double sigma2, double inv_range, int nu5,
@@ -47,11 +53,11 @@ int launch_potrf_batched(double* D, int n, int b, int k, double* rhs, double* z,
 int launch_trsm(const double* D, int n, int b, int k, int nB, const double* U, double* V, double* Wd, double* Y,
                 const int* rank, int cap, const double* z, double* rhs, const int* status, cudaStream_t s);
 size_t rc_slot_doubles(int b, int cap);
-// every trailing pair of step k, or (list != NULL) the *list_count pairs listed; next_pair: a
-// counter that is zero at launch (the CTAs claim pairs past the grid through it)
+// every trailing pair of step k; next_pair: a counter that is zero at launch (the CTAs claim
+// pairs past the grid through it)
 int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, int rule_fixed,
                       double thr_rel, double thr_abs, double* scratch, size_t slot_doubles, int nslots,
-                      const int* list, const int* list_count, int* next_pair, int* status, cudaStream_t s);
+                      int* next_pair, int* rlog_step, int rmode, int* status, cudaStream_t s);
 int launch_finish(int nB, int n, const double* ldpart, const double* qpart, double* out, const int* status,
                   cudaStream_t s);
 

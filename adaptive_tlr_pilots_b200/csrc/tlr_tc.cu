@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_gemm_tc3(const GemmJob* TLR_R
   extern __shared__ __align__(1024) unsigned char tc_smem[];
   __shared__ __align__(8) uint64_t full[kTcStages], empty[kTcStages];
   __shared__ uint32_t tmem_base_sh;
-  __shared__ int timed_out, issued;
+  __shared__ int timed_out, issued, committed;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
@@ -229,6 +229,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_gemm_tc3(const GemmJob* TLR_R
     asm volatile("fence.mbarrier_init.release.cluster;");
     timed_out = 0;
     issued = 0;
+    committed = 0;
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
@@ -258,7 +259,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_gemm_tc3(const GemmJob* TLR_R
     // MMA issuer
     const uint32_t idesc = umma_idesc_tf32(kTcM, kTcN);
     const uint32_t lbo = kTcM * 16, sbo = 128;
-    for (int s = 0; s < nk; ++s) {
+    int s = 0;
+    for (; s < nk; ++s) {
       const int st = s % kTcStages;
       if (!mbar_wait(smem_u32(&full[st]), (uint32_t)((s / kTcStages) & 1))) {
         timed_out = 1;
@@ -279,6 +281,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_gemm_tc3(const GemmJob* TLR_R
       }
       mma_commit(smem_u32(&empty[st]));
     }
+    committed = s;
   }
   __syncwarp();
   __syncthreads();
@@ -288,9 +291,14 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_gemm_tc3(const GemmJob* TLR_R
       const int last = nk - 1;
       if (!mbar_wait(smem_u32(&empty[last % kTcStages]), (uint32_t)((last / kTcStages) & 1))) timed_out = 1;
     } else {
-      // failure: let the copies in flight land (the last slices issued, one per stage) before leaving
+      // failure: let the copies in flight land (the last slices issued, one per stage), and the
+      // MMAs already issued finish (their last commit), before the tensor memory is released
       for (int q = max(0, issued - kTcStages); q < issued; ++q)
         mbar_wait(smem_u32(&full[q % kTcStages]), (uint32_t)((q / kTcStages) & 1));
+      if (committed > 0) {
+        const int last = committed - 1;
+        mbar_wait(smem_u32(&empty[last % kTcStages]), (uint32_t)((last / kTcStages) & 1));
+      }
     }
   }
   __syncthreads();

@@ -97,6 +97,8 @@ class Evaluation:
 class Plan:
     """Device workspace for one (N, b) problem: owns a tlr_plan of the C ABI."""
 
+    MAX_CAP = 128  # the C plan's largest rank capacity
+
     def __init__(self, n, b, cap=64, device=0):
         torch = _torch()
         self.lib = _lib.load()
@@ -105,14 +107,42 @@ class Plan:
         self.ntiles = self.nB * (self.nB - 1) // 2
         self.dev = torch.device("cuda", self.device)
         self.stream = torch.cuda.current_stream(self.dev)
+        self.handle = None
+        self.generation = 0
+        self._data = None
+        self.precision = "fp64"
+        self.nu = None          # None: follow set_kernel; else this plan's own smoothness
+        self._create()
+
+    def _create(self):
         h = ctypes.c_void_p()
         _lib.check(self.lib.tlr_plan_create(ctypes.byref(h), self.n, self.b, self.cap, self.device,
                                             ctypes.c_void_p(self.stream.cuda_stream)))
         self.handle = h
-        self.generation = 0
-        self._data = None
-        self.nu = None          # None: follow set_kernel; else this plan's own smoothness
         self._nu_applied = 1.5  # the C plan starts with Matern 3/2
+
+    def grow(self, cap=None):
+        """Recreate the device workspace with a larger rank capacity (default: double, at most
+        MAX_CAP), keeping the loaded data, precision and kernel.  Returns False when the capacity
+        is already the largest."""
+        new = min(self.MAX_CAP, int(cap) if cap is not None else 2 * self.cap)
+        if new <= self.cap:
+            return False
+        self.close()
+        self.cap = new
+        self._create()
+        if self.precision != "fp64":
+            _lib.check(self.lib.tlr_plan_set_precision(self.handle, _lib.PRECISIONS[self.precision]))
+        self._apply_kernel()
+        if getattr(self, "rank_mode", "rule") != "rule":
+            # a recorded map does not survive the new workspace: record again
+            self.rank_map("record")
+        if self._data is not None:
+            S_t, y_t = self._data
+            _lib.check(self.lib.tlr_set_data(self.handle, ctypes.c_void_p(S_t.data_ptr()),
+                                             ctypes.c_void_p(y_t.data_ptr())))
+        self.generation += 1
+        return True
 
     def set_kernel(self, nu):
         """This plan's covariance smoothness (1.5 or 2.5), independent of set_kernel."""
@@ -150,7 +180,19 @@ class Plan:
                                          ctypes.c_void_p(y_t.data_ptr())))
 
     def evaluate(self, theta, rule, value, host_S=None, host_y=None, grad=False) -> Evaluation:
-        """One log-likelihood evaluation (and its gradient when grad=True) on the device."""
+        """One log-likelihood evaluation (and its gradient when grad=True) on the device.
+
+        A tile rank above the plan's capacity does not end the call: the workspace is recreated
+        with twice the capacity (up to MAX_CAP) and the evaluation repeated, so the call succeeds
+        wherever the reference's does, up to ranks of MAX_CAP."""
+        while True:
+            try:
+                return self._evaluate(theta, rule, value, host_S, host_y, grad)
+            except _lib.TlrError as e:
+                if e.code != _lib.ERR_RANK_CAP or not self.grow():
+                    raise
+
+    def _evaluate(self, theta, rule, value, host_S, host_y, grad) -> Evaluation:
         if rule not in RULES:
             raise ValueError(f"rule must be one of {sorted(RULES)}, got {rule!r}")
         self._apply_kernel()
@@ -196,6 +238,14 @@ class Plan:
             raise ValueError(f"precision must be one of {sorted(_lib.PRECISIONS)}")
         _lib.check(self.lib.tlr_plan_set_precision(self.handle, _lib.PRECISIONS[mode]))
         self.precision = mode
+
+    def rank_map(self, mode):
+        """'rule' (the rule picks every rank), 'record' (and they are recorded) or 'replay' (the
+        recorded ranks replace the rule's: frozen ranks at another theta)."""
+        if mode not in _lib.RANK_MAP:
+            raise ValueError(f"rank map mode must be one of {sorted(_lib.RANK_MAP)}")
+        _lib.check(self.lib.tlr_plan_rank_map(self.handle, _lib.RANK_MAP[mode]))
+        self.rank_mode = mode
 
     def set_profiling(self, on=True, kind=None):
         """Bracket every launch with CUDA events (per-kernel device time; results unchanged), or
@@ -294,7 +344,16 @@ class PlanBatch:
             _lib.check(p.lib.tlr_set_data(p.handle, ctypes.c_void_p(S_t.data_ptr()), ctypes.c_void_p(y_t.data_ptr())))
 
     def evaluate(self, thetas, rule, value):
-        """[(loglik | None, grad | None, status)] for up to `count` parameter vectors."""
+        """[(loglik | None, grad | None, status)] for up to `count` parameter vectors.  A rank above
+        the plans' capacity grows every plan (Plan.grow) and repeats the batch."""
+        while True:
+            try:
+                return self._evaluate(thetas, rule, value)
+            except _lib.TlrError as e:
+                if e.code != _lib.ERR_RANK_CAP or not all([p.grow() for p in self.plans]):
+                    raise
+
+    def _evaluate(self, thetas, rule, value):
         if rule not in RULES:
             raise ValueError(f"rule must be one of {sorted(RULES)}, got {rule!r}")
         th = np.ascontiguousarray(np.atleast_2d(np.asarray(thetas, dtype=np.float64)))
@@ -433,16 +492,18 @@ def tlr_loglik_grad(S, y, theta, bounds, rule, value, cap=64, device=0, precisio
     return ev.loglik, ev.grad, ev.info
 
 
-def tlr_loglik(S, y, theta, bounds, rule, value, cap=64, device=0):
+def tlr_loglik(S, y, theta, bounds, rule, value, cap=64, device=0, precision="fp64"):
     """Drop-in for codes/17_tlr_cholesky_pilot.py:259 tlr_loglik.
 
     Returns (loglik, factor, info) or (None, None, info) when a diagonal tile is not positive
     definite (info['completed'] False, info['failed_at'] = k), like 17:172-176.  `factor` is a
-    lazy TLRFactor on the device."""
+    lazy TLRFactor on the device.  precision 'fp64' is the reference's arithmetic (the default);
+    'mixed' is the mixed-precision path."""
     S = np.asarray(S, dtype=np.float64)
     n = S.shape[0]
     b = _tile_size(bounds, n)
     plan = get_plan(n, b, cap, device)
+    plan.set_precision(precision)
     ev = plan.evaluate(theta, rule, value, host_S=S, host_y=np.asarray(y, dtype=np.float64))
     if ev.status != 0:
         return None, None, ev.info
@@ -560,6 +621,7 @@ def loglik(theta, locs, y, b, rule, tau=None, eps=None, ordered=False, cap=64, d
         locs, y = locs[perm], y[perm]
     n = locs.shape[0]
     plan = get_plan(n, b, cap, device)
+    plan.set_precision("fp64")
     ev = plan.evaluate(theta, rule, value, host_S=locs, host_y=y)
     return ev.loglik, ev.factor_ranks.copy(), ev.status == 0
 

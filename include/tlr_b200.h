@@ -66,10 +66,13 @@ int tlr_morton_order(const double* xy_dev, int n, int order, long long* perm_dev
 /* Allocation-free form of tlr_morton_order for callers that may not allocate device memory
  * during the call (a framework's caching allocator owns the device memory, a service loop that
  * must not allocate after start-up, ...).  No counterpart in the reference.  Same inputs,
- * outputs and result as tlr_morton_order; the working memory is a 16 MiB array inside the
+ * outputs and result as tlr_morton_order; the working memory is an 8.5 MiB array inside the
  * library's device image (held by every GPU that loads the library until the process exits),
- * so n <= 1,048,576 and order <= 10, otherwise TLR_ERR_ARG.  The first call on a device looks
- * up the array's address (make that first call before any stream capture).  The work is queued
+ * so n <= 1,048,576 and order <= 10, otherwise TLR_ERR_ARG.  Every call looks up the array's
+ * device address (cheap, no allocation).  With CUDA's lazy module loading (the default), the
+ * array itself comes into existence at the first call on each device, which does take device
+ * memory once: make that first call at start-up, before any stream capture and before another
+ * framework's caching allocator has taken the device's memory.  The work is queued
  * on `stream` and the call returns without waiting.  All calls share the one array: calls
  * whose work can overlap on the GPU (different streams, or different host threads) race, so
  * serialise them, for example on one stream. */
@@ -144,6 +147,19 @@ int tlr_get_offdiag_tile(tlr_plan* plan, int i, int j, double* u_host, double* v
 #define TLR_PRECISION_FP64 0
 #define TLR_PRECISION_MIXED 1
 int tlr_plan_set_precision(tlr_plan* plan, int mode);
+
+/* Rank map of later evaluations on the plan.  TLR_RANKS_RULE: the rule picks every rank (the
+ * reference's behaviour).  TLR_RANKS_RECORD: the rule picks, and every rank it picks (each
+ * initial compression, codes/17_tlr_cholesky_pilot.py:163, and each recompression, 17:203) is
+ * recorded in the plan.  TLR_RANKS_REPLAY: the recorded ranks replace the rule's choices (frozen
+ * ranks: the TLR log-likelihood as a smooth function of theta, for central differences and the
+ * ranks-frozen gradient).  Replay needs a recorded evaluation of the same rule on the same data.
+ * No counterpart in the reference, whose finite-difference Hessian
+ * (codes/15_pilot_standard_errors.py:21-31) lets the rule re-pick the ranks at every point. */
+#define TLR_RANKS_RULE 0
+#define TLR_RANKS_RECORD 1
+#define TLR_RANKS_REPLAY 2
+int tlr_plan_rank_map(tlr_plan* plan, int mode);
 
 /* Kernel kinds counted by tlr_plan_kernel_stats (launches issued by the plan's evaluations). */
 #define TLR_K_FILL 0

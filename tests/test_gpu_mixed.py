@@ -1,5 +1,5 @@
-"""The mixed-precision path (Gram-form recompression on the FP64 tensor cores, two-pass sketches,
-3xTF32 backward GEMMs) against the FP64 parity path and the dense FP64 likelihood.
+"""The mixed-precision path (three-pass sketches bounded by the exact FP64 residual, split-TF32
+tensor-core GEMMs in the backward pass) against the FP64 parity path and the dense FP64 likelihood.
 
 Budget (the accuracy contract of the mixed path): |loglik_mixed - loglik_fp64| <= 1e-2 nats and a
 gradient within 1e-3 (relative, 2-norm) of the FP64 path's on the same inputs and rule; PD
@@ -53,7 +53,7 @@ def test_mixed_within_budget_of_fp64(tlr, case, b, theta, rule, value):
         return
     assert abs(emx.loglik - e64.loglik) <= 1e-2
     assert np.linalg.norm(emx.grad - e64.grad) <= 1e-3 * np.linalg.norm(e64.grad), (emx.grad, e64.grad)
-    # the initial compression ranks are the FP64 ones up to ties (two-pass sketch, exact residual)
+    # the initial compression ranks are the FP64 ones up to ties (three-pass sketch, exact residual)
     assert np.mean(emx.sigma_ranks != e64.sigma_ranks) <= 0.02
     # bit-identical on a repeat (fixed reduction orders everywhere)
     assert emx2.loglik == emx.loglik and np.array_equal(emx2.grad, emx.grad)

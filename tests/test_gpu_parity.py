@@ -37,6 +37,21 @@ def test_morton_large_random(tlr):
     np.testing.assert_array_equal(tlr.morton_order(xy), O.morton_order(xy))
 
 
+@pytest.mark.parametrize("order", [3, 10, 12])
+def test_morton_most_sites_in_one_cell(tlr, order):
+    """Raw coordinates far outside the unit square (longitude / latitude, say) and NaNs all clip
+    into one or two cells; the sort's work does not depend on how many sites share a key, and
+    ties keep input order."""
+    rng = np.random.default_rng(5)
+    xy = rng.random((20000, 2))
+    xy[: 16000] = rng.uniform(-120.0, 45.0, (16000, 2))
+    xy[16000:16500] = np.nan
+    xy[17000:17100] = xy[17100]
+    with np.errstate(invalid="ignore"):
+        want = O.morton_order(xy, order)
+    np.testing.assert_array_equal(tlr.morton_order(xy, order=order), want)
+
+
 @pytest.mark.parametrize("case", [c["name"] for c in gold_cases()])
 def test_loglik_matches_reference(tlr, case):
     gold = {c["name"]: c for c in gold_cases()}[case]
@@ -178,3 +193,20 @@ def test_matern52_dense_helpers_match_oracle(tlr):
     finally:
         tlr.set_kernel(1.5)
         O.set_kernel(1.5)
+
+
+def test_rank_above_capacity_grows_the_plan(tlr):
+    """A tile rank above the plan's capacity does not end the call (the reference has no cap):
+    the shim recreates the workspace with twice the capacity and repeats the evaluation."""
+    d = np.load(os.path.join(GOLD, "n1030_b100_data.npz"))
+    S, y = d["S"], d["y"]
+    bounds = O.tile_bounds(1030, 100)
+    plan = tlr.Plan(1030, 100, cap=4, device=0)
+    try:
+        ev = plan.evaluate((1.0, 0.3, 0.05), "fixed", 1e-6, host_S=S, host_y=y)
+        assert plan.cap >= ev.info["max_rank_factor"] and plan.cap > 4
+    finally:
+        plan.close()
+    ll_o, _, info_o = O.tlr_loglik(S, y, (1.0, 0.3, 0.05), bounds, "fixed", 1e-6)
+    assert ev.info["stored_factor"] == info_o["stored_factor"]
+    assert abs(ev.loglik - ll_o) <= REL_TOL * abs(ll_o)
