@@ -24,6 +24,16 @@ KERNEL_KINDS = ["fill", "gen_offdiag", "sketch", "orth", "project", "resid", "fi
                 "trsm", "recompress", "finish", "bwd_gemm", "tri_inv", "bwd_copy", "alpha", "dtrace", "grad_finish"]
 
 
+class TlrTileStats(ctypes.Structure):
+    _fields_ = [
+        ("stored", ctypes.c_longlong),
+        ("max_rel", ctypes.c_double),
+        ("max_abs", ctypes.c_double),
+        ("fro_err", ctypes.c_double),
+        ("max_rank", ctypes.c_int),
+    ]
+
+
 class TlrInfo(ctypes.Structure):
     _fields_ = [
         ("completed", ctypes.c_int),
@@ -70,6 +80,9 @@ SIGNATURES = {
                                             ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "tlr_plan_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tlr_plan_rank_map": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tlr_truncate_tiles": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                                          ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong,
+                                          ctypes.POINTER(TlrTileStats), ctypes.POINTER(ctypes.c_int)]),
     "tlr_plan_set_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "tlr_plan_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tlr_plan_kernel_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),

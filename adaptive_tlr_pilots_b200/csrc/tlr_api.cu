@@ -89,6 +89,8 @@ struct tlr_plan {
   // pairs from rlog_off[k]
   int* rlog = nullptr;
   int rmode = 0;
+  // per initial tile: truncation error ||T - T_r||_F and ||T||_F (the assembled rule's outputs)
+  double *tail0 = nullptr, *fro0 = nullptr;
   std::vector<size_t> rlog_off;
   // launch accounting and optional per-kernel event timing
   bool prof = false;
@@ -217,7 +219,7 @@ int run_compression(tlr_plan* p, double sigma2, double inv_range, int rule_fixed
       }
       LAUNCH(TLR_K_FINALIZE, tlr::launch_finalize(p->n, p->b, k, ldp, p->cap, kMargin, rule_fixed, thr_rel, thr_abs, base, p->ti,
                                 p->tj, p->need, Pp, p->C, p->parts, p->fparts, fused ? 1 : p->nblk, p->gscr, p->gsv, p->U,
-                                p->V, p->rank, lev == kLevels - 1 ? 1 : 0, nc, p->rlog, p->rmode, p->status, s));
+                                p->V, p->rank, lev == kLevels - 1 ? 1 : 0, nc, p->rlog, p->rmode, p->tail0, p->fro0, p->status, s));
     }
   }
   return 0;
@@ -662,6 +664,8 @@ int tlr_plan_create(tlr_plan** plan, int n, int b, int cap, int device, void* st
   }
   p->rlog_off[p->nB] = rl;
   A(dalloc(p, &p->rlog, rl));
+  A(dalloc(p, &p->tail0, nt));
+  A(dalloc(p, &p->fro0, nt));
   if (rc == 0) {
     rc = cuda_check(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking), "side stream");
     if (!rc) rc = cuda_check(cudaEventCreateWithFlags(&p->ev_panel, cudaEventDisableTiming), "event");
@@ -936,6 +940,68 @@ int tlr_loglik_grad_batch(tlr_plan* const* plans, int count, const double* theta
   }
   if (status)
     for (int q = 0; q < count; ++q) status[q] = st[q];
+  return 0;
+}
+
+int tlr_truncate_tiles(tlr_plan* p, const double theta[3], int rule, double value, double* K_dev, long long ldk,
+                       tlr_tile_stats* stats, int* ranks) {
+  if (!p || !theta) return fail(TLR_ERR_ARG, "invalid arguments to tlr_truncate_tiles");
+  if (!p->has_data) return fail(TLR_ERR_NOT_READY, "tlr_set_data has not been called");
+  if (rule != TLR_RULE_FIXED && rule != TLR_RULE_ADAPTIVE) return fail(TLR_ERR_ARG, "rule must be fixed or adaptive");
+  const double sigma2 = theta[0], range = theta[1], eta = theta[2];
+  if (!(range > 0.0) || !std::isfinite(sigma2) || !std::isfinite(eta) || !std::isfinite(range))
+    return fail(TLR_ERR_ARG, "theta must be finite with range > 0");
+  if (K_dev && ldk < p->n) return fail(TLR_ERR_ARG, "ldk must be at least N");
+  if (K_dev && (long long)p->nB * (p->nB + 1) / 2 > 65535)
+    return fail(TLR_ERR_ARG, "the dense write-out takes at most 361 tiles per side");
+  TRY(cuda_check(cudaSetDevice(p->device), "cudaSetDevice"));
+  cudaStream_t s = p->stream;
+  p->factor_ok = false;
+  // thresholds: codes/11_tlr_rank_rules.py:81-98 (emax = tau * b * m_theta / N, b the largest tile)
+  const int rule_fixed = rule == TLR_RULE_FIXED;
+  const double thr_rel = rule_fixed ? value : 0.0;
+  const double thr_abs = rule_fixed ? 0.0 : value * (double)std::min(p->b, p->n) * sigma2 * eta / (double)p->n;
+  TRY(cuda_check(cudaMemsetAsync(p->status, 0, sizeof(int) * (4 + 4 * TLR_NKINDS), s), "reset status"));
+  TRY(cuda_check(cudaMemsetAsync(p->rank, 0, sizeof(int) * std::max(p->ntiles, 1), s), "reset ranks"));
+  TRY(run_compression(p, sigma2, 1.0 / range, rule_fixed, thr_rel, thr_abs));
+  if (K_dev)
+    LAUNCH(TLR_K_GEN, tlr::launch_assemble(p->xy, p->n, p->b, sigma2, 1.0 / range, p->nu5, sigma2 * eta, p->U, p->V,
+                                           p->rank, p->cap, K_dev, ldk, p->status, s));
+  const size_t nt = (size_t)std::max(p->ntiles, 1);
+  std::vector<double> tail(nt, 0.0), fro(nt, 0.0);
+  TRY(cuda_check(cudaMemcpyAsync(&p->hb->status, p->status, sizeof(int), cudaMemcpyDeviceToHost, s), "status"));
+  if (p->ntiles > 0) {
+    TRY(cuda_check(cudaMemcpyAsync(p->h_rank0, p->rank, sizeof(int) * p->ntiles, cudaMemcpyDeviceToHost, s), "ranks"));
+    TRY(cuda_check(cudaMemcpyAsync(tail.data(), p->tail0, sizeof(double) * p->ntiles, cudaMemcpyDeviceToHost, s),
+                   "tails"));
+    TRY(cuda_check(cudaMemcpyAsync(fro.data(), p->fro0, sizeof(double) * p->ntiles, cudaMemcpyDeviceToHost, s),
+                   "norms"));
+  }
+  TRY(cuda_check(cudaStreamSynchronize(s), "truncate tiles"));
+  const int status = p->hb->status;
+  if (status < 0)
+    return fail(status, status == TLR_ERR_RANK_CAP   ? "a tile rank exceeded the plan's rank capacity"
+                        : status == TLR_ERR_COMPRESS ? "a tile needed more than 120 singular directions"
+                                                     : "device error");
+  // statistics as codes/11_tlr_rank_rules.py:83, 99-108
+  const int nB = p->nB, b = p->b, n = p->n;
+  auto bsz = [&](int i) { return std::min(b, n - i * b); };
+  tlr_tile_stats st{};
+  for (int i = 0; i < nB; ++i) st.stored += (long long)bsz(i) * bsz(i);
+  double fro2 = 0.0;
+  for (int i = 0; i < nB; ++i)
+    for (int j = 0; j < i; ++j) {
+      const int t = i * (i - 1) / 2 + j;
+      const int r = p->h_rank0[t];
+      st.stored += 2LL * r * std::max(bsz(i), bsz(j));
+      st.max_rank = std::max(st.max_rank, r);
+      fro2 += 2.0 * tail[t] * tail[t];
+      st.max_abs = std::max(st.max_abs, tail[t]);
+      st.max_rel = std::max(st.max_rel, tail[t] / std::max(fro[t], 1e-300));
+      if (ranks) ranks[t] = r;
+    }
+  st.fro_err = std::sqrt(fro2);
+  if (stats) *stats = st;
   return 0;
 }
 

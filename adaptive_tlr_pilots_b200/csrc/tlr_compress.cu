@@ -640,7 +640,8 @@ __global__ void __launch_bounds__(1024) k_finalize(int n, int b, int k, int ldp,
                                                  double* TLR_RESTRICT Uo,
                                                  double* TLR_RESTRICT Vo, int* TLR_RESTRICT rank,
                                                  int last_level, int w_in_smem, int* TLR_RESTRICT rlog,
-                                                 int rmode, int* TLR_RESTRICT status) {
+                                                 int rmode, double* TLR_RESTRICT tail0, double* TLR_RESTRICT fro0,
+                                                 int* TLR_RESTRICT status) {
   if (*status != 0) return;
   const int c = blockIdx.x;
   if (!need[c]) return;
@@ -683,6 +684,12 @@ __global__ void __launch_bounds__(1024) k_finalize(int n, int b, int k, int ldp,
     else if (last_level) out = -2;  // compression limit reached
     else out = -1;                  // redo with a larger k
     if (out >= 0 && out > cap) out = -3;
+    if (out >= 0) {  // truncation error ||T - T_r||_F and ||T||_F of the accepted tile
+      double acc = rho2;
+      for (int q = out; q < k; ++q) acc += sorted[q] * sorted[q];
+      tail0[t] = sqrt(acc);
+      fro0[t] = sqrt(fro2);
+    }
     *rsel = out;
   }
   __syncthreads();
@@ -803,14 +810,14 @@ int launch_finalize(int n, int b, int k, int ldp, int cap, int margin, int rule_
                     double thr_abs, int tile_base, const int* ti, const int* tj, int* need, const double* P,
                     const double* C, const double* parts, const double* fparts, int nblk, double* gscratch,
                     double* gsv, double* U, double* V, int* rank, int last_level, int nchunk, int* rlog,
-                    int rmode, int* status, cudaStream_t s) {
+                    int rmode, double* tail0, double* fro0, int* status, cudaStream_t s) {
   size_t sm = (40 + 136 * 3 + 8 + (k <= 64 ? 2 * (size_t)k * k : 0)) * 8;
   const int w_in_smem = k <= 64 && (size_t)b * k * 8 <= 160 * 1024;
   if (w_in_smem) sm += (size_t)b * k * 8;
   cudaFuncSetAttribute(k_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   k_finalize<<<nchunk, k >= 32 ? 1024 : 256, sm, s>>>(n, b, k, ldp, cap, margin, rule_fixed, thr_rel, thr_abs, tile_base, ti, tj, need,
                                      P, C, parts, fparts, nblk, gscratch, gsv, U, V, rank, last_level, w_in_smem,
-                                     rlog, rmode, status);
+                                     rlog, rmode, tail0, fro0, status);
   return (int)cudaGetLastError();
 }
 

@@ -6,7 +6,8 @@ Mirrors the functions the pilot scripts call (marysalvana/adaptive-tlr-pilots):
   morton_order(xy, order=10)                codes/11_tlr_rank_rules.py:40-53   (on the GPU)
   tlr_loglik(S, y, theta, bounds, rule, v)  codes/17_tlr_cholesky_pilot.py:259-266
   neg_loglik_tlr(logth, S, y, bounds, ...)  codes/17_tlr_cholesky_pilot.py:279-290
-  Likelihood(S, y, b, device)(theta, ...)   codes/19_tlr_mcmc_gpu.py:27-138 (call surface)
+  make_cov, neg_loglik (assembled rule)     codes/11_tlr_rank_rules.py:74-138
+  Likelihood(S, y, b, device, svd_mode)     codes/19_tlr_mcmc_gpu.py:27-138 (assembled Sigma^TLR)
   loglik(theta, locs, y, b, rule, tau|eps)  the (loglik, per-tile ranks, PD) form
 
 Every evaluation runs on the GPU through libtlr_b200.so (include/tlr_b200.h).  There is no CPU
@@ -238,6 +239,36 @@ class Plan:
             raise ValueError(f"precision must be one of {sorted(_lib.PRECISIONS)}")
         _lib.check(self.lib.tlr_plan_set_precision(self.handle, _lib.PRECISIONS[mode]))
         self.precision = mode
+
+    def truncate_tiles(self, theta, rule, value, assemble=False):
+        """The assembled-matrix rule on the loaded sites (codes/11_tlr_rank_rules.py:74-108):
+        (stats, ranks, K) with stats = dict(stored, max_rel, max_abs, fro_err, max_rank), the
+        initial ranks in the order (i, j < i), and K the dense Sigma^TLR as a device tensor
+        (assemble=True) or None.  Leaves no factor in the plan.  A rank above the capacity grows
+        the plan, as evaluate does."""
+        torch = _torch()
+        if rule not in RULES:
+            raise ValueError(f"rule must be one of {sorted(RULES)}, got {rule!r}")
+        while True:
+            self._apply_kernel()
+            K = torch.empty((self.n, self.n), dtype=torch.float64, device=self.dev) if assemble else None
+            th = (ctypes.c_double * 3)(*[float(v) for v in theta])
+            st = _lib.TlrTileStats()
+            rk = np.zeros(max(self.ntiles, 1), dtype=np.int32)
+            try:
+                _lib.check(self.lib.tlr_truncate_tiles(self.handle, th, RULES[rule], float(value),
+                                                       ctypes.c_void_p(K.data_ptr() if K is not None else 0),
+                                                       self.n, ctypes.byref(st),
+                                                       rk.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+                break
+            except _lib.TlrError as e:
+                del K
+                if e.code != _lib.ERR_RANK_CAP or not self.grow():
+                    raise
+        self.generation += 1
+        stats = dict(stored=int(st.stored), max_rel=float(st.max_rel), max_abs=float(st.max_abs),
+                     fro_err=float(st.fro_err), max_rank=int(st.max_rank))
+        return stats, rk[: self.ntiles], K
 
     def rank_map(self, mode):
         """'rule' (the rule picks every rank), 'record' (and they are recorded) or 'replay' (the
@@ -626,24 +657,115 @@ def loglik(theta, locs, y, b, rule, tau=None, eps=None, ordered=False, cap=64, d
     return ev.loglik, ev.factor_ranks.copy(), ev.status == 0
 
 
-class Likelihood:
-    """Call surface of codes/19_tlr_mcmc_gpu.py:27-138: Likelihood(S, y, b, device)(theta, rule,
-    value) -> log-likelihood, or -inf when the factorization fails; self.last records
-    ok / stored values / time.  Here the likelihood is the TLR Cholesky one (never assembled)."""
+def _dense_cov(S, theta, device=0):
+    """Dense Sigma(theta) = sigma2 M + sigma2 eta I on the device (codes/11_tlr_rank_rules.py:61-65),
+    with the kernel chosen by set_kernel."""
+    torch = _torch()
+    dev = torch.device("cuda", device)
+    St = torch.as_tensor(np.asarray(S, dtype=np.float64), device=dev)
+    sigma2, rng, eta = [float(v) for v in theta]
+    with torch.no_grad():
+        K = torch.cdist(St, St)
+        if _NU == 2.5:
+            K.mul_((5.0 ** 0.5) / rng)
+            E = torch.exp(-K)
+            K.mul_(K.div(3.0).add_(1.0)).add_(1.0).mul_(E).mul_(sigma2)
+        else:
+            K.mul_((3.0 ** 0.5) / rng)
+            E = torch.exp(-K)
+            K.add_(1.0).mul_(E).mul_(sigma2)
+        del E
+        K.diagonal().add_(sigma2 * eta)
+    return K
 
-    def __init__(self, S, y, b, device=0, cap=64):
+
+def make_cov(S, theta, rule, value, bounds, device=0, cap=64):
+    """(K, info): Sigma(theta) on the device, with every off-diagonal tile truncated under the rule
+    for rule 'fixed' / 'adaptive' (info = (stored, max_rel, max_abs, ||Sigma - Sigma^TLR||_F,
+    ranks), the return of truncate_tiles), or exact for rule 'dense' (info None).  Drop-in for
+    codes/11_tlr_rank_rules.py:121-126 make_cov with truncate_tiles (11:74-108) inside; S must be
+    Morton-ordered and bounds = tile_bounds(N, b)."""
+    S = np.asarray(S, dtype=np.float64)
+    if rule == "dense":
+        return _dense_cov(S, theta, device), None
+    n = S.shape[0]
+    b = _tile_size(bounds, n)
+    plan = get_plan(n, b, cap, device)
+    plan.set_data(S, np.zeros(n))
+    st, ranks, K = plan.truncate_tiles(theta, rule, value, assemble=True)
+    return K, (st["stored"], st["max_rel"], st["max_abs"], st["fro_err"], [int(r) for r in ranks])
+
+
+def loglik_dense_K(K, y):
+    """(loglik, L) of y under the dense device matrix K, or (None, None) when K is not positive
+    definite: codes/11_tlr_rank_rules.py:112-120 loglik_dense, the Cholesky on the device."""
+    torch = _torch()
+    with torch.no_grad():
+        yt = torch.as_tensor(np.asarray(y, dtype=np.float64), device=K.device)
+        L, info = torch.linalg.cholesky_ex(K)
+        if int(info.item()) != 0:
+            return None, None
+        z = torch.linalg.solve_triangular(L, yt[:, None], upper=False)[:, 0]
+        ld = 2.0 * torch.log(torch.diagonal(L)).sum()
+        return float(-0.5 * (z @ z + ld + len(yt) * np.log(2 * np.pi))), L
+
+
+def neg_loglik(logth, S, y, rule, value, bounds, trace, device=0):
+    """Negative log-likelihood of the assembled-matrix rule at exp(logth), 1e12 when Sigma^TLR is
+    not positive definite: codes/11_tlr_rank_rules.py:130-138 (trace counts evals and failures)."""
+    theta = np.exp(np.asarray(logth, dtype=np.float64))
+    K, _ = make_cov(S, theta, rule, value, bounds, device=device)
+    ll, _ = loglik_dense_K(K, y)
+    del K
+    trace["evals"] += 1
+    if ll is None:
+        trace["failures"] += 1
+        return 1e12
+    return -ll
+
+
+class Likelihood:
+    """codes/19_tlr_mcmc_gpu.py:27-138: Likelihood(S, y, b, device, svd_mode=...)(theta, rule, value)
+    is the log-likelihood of y under Sigma^TLR(theta), the covariance with every off-diagonal tile
+    truncated under the rule (assembled densely on the device), through a dense Cholesky; -inf
+    when that Cholesky fails; self.last = dict(ok, stored, time, L).  rule 'dense' skips the
+    truncation.
+
+    svd_mode: the reference offers 'fp64' (exact batched SVD, the minimal rank meeting the rule),
+    'fp32' and 'rand' (ranks whose FP64-verified error meets the rule, possibly above the minimal
+    one).  Here every mode uses the device compression (randomized sketch, exact FP64 residual,
+    widened until the rank is resolved), which gives the minimal ranks of 'fp64'; so the ranks are
+    those of 'fp64' in all three modes and never above the reference's 'fp32' / 'rand' ones.
+    rand_k, rand_power and seed are accepted for the call surface; last_fallback is always 0."""
+
+    MODES = ("fp64", "fp32", "rand")
+
+    def __init__(self, S, y, b, device=0, dtype=None, svd_mode="fp32", rand_k=64, rand_power=2, seed=0, cap=64):
+        if svd_mode not in self.MODES:
+            raise ValueError(f"svd_mode must be one of {self.MODES}")
+        self.svd_mode, self.rand_k, self.rand_power, self.last_fallback = svd_mode, rand_k, rand_power, 0
         self.n = int(np.asarray(S).shape[0])
         self.b = int(b)
         dev = device.index if hasattr(device, "index") and device.index is not None else (
             0 if not isinstance(device, int) else device)
+        self.device = dev
+        self.S = np.asarray(S, dtype=np.float64)
+        self.y = np.asarray(y, dtype=np.float64)
         self.plan = Plan(self.n, self.b, cap, dev)
-        self.plan.set_data(S, y)
+        self.plan.set_data(self.S, self.y)
         self.last = {}
 
     def __call__(self, theta, rule, value):
+        torch = _torch()
         t0 = time.time()
-        ev = self.plan.evaluate(theta, rule, value)
-        ok = ev.status == 0
-        self.last = dict(ok=ok, stored=ev.info.get("stored_factor", ev.info["stored_sigma"]), time=time.time() - t0,
-                         info=ev.info)
-        return ev.loglik if ok else -float("inf")
+        if rule == "dense":
+            K, stored = _dense_cov(self.S, theta, self.device), self.n * self.n
+        else:
+            st, _, K = self.plan.truncate_tiles(theta, rule, value, assemble=True)
+            stored = st["stored"]
+        ll, L = loglik_dense_K(K, self.y)
+        del K
+        torch.cuda.synchronize(self.device)
+        ok = ll is not None
+        self.last = dict(ok=ok, stored=stored, time=time.time() - t0, L=L)
+        return ll if ok else -float("inf")

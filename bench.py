@@ -41,7 +41,9 @@ def parse():
     ap.add_argument("--tau", type=float, default=0.9)
     ap.add_argument("--cpu-sample", type=int, default=1, help="0: skip the CPU baseline leg")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
-    ap.add_argument("--plain-steps", type=int, default=2, help="timed steps of the plain FP64 comparison (0: skip)")
+    ap.add_argument("--plain-steps", type=int, default=-1,
+                    help="timed evaluations of the plain FP64 comparison (-1: as many as the batched leg, steps x "
+                         "batch; 0: skip)")
     ap.add_argument("--batch", type=int, default=4, help="parameter vectors per step (one batched call)")
     ap.add_argument("--dense", type=int, default=1, help="0: skip the dense FP64 oracle")
     ap.add_argument("--sim", choices=["dense", "tlr"], default="dense",
@@ -53,6 +55,8 @@ def parse():
 # dram__bytes_read.sum + dram__bytes_write.sum over the 98 launches of one evaluation, from an ncu
 # capture of `bench.py --steps 1 --warmup 1 --cpu-sample 0 --plain-steps 0 --batch 1 --dense 0`
 RC_TRAFFIC_N50K = 283.5e6
+RC_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, mean over the 98 k_recompress launches of "
+                     "one evaluation (batch 1, same workload, 1-pass capture)")
 METRIC = "TLR loglik+grad evals/s at N=50k vs plain FP64 on B200; |dl| vs FP64 dense"
 
 
@@ -135,6 +139,13 @@ def cpu_baseline(S, y, a):
 
 
 def run_reference(a):
+    """The reference arm: the reference's algorithm on the host's cores (the oracle, a NumPy/SciPy
+    restatement of codes/17_tlr_cholesky_pilot.py with the same LAPACK calls; the reference itself
+    is not present where this runs), every BLAS thread the host has.  The K timed steps are K
+    consecutive slices of ONE complete evaluation at the workload's size (oracle/cpu_sample.py:
+    timed_full_evaluation), so ms_per_step x K is the measured time of one log-likelihood;
+    loglik+grad = 7 evaluations (the value and central differences in 3 parameters, the
+    reference's only derivative method).  Warm-up: W complete evaluations at N = 4,000, b = 250."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -142,26 +153,23 @@ def run_reference(a):
 
     from adaptive_tlr_pilots_b200 import synth
     from oracle import tlr_oracle as O
-    from oracle.cpu_sample import SampledPipeline, blas_threads
+    from oracle.cpu_sample import blas_threads, timed_full_evaluation
     S, y, _, _ = synth.simulate_field(a.n, THETA, order_fn=O.morton_order)
-    sp = SampledPipeline(S, y, THETA, a.b, "adaptive", a.tau, n_pairs=48)
-    for w in range(a.warmup):
-        sp.step(n_compress=4, n_trsm=4, n_recompress=8, seed=100 + w)
-    ests, walls = [], []
-    for s in range(a.steps):
-        est, wall = sp.step(n_compress=6, n_trsm=8, n_recompress=24, seed=s)
-        ests.append(est)
-        walls.append(wall)
-    est = sum(ests) / len(ests)
-    value = 1.0 / (7.0 * est)
-    sample = (f"oracle port of codes/17_tlr_cholesky_pilot.py per-tile operations at N={a.n}, b={a.b}: per step 6 "
-              f"compressions, 1 POTRF, 8 panel solves/diag updates, 24 step-0 recompressions, scaled by their counts "
-              f"in one evaluation ({est:.1f} s per log-likelihood estimated); loglik+grad = 7 evaluations (value "
-              f"and central differences in 3 parameters)")
+    if a.warmup:
+        Sw, yw, _, _ = O.simulate_field(4000, THETA)
+        for _ in range(a.warmup):
+            timed_full_evaluation(Sw, yw, THETA, 250, "adaptive", a.tau, 1)
+    r = timed_full_evaluation(S, y, THETA, a.b, "adaptive", a.tau, a.steps)
+    k = len(r["step_seconds"])
+    value = 1.0 / (7.0 * r["seconds"])
+    sample = (f"one complete evaluation of the oracle's tlr_loglik (the reference's algorithm, NumPy/SciPy) at "
+              f"N={a.n}, b={a.b}, adaptive tau={a.tau}: {r['seconds']:.1f} s measured, timed as {k} consecutive "
+              f"slices of its {r['stages']} stages (compression rows, factorization steps, solve); loglik+grad = 7 "
+              f"evaluations (value and central differences in 3 parameters); loglik {r['loglik']}")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": a.gpus,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 7000.0 * est, "higher_is_better": True,
+            "steps": k, "warmup": a.warmup, "ms_per_step": 1e3 * r["seconds"] / k, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded reference protocol)",
-            "config": workload(a),
+            "config": workload(a), "step_seconds": r["step_seconds"], "seconds_per_loglik": r["seconds"],
             "cpu_baseline": {"value": value, "unit": "evals/s", "cores": blas_threads(), "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -170,7 +178,11 @@ def run_reference(a):
 
 def main():
     a = parse()
+    if a.plain_steps < 0:
+        a.plain_steps = a.steps * a.batch  # as many plain evaluations as batched ones
     if a.impl == "reference":
+        for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+            os.environ.setdefault(var, str(os.cpu_count() or 1))  # every host thread for the BLAS
         run_reference(a)
         return
     import numpy as np
@@ -230,22 +242,8 @@ def main():
     free_b, total_b = torch.cuda.mem_get_info(local)
     for _ in range(a.warmup):
         out = pb.evaluate(thetas, "adaptive", a.tau)
-    # one untimed step with every launch bracketed by events: the per-kernel table and the
-    # dominant kernel; the timed steps then bracket only that kernel's launches (its roofline)
     for p in pb.plans:
-        p.set_profiling(True)
         p.kernel_stats(reset=True)
-    out = pb.evaluate(thetas, "adaptive", a.tau)
-    torch.cuda.synchronize()
-    prof_stats = {}
-    for p in pb.plans:
-        for k, v in p.kernel_stats(reset=True).items():
-            acc = prof_stats.setdefault(k, dict(ms=0.0, launches=0, flops=0.0, bytes=0.0))
-            for f in acc:
-                acc[f] += v[f]
-    top = max(prof_stats, key=lambda k: prof_stats[k]["ms"])
-    for p in pb.plans:
-        p.set_profiling(True, kind=top)
     sampler = ClockSampler(local)
     sampler.start()
     barrier()
@@ -264,7 +262,18 @@ def main():
             acc = stats.setdefault(k, dict(ms=0.0, launches=0, flops=0.0, bytes=0.0))
             for f in acc:
                 acc[f] += v[f]
-        p.set_profiling(False)
+    # the roofline of the dominant kernel, from one evaluation of one plan alone (batch 1, every
+    # launch bracketed by two events on its stream), so that no other plan's work lies inside a
+    # kernel's event interval: the per-kernel table, the dominant kernel and its mean launch time
+    p0 = pb.plans[0]
+    p0.set_profiling(True)
+    torch.cuda.synchronize()
+    t_one = time.perf_counter()
+    p0.evaluate(THETA, "adaptive", a.tau, grad=True)
+    torch.cuda.synchronize()
+    t_one = time.perf_counter() - t_one
+    prof_stats = p0.kernel_stats(reset=True)
+    p0.set_profiling(False)
     ll0, g0, st0 = out[0]
     info0 = pb.plans[0].evaluate(THETA, "adaptive", a.tau).info  # storage of the factor at theta_0
 
@@ -288,23 +297,29 @@ def main():
     if rank == 0:
         pk, pk_kind = peaks()
         launches = int(sum(v["launches"] for v in stats.values()))
-        st = stats[top]
+        top = max(prof_stats, key=lambda k: prof_stats[k]["ms"])
+        st = prof_stats[top]
         per_launch_ms = st["ms"] / max(st["launches"], 1)
         achieved_gbs = st["bytes"] / max(st["launches"], 1) / (per_launch_ms * 1e-3) / 1e9
         roof = {"kernel": top, "bound": "hbm", "achieved": achieved_gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved_gbs / pk["hbm_gbs"], "peak_kind": pk_kind,
                 # DRAM bytes per launch from one ncu capture of this kernel on this workload
                 "traffic": (RC_TRAFFIC_N50K if top == "recompress" and (a.n, a.b, a.tau) == (50000, 500, 0.9)
-                            and a.precision == "mixed" else None),
-                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum, mean over the 98 "
-                                   "k_recompress launches of one evaluation (batch 1, same workload, 1-pass capture)"),
+                            else None),
+                "traffic_source": RC_TRAFFIC_SOURCE,
+                "algorithmic_bytes_per_launch": st["bytes"] / max(st["launches"], 1),
                 "fp64_tflops": st["flops"] / max(st["launches"], 1) / (per_launch_ms * 1e-3) / 1e12,
                 "fp64_peak_nominal_tflops": 37.0,
-                "share": prof_stats[top]["ms"] / sum(v["ms"] for v in prof_stats.values()),
-                "per_launch_ms": per_launch_ms, "launches_per_step": st["launches"] / a.steps}
-        # per-kernel table of the profiled step (event intervals of concurrent plans overlap)
-        kern = {k: {"ms_per_step": v["ms"], "launches_per_step": v["launches"],
-                    "gflop_per_step": v["flops"] / 1e9, "gb_per_step": v["bytes"] / 1e9}
+                "timing": "one evaluation of one plan alone (batch 1), every launch between two CUDA events on "
+                          "its stream; achieved = the kernel's own algorithmic bytes per launch / mean launch time",
+                "share": st["ms"] / sum(v["ms"] for v in prof_stats.values()),
+                "per_launch_ms": per_launch_ms, "launches_per_eval": st["launches"],
+                "kernel_ms_per_eval": st["ms"], "eval_wall_ms": 1e3 * t_one}
+        # per-kernel table of the profiled evaluation (one plan alone: kernels on its side stream,
+        # POTRF and the alpha solve, overlap those of the main stream, so the column does not add
+        # up to the evaluation's wall time)
+        kern = {k: {"ms_per_eval": v["ms"], "launches_per_eval": v["launches"],
+                    "gflop_per_eval": v["flops"] / 1e9, "gb_per_eval": v["bytes"] / 1e9}
                 for k, v in prof_stats.items() if v["launches"]}
         value = world * a.steps * B / (ms_max / 1e3)
         line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world,

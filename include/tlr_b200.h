@@ -53,6 +53,15 @@ typedef struct {
   double quad;              /* z^T z, z = L^{-1} y */
 } tlr_info;
 
+/* Outputs of the assembled-matrix rule, codes/11_tlr_rank_rules.py:74-108 truncate_tiles. */
+typedef struct {
+  long long stored;   /* dense diagonal tiles + 2 b_max r_ij per off-diagonal tile (11:83, 101) */
+  double max_rel;     /* max over tiles of ||T - T_r||_F / ||T||_F */
+  double max_abs;     /* max over tiles of ||T - T_r||_F */
+  double fro_err;     /* ||Sigma - Sigma^TLR||_F = sqrt(2 sum ||T - T_r||_F^2) */
+  int max_rank;
+} tlr_tile_stats;
+
 /* Create a plan for N sites in tiles of b (the last tile may be short, as
  * codes/11_tlr_rank_rules.py:69-71 tile_bounds), with room for `cap` columns per off-diagonal
  * factor.  stream may be NULL (the legacy default stream).  Allocates all device memory. */
@@ -115,6 +124,18 @@ int tlr_loglik_grad(tlr_plan* plan, const double theta[3], int rule, double valu
  * codes/19_tlr_mcmc_gpu.py:170-202). */
 int tlr_loglik_grad_batch(tlr_plan* const* plans, int count, const double* thetas, int rule, double value,
                           double* loglik, double* grad, int* status);
+
+/* The assembled-matrix rule: every off-diagonal tile of Sigma(theta) truncated under the rule
+ * (the plan's initial compression, the reference's ranks), with the reference's statistics in
+ * `stats` and the per-tile ranks in `ranks` (ntiles, order (i, j < i); may be NULL).  When K_dev
+ * is not NULL, Sigma^TLR is written there densely (N x N FP64 on the plan's device, leading
+ * dimension ldk >= N; symmetric, so either storage order): the diagonal tiles exact, every
+ * off-diagonal tile U V^T and its transpose.  Replaces truncate_tiles / make_cov,
+ * codes/11_tlr_rank_rules.py:74-108, 121-126 (whose input is the dense K; here the tiles are
+ * generated from the sites), and the truncation of codes/19_tlr_mcmc_gpu.py:51-123.  Leaves no
+ * factor in the plan.  Tiles per side (N / b) at most 361. */
+int tlr_truncate_tiles(tlr_plan* plan, const double theta[3], int rule, double value, double* K_dev,
+                       long long ldk, tlr_tile_stats* stats, int* ranks);
 
 /* The same evaluation with HOST sites and observations (Morton-ordered), copied to the device
  * inside the call: the end-to-end form of tlr_loglik for callers that hold numpy arrays. */

@@ -134,3 +134,27 @@ def blas_threads():
         return int(max(n)) if n else 1
     except Exception:
         return 1
+
+
+def timed_full_evaluation(S, y, theta, b, rule, value, steps):
+    """One complete evaluation of the reference pipeline (oracle.tlr_loglik: tile generation and
+    compression, the right-looking TLR Cholesky, the forward solve; codes/17_tlr_cholesky_pilot.py:
+    137-266), timed stage by stage.  The 2 nB + 1 stages (nB compression rows, nB factorization
+    steps, the solve) are dealt into `steps` consecutive groups of nearly equal count; a group's
+    time is the sum of its stages' times, so the groups add up to the measured evaluation.
+
+    Returns dict(seconds, step_seconds, loglik, completed, stages)."""
+    bounds = O.tile_bounds(S.shape[0], b)
+    marks = []
+    t0 = time.perf_counter()
+    ll, _, info = O.tlr_loglik(S, y, tuple(float(v) for v in theta), bounds, rule, value,
+                               on_stage=lambda lab: marks.append(time.perf_counter()))
+    t1 = time.perf_counter()
+    marks.append(t1)  # the solve (or the end of a failed factorization)
+    stage_s = np.diff(np.concatenate(([t0], marks)))
+    nst = len(stage_s)
+    steps = max(1, min(int(steps), nst))
+    group = (np.arange(nst) * steps) // nst
+    step_s = [float(stage_s[group == q].sum()) for q in range(steps)]
+    return dict(seconds=t1 - t0, step_seconds=step_s, loglik=ll, completed=bool(info.get("completed", False)),
+                stages=nst)

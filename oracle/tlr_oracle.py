@@ -174,7 +174,7 @@ def thresholds(n, b, theta, rule, value):
 
 
 # ------------------------------------------------------------------ TLR Cholesky
-def tlr_cholesky(S, theta, bounds, rule, value, rank_log=None, frozen=None):
+def tlr_cholesky(S, theta, bounds, rule, value, rank_log=None, frozen=None, on_stage=None):
     """Right-looking TLR Cholesky of Sigma(theta) without forming Sigma.
 
     Returns (L_diag, L_off, info) or (None, None, info) when a diagonal tile is not
@@ -184,6 +184,8 @@ def tlr_cholesky(S, theta, bounds, rule, value, rank_log=None, frozen=None):
 
     rank_log: optional dict, filled with {('init', i, j): r, ('rc', k, i, j): r}.
     frozen:   optional dict of the same form; its ranks replace the rule's choice.
+    on_stage: optional callable, called with ("compress", i) after tile row i is generated and
+              compressed and with ("factor", k) after factorization step k (for stage timings).
     """
     if rule not in ("fixed", "adaptive"):
         raise ValueError(f"rule must be 'fixed' or 'adaptive', got {rule!r}")
@@ -213,6 +215,8 @@ def tlr_cholesky(S, theta, bounds, rule, value, rank_log=None, frozen=None):
                 rank_log[("init", i, j)] = r
             A_off[(i, j)] = (U, V)
             stored0 += 2 * r * max(i1 - i0, j1 - j0)
+        if on_stage is not None:
+            on_stage(("compress", i))
     sigma_ranks = [u.shape[1] for u, _ in A_off.values()]
     info = dict(stored_sigma=int(stored0), max_rank_sigma=max(sigma_ranks) if sigma_ranks else 0,
                 sigma_ranks=sigma_ranks)
@@ -252,6 +256,8 @@ def tlr_cholesky(S, theta, bounds, rule, value, rank_log=None, frozen=None):
                     if rank_log is not None:
                         rank_log[("rc", k, i, j)] = r
                     A_off[(i, j)] = (Ur, Vr)
+        if on_stage is not None:
+            on_stage(("factor", k))
     # storage statistics: 17:206-209
     ranks = [u.shape[1] for u, _ in L_off.values()]
     stored = sum(d.shape[0] ** 2 for d in L_diag) + sum(2 * u.shape[1] * u.shape[0] for u, _ in L_off.values())
@@ -323,12 +329,13 @@ def skill(yp, mu, sig):
     return dict(rmse=float(np.sqrt(((yp - mu) ** 2).mean())), crps=crps, cover90=float((np.abs(z) <= 1.6448536).mean()))
 
 
-def tlr_loglik(S, y, theta, bounds, rule, value, rank_log=None, frozen=None):
+def tlr_loglik(S, y, theta, bounds, rule, value, rank_log=None, frozen=None, on_stage=None):
     """(loglik | None, (L_diag, L_off) | None, info).
 
     l = -1/2 (z^T z + 2 sum log diag L_kk + N log 2 pi), z = L^{-1} y.
     codes/17_tlr_cholesky_pilot.py:259-266."""
-    L_diag, L_off, info = tlr_cholesky(S, theta, bounds, rule, value, rank_log=rank_log, frozen=frozen)
+    L_diag, L_off, info = tlr_cholesky(S, theta, bounds, rule, value, rank_log=rank_log, frozen=frozen,
+                                       on_stage=on_stage)
     if L_diag is None:
         return None, None, info
     z = tlr_forward(L_diag, L_off, bounds, y[:, None])[:, 0]

@@ -140,3 +140,25 @@ def test_oracle_matern52_matches_reference(case):
         assert abs(ll_d - gold["dense_loglik"]) <= 1e-10 * abs(gold["dense_loglik"])
     finally:
         O.set_kernel(1.5)
+
+
+def test_oracle_assembled_rule_matches_reference():
+    """The oracle's truncate_tiles + loglik_dense against the reference's own outputs
+    (codes/11_tlr_rank_rules.py:74-126 run by tests/golden/make_golden_assembled.py)."""
+    g = json.load(open(os.path.join(GOLD, "golden_assembled.json")))
+    d = np.load(os.path.join(GOLD, g["data"]))
+    S, y = d["S"], d["y"]
+    theta = tuple(g["theta"])
+    bounds = O.tile_bounds(g["n"], g["b"])
+    for rec in g["rules"]:
+        K = O.cov_dense(S, theta)
+        stored, max_rel, max_abs, fro, ranks = O.truncate_tiles(K, bounds, rec["rule"], rec["value"],
+                                                                theta[0] * theta[2])
+        assert stored == rec["stored"] and ranks == rec["ranks"]
+        np.testing.assert_allclose([max_rel, max_abs, fro], [rec["max_rel"], rec["max_abs"], rec["fro_err"]],
+                                   rtol=1e-9)
+        ll = O.loglik_dense(K, y)[0]
+        if rec["loglik"] is None:
+            assert ll is None
+        else:
+            assert abs(ll - rec["loglik"]) <= 1e-10 * abs(rec["loglik"])
