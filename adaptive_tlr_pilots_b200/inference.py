@@ -35,9 +35,10 @@ class TLRObjective:
     __call__(x, grad) -> (ll, g) with g = d ll / d x = theta * d ll / d theta; ll = -inf and g =
     None when the factorization fails (a diagonal tile is not positive definite).
     batch(X, grad) evaluates many parameter vectors: with batch=B > 1 through B plans and the
-    batched entry point (tlr_loglik_grad_batch), B vectors per call."""
+    batched entry point (tlr_loglik_grad_batch), B vectors per call; `workspaces` < B runs them
+    through that many device workspaces in groups (PlanBatch), bounding the memory."""
 
-    def __init__(self, S, y, b, rule, value, precision="mixed", cap=64, device=0, batch=1):
+    def __init__(self, S, y, b, rule, value, precision="mixed", cap=64, device=0, batch=1, workspaces=None):
         from .tlr import Plan, PlanBatch
         S = np.asarray(S, dtype=np.float64)
         y = np.asarray(y, dtype=np.float64)
@@ -46,7 +47,7 @@ class TLRObjective:
         self.plan.set_precision(precision)
         self.pbatch = None
         if batch > 1:
-            self.pbatch = PlanBatch(S.shape[0], b, batch, cap, device, precision)
+            self.pbatch = PlanBatch(S.shape[0], b, batch, cap, device, precision, workspaces=workspaces)
             self.pbatch.set_data(S, y)
         self.rule, self.value = rule, value
         self.evals = 0

@@ -342,16 +342,24 @@ class Plan:
 
 
 class PlanBatch:
-    """`count` plans on one device, each with its own stream, sharing the sites and observations:
-    evaluate(thetas) runs one batched call (tlr_loglik_grad_batch) in which every plan's forward
-    pass is queued before any is waited on, so the GPU overlaps the plans' latency-bound
-    factorization steps.  The batch of MCMC chains or optimizer restarts of one iteration."""
+    """Batched evaluation of `count` parameter vectors on one device, sharing the sites and
+    observations: evaluate(thetas) runs batched calls (tlr_loglik_grad_batch) in which every
+    workspace's forward pass is queued before any is waited on, so the GPU overlaps the plans'
+    latency-bound factorization steps.  The batch of MCMC chains or optimizer restarts of one
+    iteration.
 
-    def __init__(self, n, b, count, cap=64, device=0, precision="mixed"):
+    `workspaces` (default: count, at most count) is the number of device workspaces (plans, one
+    stream each) that run at once; with fewer workspaces than parameter vectors the vectors go
+    through them in consecutive groups, so memory is workspaces x (one plan) whatever the count
+    (at N = 50,000, b = 500 a plan holds about 10 GB: 64 chains through 8 workspaces fit one
+    B200)."""
+
+    def __init__(self, n, b, count, cap=64, device=0, precision="mixed", workspaces=None):
         torch = _torch()
         self.n, self.b, self.count, self.device = int(n), int(b), int(count), int(device)
+        self.workspaces = self.count if workspaces is None else max(1, min(int(workspaces), self.count))
         self.lib = _lib.load()
-        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(self.count)]
+        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(self.workspaces)]
         self.plans = []
         for st in self.streams:
             with torch.cuda.stream(st):
@@ -375,22 +383,31 @@ class PlanBatch:
             _lib.check(p.lib.tlr_set_data(p.handle, ctypes.c_void_p(S_t.data_ptr()), ctypes.c_void_p(y_t.data_ptr())))
 
     def evaluate(self, thetas, rule, value):
-        """[(loglik | None, grad | None, status)] for up to `count` parameter vectors.  A rank above
-        the plans' capacity grows every plan (Plan.grow) and repeats the batch."""
-        while True:
-            try:
-                return self._evaluate(thetas, rule, value)
-            except _lib.TlrError as e:
-                if e.code != _lib.ERR_RANK_CAP or not all([p.grow() for p in self.plans]):
-                    raise
+        """[(loglik | None, grad | None, status)] for up to `count` parameter vectors, in groups of
+        `workspaces`.  A rank above the plans' capacity grows every plan (Plan.grow) and repeats
+        the group."""
+        th = np.atleast_2d(np.asarray(thetas, dtype=np.float64))
+        if th.shape[0] > self.count or th.shape[1] != 3:
+            raise ValueError(f"thetas must be at most {self.count} x 3")
+        out = []
+        for g0 in range(0, th.shape[0], self.workspaces):
+            grp = th[g0:g0 + self.workspaces]
+            while True:
+                try:
+                    out.extend(self._evaluate(grp, rule, value))
+                    break
+                except _lib.TlrError as e:
+                    if e.code != _lib.ERR_RANK_CAP or not all([p.grow() for p in self.plans]):
+                        raise
+        return out
 
     def _evaluate(self, thetas, rule, value):
         if rule not in RULES:
             raise ValueError(f"rule must be one of {sorted(RULES)}, got {rule!r}")
         th = np.ascontiguousarray(np.atleast_2d(np.asarray(thetas, dtype=np.float64)))
         m = th.shape[0]
-        if m > self.count or th.shape[1] != 3:
-            raise ValueError(f"thetas must be at most {self.count} x 3")
+        if m > self.workspaces or th.shape[1] != 3:
+            raise ValueError(f"at most {self.workspaces} parameter vectors per batched call")
         for p in self.plans[:m]:
             p._apply_kernel()
         handles = (ctypes.c_void_p * m)(*[p.handle.value for p in self.plans[:m]])

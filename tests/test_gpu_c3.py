@@ -11,9 +11,10 @@ inversion) is compared with
 
 The reference has no gradient (its only derivative is the finite-difference Hessian of
 codes/15_pilot_standard_errors.py:21-31); these are the checks the gradient is held to.  With the
-adaptive rule (tau = 0.9) the TLR gradient differs from both by the truncation: the bounds below
-are the measured spread with a margin.  With a tight rule (fixed eps = 1e-8) all three agree to
-1e-5."""
+adaptive rule (tau = 0.9) the TLR gradient differs from both by the truncation; measured on a B200:
+at most 1.03e-3 from the frozen-rank differences and 2.6e-4 from the dense gradient over the 16
+points (so within the 1e-3 relative gradient budget against dense FP64), and the bounds below are
+those with a margin.  With a tight rule (fixed eps = 1e-8) all three agree to 1.7e-5 (bound 1e-4)."""
 import json
 import os
 
@@ -24,9 +25,9 @@ pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 THETA0 = np.array([1.0, 0.3, 0.05])
 FD_REL = 1e-5
-TOL_FD_ADAPTIVE = 5e-2      # |g - fd| / |fd|, adaptive tau = 0.9
-TOL_DENSE_ADAPTIVE = 1e-1   # |g - g_dense| / |g_dense|, adaptive tau = 0.9
-TOL_TIGHT = 1e-5            # both, fixed eps = 1e-8
+TOL_FD_ADAPTIVE = 2e-3      # |g - fd| / |fd|, adaptive tau = 0.9
+TOL_DENSE_ADAPTIVE = 1e-3   # |g - g_dense| / |g_dense|, adaptive tau = 0.9
+TOL_TIGHT = 1e-4            # both, fixed eps = 1e-8
 
 
 def thetas16():
