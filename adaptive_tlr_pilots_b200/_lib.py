@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "libtlr_b200.so")
 
 TLR_RULE_FIXED = 0
 TLR_RULE_ADAPTIVE = 1
+TLR_RULE_MIXED = 2
 PRECISIONS = {"fp64": 0, "mixed": 1}
 RANK_MAP = {"rule": 0, "record": 1, "replay": 2}
 ERR_RANK_CAP = -2  # TLR_ERR_RANK_CAP: a tile rank exceeded the plan's capacity
@@ -80,6 +81,8 @@ SIGNATURES = {
                                             ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "tlr_plan_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tlr_plan_rank_map": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tlr_factor_storage": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_longlong)]),
     "tlr_truncate_tiles": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int,
                                           ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong,
                                           ctypes.POINTER(TlrTileStats), ctypes.POINTER(ctypes.c_int)]),

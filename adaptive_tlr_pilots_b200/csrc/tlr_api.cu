@@ -96,6 +96,10 @@ struct tlr_plan {
   int rmode = 0;
   // per initial tile: truncation error ||T - T_r||_F and ||T||_F (the assembled rule's outputs)
   double *tail0 = nullptr, *fro0 = nullptr;
+  // storage rule 'mixed': bits of every stored factor tile (index i (i - 1) / 2 + k), and whether the
+  // last evaluation used the rule
+  int* prec = nullptr;
+  int round_store = 0;
   std::vector<size_t> rlog_off;
   // launch accounting and optional per-kernel event timing
   bool prof = false;
@@ -225,7 +229,8 @@ int run_compression(tlr_plan* p, double sigma2, double inv_range, int rule_fixed
       LAUNCH(TLR_K_FINALIZE, tlr::launch_finalize(p->n, p->b, k, ldp, p->cap,
                                 p->precision == TLR_PRECISION_MIXED ? kMarginMixed : kMargin, rule_fixed, thr_rel, thr_abs, base, p->ti,
                                 p->tj, p->need, Pp, p->C, p->parts, p->fparts, fused ? 1 : p->nblk, p->gscr, p->gsv, p->U,
-                                p->V, p->rank, lev == kLevels - 1 ? 1 : 0, nc, p->rlog, p->rmode, p->tail0, p->fro0, p->status, s));
+                                p->V, p->rank, lev == kLevels - 1 ? 1 : 0, nc, p->rlog, p->rmode, p->tail0, p->fro0,
+                                p->round_store, p->status, s));
     }
   }
   return 0;
@@ -240,7 +245,7 @@ int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugge
   LAUNCH(TLR_K_POTRF, tlr::launch_potrf(p->D, p->n, p->b, 0, p->rhs, p->z, p->ldpart, p->qpart, p->status, s));
   for (int k = 0; k < p->nB; ++k) {
     LAUNCH(TLR_K_TRSM, tlr::launch_trsm(p->D, p->n, p->b, k, p->nB, p->U, p->V, p->Wd, p->Yd, p->rank, p->cap, p->z, p->rhs,
-                                        p->status, s));
+                                        p->round_store, thr_abs, p->prec, p->status, s));
     const bool ahead = k + 1 < p->nB;
     if (ahead) {
       // A_{k+1,k+1} needs only the panels m <= k, all final once the panel solve of step k is
@@ -255,8 +260,8 @@ int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugge
     }
     LAUNCH(TLR_K_RECOMPRESS, tlr::launch_recompress(p->n, p->b, k, p->nB, p->U, p->V, p->rank, p->cap, rule_fixed,
                                                     thr_rel, thr_abs, p->rcs, p->slot_doubles, p->nslots,
-                                                    p->rc_next + k, p->rlog + p->rlog_off[k], p->rmode, p->status,
-                                                    s));
+                                                    p->rc_next + k, p->rlog + p->rlog_off[k], p->rmode,
+                                                    p->round_store, p->round_store, p->status, s));
     if (ahead) TRY(cuda_check(cudaStreamWaitEvent(s, p->ev_diag, 0), "wait"));
   }
   LAUNCH(TLR_K_FINISH, tlr::launch_finish(p->nB, p->n, p->ldpart, p->qpart, p->out, p->status, s));
@@ -672,6 +677,7 @@ int tlr_plan_create(tlr_plan** plan, int n, int b, int cap, int device, void* st
   A(dalloc(p, &p->rlog, rl));
   A(dalloc(p, &p->tail0, nt));
   A(dalloc(p, &p->fro0, nt));
+  A(dalloc(p, &p->prec, nt));
   if (rc == 0) {
     rc = cuda_check(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking), "side stream");
     if (!rc) rc = cuda_check(cudaEventCreateWithFlags(&p->ev_panel, cudaEventDisableTiming), "event");
@@ -824,13 +830,16 @@ namespace {
 int enqueue_forward(tlr_plan* p, const double theta[3], int rule, double value) {
   if (!p || !theta) return fail(TLR_ERR_ARG, "invalid arguments to tlr_loglik");
   if (!p->has_data) return fail(TLR_ERR_NOT_READY, "tlr_set_data has not been called");
-  if (rule != TLR_RULE_FIXED && rule != TLR_RULE_ADAPTIVE) return fail(TLR_ERR_ARG, "rule must be fixed or adaptive");
+  if (rule != TLR_RULE_FIXED && rule != TLR_RULE_ADAPTIVE && rule != TLR_RULE_MIXED)
+    return fail(TLR_ERR_ARG, "rule must be fixed, adaptive or mixed");
   const double sigma2 = theta[0], range = theta[1], eta = theta[2];
   if (!(range > 0.0) || !std::isfinite(sigma2) || !std::isfinite(eta) || !std::isfinite(range))
     return fail(TLR_ERR_ARG, "theta must be finite with range > 0");
   TRY(cuda_check(cudaSetDevice(p->device), "cudaSetDevice"));
   cudaStream_t s = p->stream;
   p->factor_ok = false;
+  // rule 'mixed' (17:145-148): the adaptive thresholds, every stored factor pair rounded
+  p->round_store = rule == TLR_RULE_MIXED ? 1 : 0;
   // thresholds: codes/17_tlr_cholesky_pilot.py:143-150 (b = largest tile = b)
   const int rule_fixed = rule == TLR_RULE_FIXED;
   const double thr_rel = rule_fixed ? value : 0.0;
@@ -957,6 +966,7 @@ int tlr_truncate_tiles(tlr_plan* p, const double theta[3], int rule, double valu
   const double sigma2 = theta[0], range = theta[1], eta = theta[2];
   if (!(range > 0.0) || !std::isfinite(sigma2) || !std::isfinite(eta) || !std::isfinite(range))
     return fail(TLR_ERR_ARG, "theta must be finite with range > 0");
+  p->round_store = 0;
   if (K_dev && ldk < p->n) return fail(TLR_ERR_ARG, "ldk must be at least N");
   if (K_dev && (long long)p->nB * (p->nB + 1) / 2 > 65535)
     return fail(TLR_ERR_ARG, "the dense write-out takes at most 361 tiles per side");
@@ -1036,6 +1046,30 @@ int tlr_plan_rank_map(tlr_plan* p, int mode) {
     return fail(TLR_ERR_ARG, "rank map mode must be TLR_RANKS_RULE, TLR_RANKS_RECORD or TLR_RANKS_REPLAY");
   static_assert(TLR_RANKS_RECORD == tlr::kRankRecord && TLR_RANKS_REPLAY == tlr::kRankReplay, "rank map modes");
   p->rmode = mode;
+  return 0;
+}
+
+int tlr_factor_storage(tlr_plan* p, int* bits, long long* stored_bytes) {
+  if (!p) return fail(TLR_ERR_ARG, "plan is NULL");
+  if (!p->factor_ok) return fail(TLR_ERR_NOT_READY, "the plan holds no completed factorization");
+  TRY(cuda_check(cudaSetDevice(p->device), "cudaSetDevice"));
+  const int nB = p->nB, b = p->b, n = p->n;
+  std::vector<int> pr((size_t)std::max(p->ntiles, 1), 64);
+  if (p->round_store && p->ntiles > 0)
+    TRY(cuda_check(cudaMemcpy(pr.data(), p->prec, sizeof(int) * p->ntiles, cudaMemcpyDeviceToHost), "bits"));
+  auto bsz = [&](int i) { return std::min(b, n - i * b); };
+  long long byt = 0;
+  int q = 0;
+  for (int k = 0; k < nB; ++k) byt += 8LL * bsz(k) * bsz(k);
+  for (int k = 0; k < nB; ++k)
+    for (int i = k + 1; i < nB; ++i) {
+      const int t = i * (i - 1) / 2 + k;
+      const int r = p->h_rank[t];
+      const int bt = (p->round_store && r > 0) ? pr[t] : 64;
+      byt += 2LL * r * bsz(i) * bt / 8;
+      if (bits) bits[q++] = bt;
+    }
+  if (stored_bytes) *stored_bytes = byt;
   return 0;
 }
 

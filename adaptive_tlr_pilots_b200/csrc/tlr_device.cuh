@@ -5,6 +5,7 @@
 // All reductions are deterministic (fixed shuffle/shared-memory order): a log-likelihood
 // evaluated twice on the same inputs is bit-identical.
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -107,6 +108,112 @@ __device__ __forceinline__ int select_rank(const double* sig, int m, double extr
   }
   if (tail_at_rank) *tail_at_rank = tr;
   return r;
+}
+
+// ---------------------------------------------------------------- storage precision (rule 'mixed')
+// x rounded to p-bit storage as the reference simulates it (codes/17_tlr_cholesky_pilot.py:41-55):
+// p = 32 / 16 an IEEE cast with round-to-nearest-even (numpy's astype), p = 8 |x| = m 2^e with
+// e = floor(log2 |x|) clipped to [-9, 8] and m rounded to 3 fraction bits (half to even), at most
+// 448.  The exponent is read exactly with frexp; where numpy's floor(log2) lands one higher (|x|
+// just below a power of two) both roundings give the same power of two.
+__device__ __forceinline__ double round_bits(double x, int p) {
+  if (p == 32) return (double)__double2float_rn(x);
+  if (p == 16) return (double)__half2float(__double2half(x));
+  if (p == 8) {
+    const double a = fabs(x);
+    if (a == 0.0) return 0.0;
+    int ex;
+    frexp(a, &ex);
+    const int e = min(max(ex - 1, -9), 8);
+    const double v = fmin(rint(ldexp(a, -e) * 8.0) / 8.0 * ldexp(1.0, e), 448.0);
+    return copysign(v, x);
+  }
+  return x;
+}
+
+// A factor entry as stored in p bits (17:58-66): for p < 32 scaled so that the factor's largest
+// magnitude `top` maps to half the format's largest value (224 FP8, 32752 FP16), rounded, unscaled.
+__device__ __forceinline__ double store_entry(double x, int p, double top) {
+  if (p == 64 || top == 0.0) return x;
+  if (p == 32) return round_bits(x, 32);
+  const double scale = (p == 8 ? 224.0 : 32752.0) / top;
+  return round_bits(x * scale, p) / scale;
+}
+
+// Maximum over the CTA; every thread gets the result.  `red` needs 33 doubles of shared memory.
+__device__ __forceinline__ double block_max(double v, double* red) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_max(v);
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    double m = lane < nw ? red[lane] : 0.0;
+    m = warp_max(m);
+    if (lane == 0) red[32] = m;
+  }
+  __syncthreads();
+  return red[32];
+}
+
+// Store the pair (U: mu x r, V: mv x r, column-major, leading dimension ld) in the fewest bits
+// p in {8, 16, 32} with ||U V^T - U~ V~^T||_F <= budget, else keep FP64 (17:69-82); U and V are
+// rounded in place and p returned (every thread).  The error is formed from six r x r Gram
+// products, ||E||^2 = <dU^T dU, V^T V> + 2 <dU^T U~, V^T dV> + <U~^T U~, dV^T dV> (E = dU V^T +
+// U~ dV^T, dU = U - U~, dV = V - V~), whose terms are all of the size of the rounding error, so
+// nothing large cancels.  `red` needs 33 doubles of shared memory.
+__device__ inline int cta_round_pair(double* U, double* V, int mu, int mv, int r, int ld, double budget,
+                                     double* red) {
+  if (r == 0) return 64;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+  double mxu = 0.0, mxv = 0.0;
+  for (int q = 0; q < r; ++q) {
+    for (int a = tid; a < mu; a += blockDim.x) mxu = fmax(mxu, fabs(U[(size_t)q * ld + a]));
+    for (int a = tid; a < mv; a += blockDim.x) mxv = fmax(mxv, fabs(V[(size_t)q * ld + a]));
+  }
+  const double topu = block_max(mxu, red);
+  const double topv = block_max(mxv, red);
+  int chosen = 64;
+  for (int p = 8; p <= 32; p *= 2) {
+    // one warp per (c, d): the (c, d) entries of the six Gram products
+    double part = 0.0;
+    for (int e = warp; e < r * r; e += nwarp) {
+      const int c = e % r, d = e / r;
+      double g1 = 0.0, g2 = 0.0, g3 = 0.0, h1 = 0.0, h2 = 0.0, h3 = 0.0;
+      const double* uc = U + (size_t)c * ld;
+      const double* ud = U + (size_t)d * ld;
+      const double* vc = V + (size_t)c * ld;
+      const double* vd = V + (size_t)d * ld;
+      for (int a = lane; a < mu; a += 32) {
+        const double rc = store_entry(uc[a], p, topu), rd = store_entry(ud[a], p, topu);
+        const double dc = uc[a] - rc, dd = ud[a] - rd;
+        g1 = fma(dc, dd, g1);  // dU^T dU
+        g2 = fma(dc, rd, g2);  // dU^T U~
+        g3 = fma(rc, rd, g3);  // U~^T U~
+      }
+      for (int a = lane; a < mv; a += 32) {
+        const double rd = store_entry(vd[a], p, topv);
+        const double dc = vc[a] - store_entry(vc[a], p, topv), dd = vd[a] - rd;
+        h1 = fma(vc[a], vd[a], h1);  // V^T V
+        h2 = fma(vc[a], dd, h2);     // V^T dV
+        h3 = fma(dc, dd, h3);        // dV^T dV
+      }
+      g1 = warp_sum(g1); g2 = warp_sum(g2); g3 = warp_sum(g3);
+      h1 = warp_sum(h1); h2 = warp_sum(h2); h3 = warp_sum(h3);
+      part += g1 * h1 + 2.0 * g2 * h2 + g3 * h3;
+    }
+    // every lane of a warp holds the warp's sum; count it once per warp
+    const double err2 = block_sum(lane == 0 ? part : 0.0, red);
+    if (sqrt(fmax(err2, 0.0)) <= budget) { chosen = p; break; }
+  }
+  if (chosen < 64) {
+    for (int q = 0; q < r; ++q) {
+      for (int a = tid; a < mu; a += blockDim.x) U[(size_t)q * ld + a] = store_entry(U[(size_t)q * ld + a], chosen, topu);
+      for (int a = tid; a < mv; a += blockDim.x) V[(size_t)q * ld + a] = store_entry(V[(size_t)q * ld + a], chosen, topv);
+    }
+  }
+  __syncthreads();
+  return chosen;
 }
 
 // ---------------------------------------------------------------- Householder QR

@@ -109,10 +109,11 @@ __global__ void __launch_bounds__(256) k_diag_build(const double* TLR_RESTRICT x
 // ----------------------------------------------------------------------------------------
 // Panel solve for column k: one CTA per row tile i > k.
 __global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int n, int b, int k, int nB,
-                                             const double* TLR_RESTRICT U, double* TLR_RESTRICT V,
+                                             double* TLR_RESTRICT U, double* TLR_RESTRICT V,
                                              double* TLR_RESTRICT Wd, double* TLR_RESTRICT Y,
                                              const int* TLR_RESTRICT rank, int cap,
                                              const double* TLR_RESTRICT z, double* TLR_RESTRICT rhs,
+                                             int round_store, double thr_abs, int* TLR_RESTRICT prec,
                                              const int* TLR_RESTRICT status) {
   if (*status != 0) return;
   const int i = k + 1 + blockIdx.x;
@@ -123,7 +124,7 @@ __global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int 
   const int bk = min(b, n - k * b), bi = min(b, n - i * b);
   const double* L = D + (size_t)k * b * b;
   double* Vt = V + (size_t)t * b * cap;
-  const double* Ut = U + (size_t)t * b * cap;
+  double* Ut = U + (size_t)t * b * cap;
   if (threadIdx.x == 0) add_work(status, 9, (double)bk * bk * r + 2.0 * bk * r * r + 4.0 * bk * r,
                                  8.0 * ((double)bk * bk * 0.5 + 2.0 * bk * r + bi * r));
   __shared__ double L11[32][33];
@@ -189,6 +190,11 @@ __global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int 
     }
   }
   __syncthreads();
+  if (round_store) {  // storage rule 'mixed': the factor tile rounded under the full budget (17:183-184)
+    __shared__ double rred[40];
+    const int bits = cta_round_pair(Ut, Vt, bi, bk, r, b, thr_abs, rred);
+    if (tid == 0) prec[t] = bits;
+  }
   // W = V^T V (r x r) and t = V^T z_k
   const double* zk = z + (size_t)k * b;
   double* W = Wd + (size_t)t * cap * cap;
@@ -297,6 +303,98 @@ __device__ void cta_atb(const double* A, int lda, const double* B, int ldb, int 
   }
 }
 
+// General recompression of one trailing pair, the reference's recompress as written
+// (codes/17_tlr_cholesky_pilot.py:119-133): Householder QR of A = [U_ij, -U_ik W] and
+// B = [V_ij, U_jk] (no orthogonality assumed), SVD of the core R_u R_v^T by one-sided Jacobi on
+// its transpose, the rule's rank, U' = Q_u U_w s, V' = Q_v V_w.  The storage rule 'mixed' uses it:
+// its rounded factors are no longer orthogonal, which the structured projection needs.  The new
+// pair overwrites the tile (i, j); with round_store it is then rounded under the budget left after
+// truncation (17:203-204).  Returns the new rank, or -1 after setting an error status.
+__device__ int rc_general_pair(int bi, int bj, int b, int cap, int r1, int ri, int rj, const double* Uik,
+                               const double* Ujk, const double* W, double* Uw, double* Vw, RcScratch& S,
+                               double* sig, int* perm, int* iflag, double* red, int* rsel, int rule_fixed,
+                               double thr_rel, double thr_abs, int round_store, int* rlog_pp, int rmode,
+                               int* status) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int s = r1 + rj, ls = 2 * cap;
+  const int ku = min(bi, s), kv = min(bj, s);
+  double* A = S.X;   // b x 2 cap (X and Y are contiguous)
+  double* B = S.Uo;  // b x 2 cap (Uo and Vo are contiguous)
+  for (int q = 0; q < r1; ++q) {
+    for (int a = tid; a < bi; a += nt) A[(size_t)q * b + a] = Uw[(size_t)q * b + a];
+    for (int a = tid; a < bj; a += nt) B[(size_t)q * b + a] = Vw[(size_t)q * b + a];
+  }
+  for (int q = 0; q < rj; ++q) {
+    for (int a = tid; a < bi; a += nt) {
+      double acc = 0.0;
+      for (int p = 0; p < ri; ++p) acc = fma(Uik[(size_t)p * b + a], W[(size_t)q * cap + p], acc);
+      A[(size_t)(r1 + q) * b + a] = -acc;
+    }
+    for (int a = tid; a < bj; a += nt) B[(size_t)(r1 + q) * b + a] = Ujk[(size_t)q * b + a];
+  }
+  __syncthreads();
+  // A = Q_u R_u, B = Q_v R_v (R upper trapezoidal ku x s / kv x s, Q explicit bi x ku / bj x kv)
+  cta_geqr2(A, b, bi, s, sig, red);
+  cta_copy_r(A, b, ku, s, S.Ru, ls);
+  cta_org2r(A, b, bi, ku, sig);
+  cta_geqr2(B, b, bj, s, sig, red);
+  cta_copy_r(B, b, kv, s, S.Rv, ls);
+  cta_org2r(B, b, bj, kv, sig);
+  // Z = (R_u R_v^T)^T (kv x ku): Z[c][a] = sum_t R_u[a][t] R_v[c][t], t >= max(a, c)
+  for (int e = tid; e < ku * kv; e += nt) {
+    const int c = e % kv, a = e / kv;
+    double acc = 0.0;
+    for (int t = max(a, c); t < s; ++t) acc = fma(S.Ru[(size_t)t * ls + a], S.Rv[(size_t)t * ls + c], acc);
+    S.M[(size_t)a * ls + c] = acc;
+  }
+  __syncthreads();
+  // Z J = Z' (orthogonal columns): core = J Z'^T, left singular vectors J, right Z' / sigma
+  cta_jacobi_svd(S.M, ls, kv, ku, S.Vs, ls, sig, perm, iflag, 40, 1e-28);
+  if (tid == 0) {
+    double srt[256];
+    double fro2 = 0.0;
+    for (int q = 0; q < ku; ++q) srt[q] = sig[perm[q]];
+    for (int q = ku - 1; q >= 0; --q) fro2 += srt[q] * srt[q];
+    const double thr = rule_fixed ? thr_rel * sqrt(fro2) : thr_abs;
+    int r = select_rank(srt, ku, 0.0, thr, nullptr);
+    if (r < 0) r = ku;
+    if (rmode == kRankReplay) r = min(*rlog_pp, ku);
+    else if (rmode == kRankRecord) *rlog_pp = r;
+    double tail2 = 0.0;
+    for (int q = ku - 1; q >= r; --q) tail2 += srt[q] * srt[q];
+    if (r > cap) {
+      atomicCAS(status, 0, -2);
+      r = -1;
+    }
+    rsel[0] = r;
+    reinterpret_cast<double*>(rsel + 2)[0] = sqrt(tail2);
+  }
+  __syncthreads();
+  const int rn = rsel[0];
+  const double tail = reinterpret_cast<double*>(rsel + 2)[0];
+  if (rn < 0) return -1;
+  // U' = Q_u (J[:, perm c] sigma), V' = Q_v (Z'[:, perm c] / sigma): over the tile's own slot
+  for (int c = 0; c < rn; ++c) {
+    const int pc = perm[c];
+    const double sg = sig[pc], inv = sg > 0.0 ? 1.0 / sg : 0.0;
+    const double* jc = S.Vs + (size_t)pc * ls;
+    const double* zc = S.M + (size_t)pc * ls;
+    for (int a = tid; a < bi; a += nt) {
+      double acc = 0.0;
+      for (int q = 0; q < ku; ++q) acc = fma(A[(size_t)q * b + a], jc[q], acc);
+      Uw[(size_t)c * b + a] = acc * sg;
+    }
+    for (int a = tid; a < bj; a += nt) {
+      double acc = 0.0;
+      for (int q = 0; q < kv; ++q) acc = fma(B[(size_t)q * b + a], zc[q], acc);
+      Vw[(size_t)c * b + a] = acc * inv;
+    }
+  }
+  __syncthreads();
+  if (round_store) cta_round_pair(Uw, Vw, bi, bj, rn, b, thr_abs - tail, red);
+  return rn;
+}
+
 constexpr int kRcSmemS = 32;  // cores with s <= 32 are solved in shared memory
 constexpr int kRcT = 256;     // threads per pair
 constexpr int kRcW = kRcT / 32;
@@ -307,7 +405,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
                                                    int rule_fixed, double thr_rel, double thr_abs,
                                                    double* TLR_RESTRICT scratch, size_t slot_doubles,
                                                    int* TLR_RESTRICT next_pair, int* TLR_RESTRICT rlog, int rmode,
-                                                   int* TLR_RESTRICT status) {
+                                                   int general, int round_store, int* TLR_RESTRICT status) {
   if (*status != 0) return;
   const int mB = nB - k - 1;  // trailing tiles
   const long npairs = (long)mB * (mB - 1) / 2;  // every trailing pair (i, j), k < j < i
@@ -325,6 +423,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
   __shared__ int perm[256];
   __shared__ int iflag;
   __shared__ int rsel;
+  __shared__ __align__(8) int gsel[4];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int ls = 2 * cap;
   if (blockIdx.x == 0 && tid == 0) {  // the panel column k is read once per step
@@ -385,6 +484,19 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
       }
     }
     __syncthreads();
+    if (general) {  // storage rule 'mixed': the reference's recompression as written
+      const int rn = rc_general_pair(bi, bj, b, cap, r1, ri, rj, Uik, Ujk, S.W, U + (size_t)tij * b * cap,
+                                     V + (size_t)tij * b * cap, S, sig, perm, &iflag, red, gsel, rule_fixed,
+                                     thr_rel, thr_abs, round_store, rlog + pp, rmode, status);
+      if (rn < 0) return;
+      if (tid == 0) {
+        rank[tij] = rn;
+        add_work(status, 10, 4.0 * b * ri * rj + 16.0 * b * s * s + 4.0 * b * s * rn,
+                 8.0 * ((double)(bi + bj) * r1 + (double)(bi + bj) * rn));
+      }
+      __syncthreads();
+      continue;
+    }
     // X = -U_ik W (bi x rj)
     for (int q = 0; q < rj; ++q)
       for (int a = tid; a < bi; a += kRcT) {
@@ -603,16 +715,19 @@ int launch_diag_build(const double* xy, int n, int b, int k, double sigma2, doub
   return (int)cudaGetLastError();
 }
 
-int launch_trsm(const double* D, int n, int b, int k, int nB, const double* U, double* V, double* Wd, double* Y,
-                const int* rank, int cap, const double* z, double* rhs, const int* status, cudaStream_t s) {
+int launch_trsm(const double* D, int n, int b, int k, int nB, double* U, double* V, double* Wd, double* Y,
+                const int* rank, int cap, const double* z, double* rhs, int round_store, double thr_abs, int* prec,
+                const int* status, cudaStream_t s) {
   if (nB - k - 1 <= 0) return 0;
-  k_trsm<<<nB - k - 1, 256, 0, s>>>(D, n, b, k, nB, U, V, Wd, Y, rank, cap, z, rhs, status);
+  k_trsm<<<nB - k - 1, 256, 0, s>>>(D, n, b, k, nB, U, V, Wd, Y, rank, cap, z, rhs, round_store, thr_abs, prec,
+                                    status);
   return (int)cudaGetLastError();
 }
 
 int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, int rule_fixed,
                       double thr_rel, double thr_abs, double* scratch, size_t slot_doubles, int nslots,
-                      int* next_pair, int* rlog_step, int rmode, int* status, cudaStream_t s) {
+                      int* next_pair, int* rlog_step, int rmode, int general, int round_store, int* status,
+                      cudaStream_t s) {
   const long mB = nB - k - 1;
   const long npairs = mB * (mB - 1) / 2;
   if (npairs <= 0) return 0;
@@ -620,7 +735,7 @@ int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* ra
   const size_t sm = (size_t)3 * kRcSmemS * kRcSmemS * 8;
   cudaFuncSetAttribute(k_recompress, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   k_recompress<<<grid, kRcT, sm, s>>>(n, b, k, nB, U, V, rank, cap, rule_fixed, thr_rel, thr_abs, scratch,
-                                     slot_doubles, next_pair, rlog_step, rmode, status);
+                                     slot_doubles, next_pair, rlog_step, rmode, general, round_store, status);
   return (int)cudaGetLastError();
 }
 

@@ -39,7 +39,7 @@ int launch_finalize(int n, int b, int k, int ldp, int cap, int margin, int rule_
                     double thr_abs, int tile_base, const int* ti, const int* tj, int* need, const double* P,
                     const double* C, const double* parts, const double* fparts, int nblk, double* gscratch,
                     double* gsv, double* U, double* V, int* rank, int last_level, int nchunk, int* rlog,
-                    int rmode, double* tail0, double* fro0, int* status, cudaStream_t s);
+                    int rmode, double* tail0, double* fro0, int round_store, int* status, cudaStream_t s);
 
 // factorization
 int launch_diag_build(const double* xy, int n, int b, int k, double sigma2, double inv_range, int nu5,
@@ -50,14 +50,16 @@ int launch_potrf(double* D, int n, int b, int k, double* rhs, double* z, double*
 // nbatch tiles, tile q at D + q sD, rhs / z + q sV, ldpart / qpart / status + q sS
 int launch_potrf_batched(double* D, int n, int b, int k, double* rhs, double* z, double* ldpart, double* qpart,
                          int* status, int nbatch, size_t sD, size_t sV, int sS, cudaStream_t s);
-int launch_trsm(const double* D, int n, int b, int k, int nB, const double* U, double* V, double* Wd, double* Y,
-                const int* rank, int cap, const double* z, double* rhs, const int* status, cudaStream_t s);
+int launch_trsm(const double* D, int n, int b, int k, int nB, double* U, double* V, double* Wd, double* Y,
+                const int* rank, int cap, const double* z, double* rhs, int round_store, double thr_abs, int* prec,
+                const int* status, cudaStream_t s);
 size_t rc_slot_doubles(int b, int cap);
 // every trailing pair of step k; next_pair: a counter that is zero at launch (the CTAs claim
 // pairs past the grid through it)
 int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, int rule_fixed,
                       double thr_rel, double thr_abs, double* scratch, size_t slot_doubles, int nslots,
-                      int* next_pair, int* rlog_step, int rmode, int* status, cudaStream_t s);
+                      int* next_pair, int* rlog_step, int rmode, int general, int round_store, int* status,
+                      cudaStream_t s);
 // assembled-matrix rule: dense Sigma^TLR from the initial compression (N x N, leading dimension ldk)
 int launch_assemble(const double* xy, int n, int b, double sigma2, double inv_range, int nu5, double nugget,
                     const double* U, const double* V, const int* rank, int cap, double* K, long long ldk,

@@ -23,7 +23,8 @@ import numpy as np
 
 from . import _lib
 
-RULES = {"fixed": _lib.TLR_RULE_FIXED, "adaptive": _lib.TLR_RULE_ADAPTIVE}
+RULES = {"fixed": _lib.TLR_RULE_FIXED, "adaptive": _lib.TLR_RULE_ADAPTIVE, "mixed": _lib.TLR_RULE_MIXED}
+STORAGE_BITS = (8, 16, 32, 64)
 KERNELS = (1.5, 2.5)  # Matern smoothness nu
 _NU = 1.5
 
@@ -228,6 +229,16 @@ class Plan:
         if rc == 0:
             d.update(stored_factor=int(info.stored_factor), mean_rank_factor=float(info.mean_rank_factor),
                      max_rank_factor=int(info.max_rank_factor), logdet=float(info.logdet), quad=float(info.quad))
+            if rule == "mixed":  # the storage bookkeeping of codes/17_tlr_cholesky_pilot.py:210-214
+                bits = np.zeros(max(self.ntiles, 1), dtype=np.int32)
+                byt = ctypes.c_longlong(0)
+                _lib.check(self.lib.tlr_factor_storage(self.handle, bits.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                                       ctypes.byref(byt)))
+                bits = [int(v) for v in bits[: self.ntiles]]
+                dense = self.n * (self.n + 1) // 2 * 8
+                d.update(stored_factor_bytes=int(byt.value), dense_factor_bytes=dense,
+                         factor_bytes_frac=byt.value / dense, factor_prec=bits,
+                         precision_mix_factor_tiles={q: bits.count(q) for q in STORAGE_BITS})
         else:
             d.update(failed_at=int(info.failed_at))
         return Evaluation(rc, float(ll.value) if rc == 0 else None, d, fr[: self.ntiles], sr[: self.ntiles],

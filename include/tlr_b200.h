@@ -27,6 +27,9 @@ extern "C" {
 /* rank rules: codes/17_tlr_cholesky_pilot.py:149-150 */
 #define TLR_RULE_FIXED 0    /* relative Frobenius tolerance eps per tile */
 #define TLR_RULE_ADAPTIVE 1 /* absolute budget tau * b * sigma2 * eta / N */
+#define TLR_RULE_MIXED 2    /* adaptive ranks, every stored factor pair rounded to the fewest bits
+                               (FP8 / FP16 / FP32 / FP64) that fit the budget left after
+                               truncation: codes/17_tlr_cholesky_pilot.py:33-82, 145-148 */
 
 /* status codes */
 #define TLR_OK 0
@@ -177,6 +180,14 @@ int tlr_plan_set_precision(tlr_plan* plan, int mode);
  * ranks-frozen gradient).  Replay needs a recorded evaluation of the same rule on the same data.
  * No counterpart in the reference, whose finite-difference Hessian
  * (codes/15_pilot_standard_errors.py:21-31) lets the rule re-pick the ranks at every point. */
+/* Storage of the factor left by the last completed evaluation: bits[q] (8, 16, 32 or 64) of
+ * every off-diagonal factor tile in the reference's L_off order (for k, for i > k), and the stored
+ * bytes (dense FP64 diagonal tiles + 2 b_i r_ik bits / 8 per off-diagonal tile).  Replaces the
+ * precision bookkeeping of rule 'mixed', codes/17_tlr_cholesky_pilot.py:38, 184, 210-214 (PREC_OF,
+ * stored_factor_bytes, precision_mix_factor_tiles); every tile is 64 bits under the other rules.
+ * bits and stored_bytes are host pointers and may be NULL.  TLR_ERR_NOT_READY without a factor. */
+int tlr_factor_storage(tlr_plan* plan, int* bits, long long* stored_bytes);
+
 #define TLR_RANKS_RULE 0
 #define TLR_RANKS_RECORD 1
 #define TLR_RANKS_REPLAY 2

@@ -173,6 +173,65 @@ def thresholds(n, b, theta, rule, value):
     return thr_rel, thr_abs
 
 
+# ------------------------------------------------------- storage precision (rule 'mixed')
+STORAGE_BITS = (8, 16, 32, 64)
+
+
+def round_fp8(x):
+    """The reference's simulated FP8 (E4M3-like) rounding: |x| = m 2^e with e = floor(log2|x|)
+    clipped to [-9, 8], m rounded to 3 fraction bits (half to even), values above 448 set to 448,
+    zeros kept.  codes/17_tlr_cholesky_pilot.py:41-55 (the p = 8 branch)."""
+    x = np.asarray(x, dtype=np.float64)
+    a = np.abs(x)
+    out = np.zeros_like(x)
+    nz = a > 0
+    e = np.clip(np.floor(np.log2(a[nz])), -9, 8)
+    v = np.round(a[nz] / 2.0 ** e * 8.0) / 8.0 * 2.0 ** e
+    out[nz] = np.sign(x[nz]) * np.minimum(v, 448.0)
+    return out
+
+
+def round_bits(x, p):
+    """x rounded to p-bit storage: 64 unchanged, 32 / 16 through numpy float32 / float16 casts,
+    8 through round_fp8.  codes/17_tlr_cholesky_pilot.py:41-55."""
+    if p == 64:
+        return x
+    if p == 32:
+        return x.astype(np.float32).astype(np.float64)
+    if p == 16:
+        return x.astype(np.float16).astype(np.float64)
+    return round_fp8(x)
+
+
+def store_factor(U, p):
+    """A factor as stored in p bits: for p < 32 scaled so its largest magnitude is half the
+    format's largest value (224 for FP8, 32752 for FP16) before rounding, unscaled after.
+    codes/17_tlr_cholesky_pilot.py:58-66."""
+    if p == 64 or U.size == 0:
+        return U
+    top = np.abs(U).max()
+    if top == 0:
+        return U
+    if p == 32:
+        return round_bits(U, 32)
+    scale = (224.0 if p == 8 else 32752.0) / top
+    return round_bits(U * scale, p) / scale
+
+
+def round_pair(U, V, budget):
+    """(U', V', p): the pair stored in the fewest bits p in (8, 16, 32) whose rounding error
+    ||U V^T - U' V'^T||_F is at most `budget`, else unchanged with p = 64.
+    codes/17_tlr_cholesky_pilot.py:69-82."""
+    if U.shape[1] == 0:
+        return U, V, 64
+    T = U @ V.T
+    for p in STORAGE_BITS[:-1]:
+        Ur, Vr = store_factor(U, p), store_factor(V, p)
+        if np.linalg.norm(T - Ur @ Vr.T) <= budget:
+            return Ur, Vr, p
+    return U, V, 64
+
+
 # ------------------------------------------------------------------ TLR Cholesky
 def tlr_cholesky(S, theta, bounds, rule, value, rank_log=None, frozen=None, on_stage=None):
     """Right-looking TLR Cholesky of Sigma(theta) without forming Sigma.
@@ -187,8 +246,13 @@ def tlr_cholesky(S, theta, bounds, rule, value, rank_log=None, frozen=None, on_s
     on_stage: optional callable, called with ("compress", i) after tile row i is generated and
               compressed and with ("factor", k) after factorization step k (for stage timings).
     """
-    if rule not in ("fixed", "adaptive"):
-        raise ValueError(f"rule must be 'fixed' or 'adaptive', got {rule!r}")
+    if rule not in ("fixed", "adaptive", "mixed"):
+        raise ValueError(f"rule must be 'fixed', 'adaptive' or 'mixed', got {rule!r}")
+    # rule 'mixed' (17:33-40, 145-148): the adaptive ranks, every stored pair rounded by round_pair
+    mixed = rule == "mixed"
+    if mixed:
+        rule = "adaptive"
+    prec = {}  # (i, j) -> bits of the stored factor tile (rule 'mixed')
     n = S.shape[0]
     nB = len(bounds)
     b = max(e - s for s, e in bounds)
@@ -210,9 +274,11 @@ def tlr_cholesky(S, theta, bounds, rule, value, rank_log=None, frozen=None, on_s
         stored0 += (i1 - i0) ** 2
         for j, (j0, j1) in enumerate(bounds[:i]):
             T = sigma2 * matern(pairwise_dist(S[i0:i1], S[j0:j1]), rng)
-            U, V, _, r = truncate_svd(T, rule, thr_rel, thr_abs, pick(("init", i, j)))
+            U, V, tail, r = truncate_svd(T, rule, thr_rel, thr_abs, pick(("init", i, j)))
             if rank_log is not None:
                 rank_log[("init", i, j)] = r
+            if mixed:  # 17:163-164
+                U, V, _ = round_pair(U, V, thr_abs - tail)
             A_off[(i, j)] = (U, V)
             stored0 += 2 * r * max(i1 - i0, j1 - j0)
         if on_stage is not None:
@@ -236,6 +302,8 @@ def tlr_cholesky(S, theta, bounds, rule, value, rank_log=None, frozen=None, on_s
             U, V = A_off.pop((i, k))
             if U.shape[1]:
                 V = solve_triangular(Lkk, V, lower=True, check_finite=False)
+            if mixed:  # 17:183-184
+                U, V, prec[(i, k)] = round_pair(U, V, thr_abs)
             L_off[(i, k)] = (U, V)
         # trailing update A_ij -= L_ik L_jk^T with recompression: 17:186-205
         for i in range(k + 1, nB):
@@ -251,10 +319,12 @@ def tlr_cholesky(S, theta, bounds, rule, value, rank_log=None, frozen=None, on_s
                     A_diag[i] -= (Ui @ W) @ Ui.T
                 else:
                     Uij, Vij = A_off[(i, j)]
-                    Ur, Vr, _, r = recompress(np.hstack([Uij, -(Ui @ W)]), np.hstack([Vij, Uj]),
-                                              rule, thr_rel, thr_abs, pick(("rc", k, i, j)))
+                    Ur, Vr, tail, r = recompress(np.hstack([Uij, -(Ui @ W)]), np.hstack([Vij, Uj]),
+                                                 rule, thr_rel, thr_abs, pick(("rc", k, i, j)))
                     if rank_log is not None:
                         rank_log[("rc", k, i, j)] = r
+                    if mixed:  # 17:203-204
+                        Ur, Vr, _ = round_pair(Ur, Vr, thr_abs - tail)
                     A_off[(i, j)] = (Ur, Vr)
         if on_stage is not None:
             on_stage(("factor", k))
@@ -264,6 +334,13 @@ def tlr_cholesky(S, theta, bounds, rule, value, rank_log=None, frozen=None, on_s
     info.update(completed=True, stored_factor=int(stored),
                 mean_rank_factor=float(np.mean(ranks)) if ranks else 0.0,
                 max_rank_factor=int(max(ranks)) if ranks else 0, factor_ranks=ranks)
+    if mixed:  # bytes of the stored factor and the precision mix: 17:210-214
+        byt = sum(d.shape[0] ** 2 * 8 for d in L_diag) + sum(2 * u.shape[1] * u.shape[0] * prec[key] // 8
+                                                             for key, (u, _) in L_off.items())
+        dense = n * (n + 1) // 2 * 8
+        info.update(stored_factor_bytes=int(byt), dense_factor_bytes=int(dense), factor_bytes_frac=byt / dense,
+                    precision_mix_factor_tiles={q: int(sum(1 for key in L_off if prec[key] == q)) for q in STORAGE_BITS},
+                    factor_prec=[prec[key] for key in L_off])
     return L_diag, L_off, info
 
 

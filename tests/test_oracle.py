@@ -162,3 +162,19 @@ def test_oracle_assembled_rule_matches_reference():
             assert ll is None
         else:
             assert abs(ll - rec["loglik"]) <= 1e-10 * abs(rec["loglik"])
+
+
+@pytest.mark.parametrize("q", [0, 1, 2])
+def test_oracle_mixed_storage_rule_matches_reference(q):
+    """Rule 'mixed' (codes/17_tlr_cholesky_pilot.py:33-82): the oracle against the reference's
+    own outputs (tests/golden/make_golden_mixed_rule.py): ranks and storage precision of every
+    factor tile, stored bytes, log-likelihood."""
+    rec = json.load(open(os.path.join(GOLD, "golden_mixed_rule.json")))["cases"][q]
+    d = np.load(os.path.join(GOLD, rec["data"]))
+    bounds = O.tile_bounds(rec["n"], rec["b"])
+    ll, _, info = O.tlr_loglik(d["S"], d["y"], tuple(rec["theta"]), bounds, "mixed", rec["tau"])
+    assert info["factor_ranks"] == rec["factor_ranks"]
+    assert info["factor_prec"] == rec["factor_prec"]
+    assert info["stored_factor_bytes"] == rec["stored_factor_bytes"]
+    assert {str(k): v for k, v in info["precision_mix_factor_tiles"].items()} == rec["precision_mix_factor_tiles"]
+    assert abs(ll - rec["loglik"]) <= 1e-10 * abs(rec["loglik"])
