@@ -81,6 +81,9 @@ SIGNATURES = {
                                             ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "tlr_plan_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tlr_plan_rank_map": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tlr_plan_rank_map_size": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "tlr_plan_rank_map_io": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                            ctypes.c_longlong, ctypes.c_int]),
     "tlr_factor_storage": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                           ctypes.POINTER(ctypes.c_longlong)]),
     "tlr_truncate_tiles": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int,

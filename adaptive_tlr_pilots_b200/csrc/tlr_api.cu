@@ -93,6 +93,7 @@ struct tlr_plan {
   // rank map (tlr_plan_rank_map): ntiles initial ranks, then per step k the ranks of its trailing
   // pairs from rlog_off[k]
   int* rlog = nullptr;
+  int* blog = nullptr;  // storage bits of every rounding (rule 'mixed'): rlog's layout, then the panel solves'
   int rmode = 0;
   // per initial tile: truncation error ||T - T_r||_F and ||T||_F (the assembled rule's outputs)
   double *tail0 = nullptr, *fro0 = nullptr;
@@ -230,7 +231,7 @@ int run_compression(tlr_plan* p, double sigma2, double inv_range, int rule_fixed
                                 p->precision == TLR_PRECISION_MIXED ? kMarginMixed : kMargin, rule_fixed, thr_rel, thr_abs, base, p->ti,
                                 p->tj, p->need, Pp, p->C, p->parts, p->fparts, fused ? 1 : p->nblk, p->gscr, p->gsv, p->U,
                                 p->V, p->rank, lev == kLevels - 1 ? 1 : 0, nc, p->rlog, p->rmode, p->tail0, p->fro0,
-                                p->round_store, p->status, s));
+                                p->round_store, p->blog, p->status, s));
     }
   }
   return 0;
@@ -245,7 +246,8 @@ int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugge
   LAUNCH(TLR_K_POTRF, tlr::launch_potrf(p->D, p->n, p->b, 0, p->rhs, p->z, p->ldpart, p->qpart, p->status, s));
   for (int k = 0; k < p->nB; ++k) {
     LAUNCH(TLR_K_TRSM, tlr::launch_trsm(p->D, p->n, p->b, k, p->nB, p->U, p->V, p->Wd, p->Yd, p->rank, p->cap, p->z, p->rhs,
-                                        p->round_store, thr_abs, p->prec, p->status, s));
+                                        p->round_store, thr_abs, p->prec, p->blog + p->rlog_off[p->nB], p->rmode,
+                                        p->status, s));
     const bool ahead = k + 1 < p->nB;
     if (ahead) {
       // A_{k+1,k+1} needs only the panels m <= k, all final once the panel solve of step k is
@@ -260,7 +262,7 @@ int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugge
     }
     LAUNCH(TLR_K_RECOMPRESS, tlr::launch_recompress(p->n, p->b, k, p->nB, p->U, p->V, p->rank, p->cap, rule_fixed,
                                                     thr_rel, thr_abs, p->rcs, p->slot_doubles, p->nslots,
-                                                    p->rc_next + k, p->rlog + p->rlog_off[k], p->rmode,
+                                                    p->rc_next + k, p->rlog + p->rlog_off[k], p->blog + p->rlog_off[k], p->rmode,
                                                     p->round_store, p->round_store, p->status, s));
     if (ahead) TRY(cuda_check(cudaStreamWaitEvent(s, p->ev_diag, 0), "wait"));
   }
@@ -675,6 +677,7 @@ int tlr_plan_create(tlr_plan** plan, int n, int b, int cap, int device, void* st
   }
   p->rlog_off[p->nB] = rl;
   A(dalloc(p, &p->rlog, rl));
+  A(dalloc(p, &p->blog, rl + nt));
   A(dalloc(p, &p->tail0, nt));
   A(dalloc(p, &p->fro0, nt));
   A(dalloc(p, &p->prec, nt));
@@ -1046,6 +1049,24 @@ int tlr_plan_rank_map(tlr_plan* p, int mode) {
     return fail(TLR_ERR_ARG, "rank map mode must be TLR_RANKS_RULE, TLR_RANKS_RECORD or TLR_RANKS_REPLAY");
   static_assert(TLR_RANKS_RECORD == tlr::kRankRecord && TLR_RANKS_REPLAY == tlr::kRankReplay, "rank map modes");
   p->rmode = mode;
+  return 0;
+}
+
+long long tlr_plan_rank_map_size(const tlr_plan* p) { return p ? (long long)p->rlog_off[p->nB] : 0; }
+
+int tlr_plan_rank_map_io(tlr_plan* p, int* ranks, int* bits, long long count, int upload) {
+  if (!p) return fail(TLR_ERR_ARG, "plan is NULL");
+  const size_t total = p->rlog_off[p->nB];
+  if (count != (long long)total) return fail(TLR_ERR_ARG, "count must be tlr_plan_rank_map_size(plan)");
+  TRY(cuda_check(cudaSetDevice(p->device), "cudaSetDevice"));
+  TRY(cuda_check(cudaStreamSynchronize(p->stream), "rank map"));
+  const auto kind = upload ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+  if (ranks)
+    TRY(cuda_check(upload ? cudaMemcpy(p->rlog, ranks, sizeof(int) * total, kind)
+                          : cudaMemcpy(ranks, p->rlog, sizeof(int) * total, kind), "rank map ranks"));
+  if (bits)  // the rounding decisions then the panel solves' (total + ntiles)
+    TRY(cuda_check(upload ? cudaMemcpy(p->blog, bits, sizeof(int) * (total + p->ntiles), kind)
+                          : cudaMemcpy(bits, p->blog, sizeof(int) * (total + p->ntiles), kind), "rank map bits"));
   return 0;
 }
 

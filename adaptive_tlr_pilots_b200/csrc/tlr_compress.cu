@@ -641,7 +641,8 @@ __global__ void __launch_bounds__(1024) k_finalize(int n, int b, int k, int ldp,
                                                  double* TLR_RESTRICT Vo, int* TLR_RESTRICT rank,
                                                  int last_level, int w_in_smem, int* TLR_RESTRICT rlog,
                                                  int rmode, double* TLR_RESTRICT tail0, double* TLR_RESTRICT fro0,
-                                                 int round_store, int* TLR_RESTRICT status) {
+                                                 int round_store, int* TLR_RESTRICT blog,
+                                                 int* TLR_RESTRICT status) {
   if (*status != 0) return;
   const int c = blockIdx.x;
   if (!need[c]) return;
@@ -719,7 +720,9 @@ __global__ void __launch_bounds__(1024) k_finalize(int n, int b, int k, int ldp,
   }
   if (round_store) {  // storage rule 'mixed': rounded under the budget left after truncation (17:163-164)
     __syncthreads();
-    cta_round_pair(Ut, Vt, bi, bj, r, b, thr_abs - tail0[t], red);
+    const int bits = cta_round_pair(Ut, Vt, bi, bj, r, b, thr_abs - tail0[t], red,
+                                    rmode == kRankReplay ? blog[t] : 0);
+    if (threadIdx.x == 0 && rmode == kRankRecord) blog[t] = bits;
   }
   if (threadIdx.x == 0) {
     rank[t] = r;
@@ -814,14 +817,15 @@ int launch_finalize(int n, int b, int k, int ldp, int cap, int margin, int rule_
                     double thr_abs, int tile_base, const int* ti, const int* tj, int* need, const double* P,
                     const double* C, const double* parts, const double* fparts, int nblk, double* gscratch,
                     double* gsv, double* U, double* V, int* rank, int last_level, int nchunk, int* rlog,
-                    int rmode, double* tail0, double* fro0, int round_store, int* status, cudaStream_t s) {
+                    int rmode, double* tail0, double* fro0, int round_store, int* blog, int* status,
+                    cudaStream_t s) {
   size_t sm = (40 + 136 * 3 + 8 + (k <= 64 ? 2 * (size_t)k * k : 0)) * 8;
   const int w_in_smem = k <= 64 && (size_t)b * k * 8 <= 160 * 1024;
   if (w_in_smem) sm += (size_t)b * k * 8;
   cudaFuncSetAttribute(k_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   k_finalize<<<nchunk, k >= 32 ? 1024 : 256, sm, s>>>(n, b, k, ldp, cap, margin, rule_fixed, thr_rel, thr_abs, tile_base, ti, tj, need,
                                      P, C, parts, fparts, nblk, gscratch, gsv, U, V, rank, last_level, w_in_smem,
-                                     rlog, rmode, tail0, fro0, round_store, status);
+                                     rlog, rmode, tail0, fro0, round_store, blog, status);
   return (int)cudaGetLastError();
 }
 

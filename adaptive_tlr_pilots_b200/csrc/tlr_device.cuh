@@ -162,8 +162,10 @@ __device__ __forceinline__ double block_max(double v, double* red) {
 // products, ||E||^2 = <dU^T dU, V^T V> + 2 <dU^T U~, V^T dV> + <U~^T U~, dV^T dV> (E = dU V^T +
 // U~ dV^T, dU = U - U~, dV = V - V~), whose terms are all of the size of the rounding error, so
 // nothing large cancels.  `red` needs 33 doubles of shared memory.
+// With forced in {8, 16, 32, 64} the search is skipped and that storage is used (replayed
+// decisions); forced <= 0 searches.
 __device__ inline int cta_round_pair(double* U, double* V, int mu, int mv, int r, int ld, double budget,
-                                     double* red) {
+                                     double* red, int forced = 0) {
   if (r == 0) return 64;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
   double mxu = 0.0, mxv = 0.0;
@@ -173,8 +175,8 @@ __device__ inline int cta_round_pair(double* U, double* V, int mu, int mv, int r
   }
   const double topu = block_max(mxu, red);
   const double topv = block_max(mxv, red);
-  int chosen = 64;
-  for (int p = 8; p <= 32; p *= 2) {
+  int chosen = forced > 0 ? forced : 64;
+  for (int p = 8; p <= 32 && forced <= 0; p *= 2) {
     // one warp per (c, d): the (c, d) entries of the six Gram products
     double part = 0.0;
     for (int e = warp; e < r * r; e += nwarp) {

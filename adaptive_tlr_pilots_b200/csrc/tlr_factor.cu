@@ -114,6 +114,7 @@ __global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int 
                                              const int* TLR_RESTRICT rank, int cap,
                                              const double* TLR_RESTRICT z, double* TLR_RESTRICT rhs,
                                              int round_store, double thr_abs, int* TLR_RESTRICT prec,
+                                             int* TLR_RESTRICT blog_trsm, int rmode,
                                              const int* TLR_RESTRICT status) {
   if (*status != 0) return;
   const int i = k + 1 + blockIdx.x;
@@ -192,8 +193,11 @@ __global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int 
   __syncthreads();
   if (round_store) {  // storage rule 'mixed': the factor tile rounded under the full budget (17:183-184)
     __shared__ double rred[40];
-    const int bits = cta_round_pair(Ut, Vt, bi, bk, r, b, thr_abs, rred);
-    if (tid == 0) prec[t] = bits;
+    const int bits = cta_round_pair(Ut, Vt, bi, bk, r, b, thr_abs, rred, rmode == kRankReplay ? blog_trsm[t] : 0);
+    if (tid == 0) {
+      prec[t] = bits;
+      if (rmode == kRankRecord) blog_trsm[t] = bits;
+    }
   }
   // W = V^T V (r x r) and t = V^T z_k
   const double* zk = z + (size_t)k * b;
@@ -313,8 +317,8 @@ __device__ void cta_atb(const double* A, int lda, const double* B, int ldb, int 
 __device__ int rc_general_pair(int bi, int bj, int b, int cap, int r1, int ri, int rj, const double* Uik,
                                const double* Ujk, const double* W, double* Uw, double* Vw, RcScratch& S,
                                double* sig, int* perm, int* iflag, double* red, int* rsel, int rule_fixed,
-                               double thr_rel, double thr_abs, int round_store, int* rlog_pp, int rmode,
-                               int* status) {
+                               double thr_rel, double thr_abs, int round_store, int* rlog_pp, int* blog_pp,
+                               int rmode, int* status) {
   const int tid = threadIdx.x, nt = blockDim.x;
   const int s = r1 + rj, ls = 2 * cap;
   const int ku = min(bi, s), kv = min(bj, s);
@@ -391,7 +395,10 @@ __device__ int rc_general_pair(int bi, int bj, int b, int cap, int r1, int ri, i
     }
   }
   __syncthreads();
-  if (round_store) cta_round_pair(Uw, Vw, bi, bj, rn, b, thr_abs - tail, red);
+  if (round_store) {
+    const int bits = cta_round_pair(Uw, Vw, bi, bj, rn, b, thr_abs - tail, red, rmode == kRankReplay ? *blog_pp : 0);
+    if (tid == 0 && rmode == kRankRecord) *blog_pp = bits;
+  }
   return rn;
 }
 
@@ -404,8 +411,9 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
                                                    double* TLR_RESTRICT V, int* TLR_RESTRICT rank, int cap,
                                                    int rule_fixed, double thr_rel, double thr_abs,
                                                    double* TLR_RESTRICT scratch, size_t slot_doubles,
-                                                   int* TLR_RESTRICT next_pair, int* TLR_RESTRICT rlog, int rmode,
-                                                   int general, int round_store, int* TLR_RESTRICT status) {
+                                                   int* TLR_RESTRICT next_pair, int* TLR_RESTRICT rlog,
+                                                   int* TLR_RESTRICT blog, int rmode, int general, int round_store,
+                                                   int* TLR_RESTRICT status) {
   if (*status != 0) return;
   const int mB = nB - k - 1;  // trailing tiles
   const long npairs = (long)mB * (mB - 1) / 2;  // every trailing pair (i, j), k < j < i
@@ -487,7 +495,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     if (general) {  // storage rule 'mixed': the reference's recompression as written
       const int rn = rc_general_pair(bi, bj, b, cap, r1, ri, rj, Uik, Ujk, S.W, U + (size_t)tij * b * cap,
                                      V + (size_t)tij * b * cap, S, sig, perm, &iflag, red, gsel, rule_fixed,
-                                     thr_rel, thr_abs, round_store, rlog + pp, rmode, status);
+                                     thr_rel, thr_abs, round_store, rlog + pp, blog + pp, rmode, status);
       if (rn < 0) return;
       if (tid == 0) {
         rank[tij] = rn;
@@ -717,17 +725,17 @@ int launch_diag_build(const double* xy, int n, int b, int k, double sigma2, doub
 
 int launch_trsm(const double* D, int n, int b, int k, int nB, double* U, double* V, double* Wd, double* Y,
                 const int* rank, int cap, const double* z, double* rhs, int round_store, double thr_abs, int* prec,
-                const int* status, cudaStream_t s) {
+                int* blog_trsm, int rmode, const int* status, cudaStream_t s) {
   if (nB - k - 1 <= 0) return 0;
   k_trsm<<<nB - k - 1, 256, 0, s>>>(D, n, b, k, nB, U, V, Wd, Y, rank, cap, z, rhs, round_store, thr_abs, prec,
-                                    status);
+                                    blog_trsm, rmode, status);
   return (int)cudaGetLastError();
 }
 
 int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, int rule_fixed,
                       double thr_rel, double thr_abs, double* scratch, size_t slot_doubles, int nslots,
-                      int* next_pair, int* rlog_step, int rmode, int general, int round_store, int* status,
-                      cudaStream_t s) {
+                      int* next_pair, int* rlog_step, int* blog_step, int rmode, int general, int round_store,
+                      int* status, cudaStream_t s) {
   const long mB = nB - k - 1;
   const long npairs = mB * (mB - 1) / 2;
   if (npairs <= 0) return 0;
@@ -735,7 +743,8 @@ int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* ra
   const size_t sm = (size_t)3 * kRcSmemS * kRcSmemS * 8;
   cudaFuncSetAttribute(k_recompress, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   k_recompress<<<grid, kRcT, sm, s>>>(n, b, k, nB, U, V, rank, cap, rule_fixed, thr_rel, thr_abs, scratch,
-                                     slot_doubles, next_pair, rlog_step, rmode, general, round_store, status);
+                                     slot_doubles, next_pair, rlog_step, blog_step, rmode, general, round_store,
+                                     status);
   return (int)cudaGetLastError();
 }
 

@@ -8,7 +8,8 @@ namespace tlr {
 
 // Rank map: every rank the rule picks (initial compression of tile t at rlog[t], recompression of
 // trailing pair p of step k at rlog[ntiles + off_k + p]) is recorded, or replayed instead of the
-// rule's choice (frozen ranks at another theta).
+// rule's choice (frozen ranks at another theta).  Under the storage rule 'mixed' the storage bits
+// of every rounding go to blog at the same positions, the panel solve's after them (blog[total + t]).
 constexpr int kRankOff = 0, kRankRecord = 1, kRankReplay = 2;
 
 // Morton order (codes/11_tlr_rank_rules.py:40-53): stable radix sort of the keys.  `work` holds
@@ -39,7 +40,8 @@ int launch_finalize(int n, int b, int k, int ldp, int cap, int margin, int rule_
                     double thr_abs, int tile_base, const int* ti, const int* tj, int* need, const double* P,
                     const double* C, const double* parts, const double* fparts, int nblk, double* gscratch,
                     double* gsv, double* U, double* V, int* rank, int last_level, int nchunk, int* rlog,
-                    int rmode, double* tail0, double* fro0, int round_store, int* status, cudaStream_t s);
+                    int rmode, double* tail0, double* fro0, int round_store, int* blog, int* status,
+                    cudaStream_t s);
 
 // factorization
 int launch_diag_build(const double* xy, int n, int b, int k, double sigma2, double inv_range, int nu5,
@@ -52,14 +54,14 @@ int launch_potrf_batched(double* D, int n, int b, int k, double* rhs, double* z,
                          int* status, int nbatch, size_t sD, size_t sV, int sS, cudaStream_t s);
 int launch_trsm(const double* D, int n, int b, int k, int nB, double* U, double* V, double* Wd, double* Y,
                 const int* rank, int cap, const double* z, double* rhs, int round_store, double thr_abs, int* prec,
-                const int* status, cudaStream_t s);
+                int* blog_trsm, int rmode, const int* status, cudaStream_t s);
 size_t rc_slot_doubles(int b, int cap);
 // every trailing pair of step k; next_pair: a counter that is zero at launch (the CTAs claim
 // pairs past the grid through it)
 int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, int rule_fixed,
                       double thr_rel, double thr_abs, double* scratch, size_t slot_doubles, int nslots,
-                      int* next_pair, int* rlog_step, int rmode, int general, int round_store, int* status,
-                      cudaStream_t s);
+                      int* next_pair, int* rlog_step, int* blog_step, int rmode, int general, int round_store,
+                      int* status, cudaStream_t s);
 // assembled-matrix rule: dense Sigma^TLR from the initial compression (N x N, leading dimension ldk)
 int launch_assemble(const double* xy, int n, int b, double sigma2, double inv_range, int nu5, double nugget,
                     const double* U, const double* V, const int* rank, int cap, double* K, long long ldk,

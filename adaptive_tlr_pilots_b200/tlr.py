@@ -289,6 +289,31 @@ class Plan:
         _lib.check(self.lib.tlr_plan_rank_map(self.handle, _lib.RANK_MAP[mode]))
         self.rank_mode = mode
 
+    def rank_map_get(self):
+        """(ranks, bits) of the plan's rank map (tlr_plan_rank_map_io): every recorded rank, and
+        under rule 'mixed' the storage bits of every rounding, then those of the panel solves."""
+        m = int(self.lib.tlr_plan_rank_map_size(self.handle))
+        ranks = np.zeros(max(m, 1), dtype=np.int32)
+        bits = np.zeros(max(m + self.ntiles, 1), dtype=np.int32)
+        ip = ctypes.POINTER(ctypes.c_int)
+        _lib.check(self.lib.tlr_plan_rank_map_io(self.handle, ranks.ctypes.data_as(ip), bits.ctypes.data_as(ip), m, 0))
+        return ranks[:m], bits[: m + self.ntiles]
+
+    def rank_map_set(self, ranks, bits=None):
+        """Load a rank map (and storage bits) for later rank_map('replay') evaluations."""
+        m = int(self.lib.tlr_plan_rank_map_size(self.handle))
+        r = np.ascontiguousarray(ranks, dtype=np.int32)
+        if r.shape != (m,):
+            raise ValueError(f"ranks must hold {m} values")
+        ip = ctypes.POINTER(ctypes.c_int)
+        bp = None
+        if bits is not None:
+            bb = np.ascontiguousarray(bits, dtype=np.int32)
+            if bb.shape != (m + self.ntiles,):
+                raise ValueError(f"bits must hold {m + self.ntiles} values")
+            bp = bb.ctypes.data_as(ip)
+        _lib.check(self.lib.tlr_plan_rank_map_io(self.handle, r.ctypes.data_as(ip), bp, m, 1))
+
     def set_profiling(self, on=True, kind=None):
         """Bracket every launch with CUDA events (per-kernel device time; results unchanged), or
         only the launches of one kernel kind (a key of kernel_stats) when `kind` is given."""

@@ -48,6 +48,11 @@ def parse():
     ap.add_argument("--dense", type=int, default=1, help="0: skip the dense FP64 oracle")
     ap.add_argument("--sim", choices=["dense", "tlr"], default="dense",
                     help="field from a dense Cholesky, or from a tau = 0.02 TLR factor (large N)")
+    ap.add_argument("--chains", type=int, default=0,
+                    help="> 0: instead of the headline, run this many lockstep random-walk chains (the 64-chain "
+                         "configuration) for --chain-iters iterations through --workspaces device workspaces")
+    ap.add_argument("--workspaces", type=int, default=8)
+    ap.add_argument("--chain-iters", type=int, default=3)
     return ap.parse_args()
 
 
@@ -176,8 +181,42 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+def run_chains_mode(a):
+    """Lockstep random-walk chains at the workload's size: every iteration is one batched call of
+    all chains' (loglik, gradient) through `workspaces` device workspaces (PlanBatch groups).
+    Starts: the reference's dispersed multipliers of theta_0 (README.md:582) cycled over the
+    chains; seeds 101, 102, ...; the prior box of codes/19_tlr_mcmc_gpu.py:23."""
+    import numpy as np
+    import torch
+
+    from adaptive_tlr_pilots_b200 import inference as I
+    from adaptive_tlr_pilots_b200 import synth
+    S, y, _, _ = synth.simulate_field(a.n, THETA, device=0)
+    mult = np.array([[1.3, 0.8, 1.5], [0.6, 1.4, 0.5], [2.0, 0.5, 2.0], [0.8, 1.2, 0.8]])
+    starts = np.log(np.array(THETA)[None, :] * mult[np.arange(a.chains) % 4])
+    obj = I.TLRObjective(S, y, a.b, "adaptive", a.tau, precision=a.precision, batch=a.chains,
+                         workspaces=a.workspaces)
+    obj.batch(starts[: min(a.chains, a.workspaces)])  # warm-up: one group
+    free_b, total_b = torch.cuda.mem_get_info(0)
+    torch.cuda.synchronize()
+    e0 = obj.evals
+    t0 = time.perf_counter()
+    out = I.run_chains(obj, starts, iters=a.chain_iters, burn=a.chain_iters, seeds=list(range(101, 101 + a.chains)))
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    evals = obj.evals - e0  # every chain's start, then the proposals inside the prior box
+    print(json.dumps({"mode": "chains", "config": dict(workload(a), chains=a.chains, workspaces=a.workspaces,
+                                                        iters=a.chain_iters, kind="rw"),
+                      "evals": evals, "seconds": dt, "evals_per_s": evals / dt,
+                      "acceptance": out["acceptance"], "failures": out["failures"],
+                      "device_used_gb": (total_b - free_b) / 1e9, "device_gb": total_b / 1e9}), flush=True)
+
+
 def main():
     a = parse()
+    if a.chains > 0:
+        run_chains_mode(a)
+        return
     if a.plain_steps < 0:
         a.plain_steps = a.steps * a.batch  # as many plain evaluations as batched ones
     if a.impl == "reference":

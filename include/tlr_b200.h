@@ -193,6 +193,15 @@ int tlr_factor_storage(tlr_plan* plan, int* bits, long long* stored_bytes);
 #define TLR_RANKS_REPLAY 2
 int tlr_plan_rank_map(tlr_plan* plan, int mode);
 
+/* The plan's rank map on the host, to keep frozen ranks across plans or processes: the number of
+ * recorded ranks (initial tiles, then every step's trailing pairs) is tlr_plan_rank_map_size(plan);
+ * ranks holds that many, bits (rule 'mixed': the storage bits chosen at each of those roundings,
+ * then at each panel solve, one per tile) that many plus nB (nB - 1) / 2.  upload = 0 copies the map
+ * out, 1 copies it in (a later TLR_RANKS_REPLAY evaluation uses it); either pointer may be NULL.
+ * No counterpart in the reference. */
+long long tlr_plan_rank_map_size(const tlr_plan* plan);
+int tlr_plan_rank_map_io(tlr_plan* plan, int* ranks, int* bits, long long count, int upload);
+
 /* Kernel kinds counted by tlr_plan_kernel_stats (launches issued by the plan's evaluations). */
 #define TLR_K_FILL 0
 #define TLR_K_GEN 1        /* off-diagonal tile generation */

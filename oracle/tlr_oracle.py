@@ -241,7 +241,9 @@ def tlr_cholesky(S, theta, bounds, rule, value, rank_log=None, frozen=None, on_s
     order of the reference (for k, for i > k).  codes/17_tlr_cholesky_pilot.py:137-215
     for rules 'fixed' and 'adaptive'.
 
-    rank_log: optional dict, filled with {('init', i, j): r, ('rc', k, i, j): r}.
+    rank_log: optional dict, filled with {('init', i, j): r, ('rc', k, i, j): r}, and under rule
+              'mixed' with the storage bits of every rounding: ('init_bits', i, j), ('trsm_bits', i, k),
+              ('rc_bits', k, i, j).
     frozen:   optional dict of the same form; its ranks replace the rule's choice.
     on_stage: optional callable, called with ("compress", i) after tile row i is generated and
               compressed and with ("factor", k) after factorization step k (for stage timings).
@@ -278,7 +280,9 @@ def tlr_cholesky(S, theta, bounds, rule, value, rank_log=None, frozen=None, on_s
             if rank_log is not None:
                 rank_log[("init", i, j)] = r
             if mixed:  # 17:163-164
-                U, V, _ = round_pair(U, V, thr_abs - tail)
+                U, V, bits = round_pair(U, V, thr_abs - tail)
+                if rank_log is not None:
+                    rank_log[("init_bits", i, j)] = bits
             A_off[(i, j)] = (U, V)
             stored0 += 2 * r * max(i1 - i0, j1 - j0)
         if on_stage is not None:
@@ -304,6 +308,8 @@ def tlr_cholesky(S, theta, bounds, rule, value, rank_log=None, frozen=None, on_s
                 V = solve_triangular(Lkk, V, lower=True, check_finite=False)
             if mixed:  # 17:183-184
                 U, V, prec[(i, k)] = round_pair(U, V, thr_abs)
+                if rank_log is not None:
+                    rank_log[("trsm_bits", i, k)] = prec[(i, k)]
             L_off[(i, k)] = (U, V)
         # trailing update A_ij -= L_ik L_jk^T with recompression: 17:186-205
         for i in range(k + 1, nB):
@@ -324,7 +330,9 @@ def tlr_cholesky(S, theta, bounds, rule, value, rank_log=None, frozen=None, on_s
                     if rank_log is not None:
                         rank_log[("rc", k, i, j)] = r
                     if mixed:  # 17:203-204
-                        Ur, Vr, _ = round_pair(Ur, Vr, thr_abs - tail)
+                        Ur, Vr, bits = round_pair(Ur, Vr, thr_abs - tail)
+                        if rank_log is not None:
+                            rank_log[("rc_bits", k, i, j)] = bits
                     A_off[(i, j)] = (Ur, Vr)
         if on_stage is not None:
             on_stage(("factor", k))

@@ -8,6 +8,12 @@ b = 250, theta = (1, 0.3, 0.05)), the module imported by file path as the refere
 Per case: log-likelihood, log-determinant, completion, factor ranks and the precision of every
 factor tile in the reference's L_off order, stored values and bytes, the precision mix.
 
+The rule is ill-conditioned in its inputs: a pair stored in FP16 turns a difference of 1e-13 in
+one factor entry into a jump of 2^-11 whenever the entry lies near a rounding boundary, and many
+of the rule's rank and storage decisions sit within a few percent of their budgets.  So every case
+also records the reference's own spread: the same rule on the sites multiplied by
+(1 + 1e-13 z), z standard normal, for eight seeds (log-likelihood, stored bytes, precision mix).
+
 Usage:  python tests/golden/make_golden_mixed_rule.py [--ref /root/reference]
 """
 import argparse
@@ -48,6 +54,16 @@ def main():
                        factor_prec=[int(tlr.PREC_OF[k]) for k in L_off.keys()])
         else:
             rec.update(failed_at=int(info["failed_at"]))
+        spread = []
+        for seed in range(8):
+            Sp = S * (1.0 + 1e-13 * np.random.default_rng(seed).standard_normal(S.shape))
+            llp, _, infop = tlr.tlr_loglik(Sp, y, theta, bounds, "mixed", tau)
+            spread.append(dict(seed=seed, completed=bool(infop["completed"]),
+                               loglik=None if llp is None else float(llp),
+                               stored_factor_bytes=int(infop.get("stored_factor_bytes", 0)),
+                               precision_mix_factor_tiles={str(k): int(v) for k, v in
+                                                           infop.get("precision_mix_factor_tiles", {}).items()}))
+        rec["perturbed_1e-13"] = spread
         out["cases"].append(rec)
         print(data, tau, rec.get("loglik"), rec.get("precision_mix_factor_tiles"), flush=True)
     json.dump(out, open(os.path.join(HERE, "golden_mixed_rule.json"), "w"), indent=1)
