@@ -41,6 +41,8 @@ constexpr int kPowerPassesMixed = 3;  // mixed path: the exact residual still bo
 // sweep case is within 5e-12), 8 in the mixed path, whose budget is 1e-2 nats
 constexpr int kMargin = 12;
 constexpr int kMarginMixed = 8;
+// block Gram-Schmidt passes of the recompression in the mixed path (2 in the FP64 parity path)
+constexpr int kGsPassesMixed = 1;
 
 }  // namespace
 
@@ -263,7 +265,9 @@ int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugge
     LAUNCH(TLR_K_RECOMPRESS, tlr::launch_recompress(p->n, p->b, k, p->nB, p->U, p->V, p->rank, p->cap, rule_fixed,
                                                     thr_rel, thr_abs, p->rcs, p->slot_doubles, p->nslots,
                                                     p->rc_next + k, p->rlog + p->rlog_off[k], p->blog + p->rlog_off[k], p->rmode,
-                                                    p->round_store, p->round_store, p->status, s));
+                                                    p->round_store, p->round_store,
+                                                    p->precision == TLR_PRECISION_MIXED ? kGsPassesMixed : 2,
+                                                    p->status, s));
     if (ahead) TRY(cuda_check(cudaStreamWaitEvent(s, p->ev_diag, 0), "wait"));
   }
   LAUNCH(TLR_K_FINISH, tlr::launch_finish(p->nB, p->n, p->ldpart, p->qpart, p->out, p->status, s));
