@@ -41,8 +41,6 @@ constexpr int kPowerPassesMixed = 3;  // mixed path: the exact residual still bo
 // sweep case is within 5e-12), 8 in the mixed path, whose budget is 1e-2 nats
 constexpr int kMargin = 12;
 constexpr int kMarginMixed = 8;
-// block Gram-Schmidt passes of the recompression in the mixed path (2 in the FP64 parity path)
-constexpr int kGsPassesMixed = 1;
 
 }  // namespace
 
@@ -266,7 +264,7 @@ int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugge
                                                     thr_rel, thr_abs, p->rcs, p->slot_doubles, p->nslots,
                                                     p->rc_next + k, p->rlog + p->rlog_off[k], p->blog + p->rlog_off[k], p->rmode,
                                                     p->round_store, p->round_store,
-                                                    p->precision == TLR_PRECISION_MIXED ? kGsPassesMixed : 2,
+                                                    p->precision == TLR_PRECISION_MIXED ? 1 : 0,
                                                     p->status, s));
     if (ahead) TRY(cuda_check(cudaStreamWaitEvent(s, p->ev_diag, 0), "wait"));
   }

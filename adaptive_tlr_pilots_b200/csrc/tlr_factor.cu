@@ -407,9 +407,10 @@ constexpr int kRcT = 256;     // threads per pair
 constexpr int kRcW = kRcT / 32;
 constexpr int kRcMinBlocks = 4;
 
-// kGs: block Gram-Schmidt passes against the existing factors (2 = with re-orthogonalisation, the
-// FP64 parity path; 1 in the mixed path, which also skips re-orthogonalising Q3 against V_ij)
-template <int kGs>
+// kMixed: the mixed path's core SVD stops rotating at |cos| <= 1e-10 (singular values to 1e-20
+// relative, vectors to 1e-10).  A single Gram-Schmidt pass was measured for that path too and
+// withdrawn: 0.024 nats and 2e-3 (gradient) from FP64 at N = 50,000, over the budget.
+template <bool kMixed>
 __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b, int k, int nB, double* TLR_RESTRICT U,
                                                    double* TLR_RESTRICT V, int* TLR_RESTRICT rank, int cap,
                                                    int rule_fixed, double thr_rel, double thr_abs,
@@ -517,7 +518,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
       }
     __syncthreads();
     // block Gram-Schmidt twice against Q1 = U_ij diag(1/n1): C = Q1^T X, X -= Q1 C
-    for (int pass = 0; pass < kGs; ++pass) {
+    for (int pass = 0; pass < 2; ++pass) {
       if (r1 > 0) {
         for (int e = warp; e < r1 * rj; e += kRcW) {
           const int u = e % r1, v = e / r1;
@@ -549,7 +550,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     for (int v = 0; v < rj; ++v)
       for (int a = tid; a < bj; a += kRcT) S.Y[(size_t)v * b + a] = Ujk[(size_t)v * b + a];
     __syncthreads();
-    for (int pass = 0; pass < kGs; ++pass) {
+    for (int pass = 0; pass < 2; ++pass) {
       if (r1 > 0) {
         cta_atb(Vij, b, S.Y, b, bj, r1, rj, S.G, cap);
         __syncthreads();
@@ -596,7 +597,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
       __syncthreads();
     }
     // re-orthogonalise Q3 against the normalised V_ij once
-    if (kGs > 1 && r1 > 0) {
+    if (r1 > 0) {
       cta_atb(Vij, b, S.Y, b, bj, r1, rj, S.G, cap);
       __syncthreads();
       for (int v = 0; v < rj; ++v)
@@ -627,7 +628,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     __syncthreads();
     // columns below 1e-14 of the largest singular value (the projections' rounding noise) are not
     // rotated: their relative orthogonality test would otherwise run to the sweep limit
-    cta_jacobi_svd(Zc, lc, s, s, Vc, lc, sig, perm, &iflag, 40, 1e-28);
+    cta_jacobi_svd(Zc, lc, s, s, Vc, lc, sig, perm, &iflag, 40, 1e-28, kMixed ? 1e-10 : 0.0);
     // Vc <- normalised Z (right singular vectors of M), in place of the rotation matrix
     for (int c = warp; c < s; c += kRcW) {
       const double inv = sig[c] > 0.0 ? 1.0 / sig[c] : 0.0;
@@ -738,22 +739,22 @@ int launch_trsm(const double* D, int n, int b, int k, int nB, double* U, double*
 int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, int rule_fixed,
                       double thr_rel, double thr_abs, double* scratch, size_t slot_doubles, int nslots,
                       int* next_pair, int* rlog_step, int* blog_step, int rmode, int general, int round_store,
-                      int gs_passes, int* status, cudaStream_t s) {
+                      int mixed, int* status, cudaStream_t s) {
   const long mB = nB - k - 1;
   const long npairs = mB * (mB - 1) / 2;
   if (npairs <= 0) return 0;
   const int grid = (int)std::min<long>(npairs, nslots);
   const size_t sm = (size_t)3 * kRcSmemS * kRcSmemS * 8;
-  if (gs_passes == 1) {
-    cudaFuncSetAttribute(k_recompress<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_recompress<1><<<grid, kRcT, sm, s>>>(n, b, k, nB, U, V, rank, cap, rule_fixed, thr_rel, thr_abs, scratch,
-                                          slot_doubles, next_pair, rlog_step, blog_step, rmode, general,
-                                          round_store, status);
+  if (mixed) {
+    cudaFuncSetAttribute(k_recompress<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_recompress<true><<<grid, kRcT, sm, s>>>(n, b, k, nB, U, V, rank, cap, rule_fixed, thr_rel, thr_abs, scratch,
+                                           slot_doubles, next_pair, rlog_step, blog_step, rmode, general,
+                                           round_store, status);
   } else {
-    cudaFuncSetAttribute(k_recompress<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_recompress<2><<<grid, kRcT, sm, s>>>(n, b, k, nB, U, V, rank, cap, rule_fixed, thr_rel, thr_abs, scratch,
-                                          slot_doubles, next_pair, rlog_step, blog_step, rmode, general,
-                                          round_store, status);
+    cudaFuncSetAttribute(k_recompress<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_recompress<false><<<grid, kRcT, sm, s>>>(n, b, k, nB, U, V, rank, cap, rule_fixed, thr_rel, thr_abs, scratch,
+                                           slot_doubles, next_pair, rlog_step, blog_step, rmode, general,
+                                           round_store, status);
   }
   return (int)cudaGetLastError();
 }
