@@ -263,9 +263,7 @@ int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugge
     LAUNCH(TLR_K_RECOMPRESS, tlr::launch_recompress(p->n, p->b, k, p->nB, p->U, p->V, p->rank, p->cap, rule_fixed,
                                                     thr_rel, thr_abs, p->rcs, p->slot_doubles, p->nslots,
                                                     p->rc_next + k, p->rlog + p->rlog_off[k], p->blog + p->rlog_off[k], p->rmode,
-                                                    p->round_store, p->round_store,
-                                                    p->precision == TLR_PRECISION_MIXED ? 1 : 0,
-                                                    p->status, s));
+                                                    p->round_store, p->round_store, p->status, s));
     if (ahead) TRY(cuda_check(cudaStreamWaitEvent(s, p->ev_diag, 0), "wait"));
   }
   LAUNCH(TLR_K_FINISH, tlr::launch_finish(p->nB, p->n, p->ldpart, p->qpart, p->out, p->status, s));

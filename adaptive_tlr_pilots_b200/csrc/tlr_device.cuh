@@ -312,8 +312,7 @@ __device__ inline void cta_org2r(double* A, int lda, int m, int n, const double*
 // (from cores assembled out of Gram matrices) would otherwise keep the relative test of their
 // pairs failing forever.
 __device__ inline int cta_jacobi_svd(double* M, int ldm, int m, int n, double* V, int ldv, double* sig,
-                                     int* perm, int* iflag, int max_sweeps = 40, double floor_rel = 0.0,
-                                     double tol_in = 0.0) {
+                                     int* perm, int* iflag, int max_sweeps = 40, double floor_rel = 0.0) {
   __shared__ double s_floor2;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   for (int j = warp; j < n; j += nwarp)
@@ -321,9 +320,7 @@ __device__ inline int cta_jacobi_svd(double* M, int ldm, int m, int n, double* V
   const int np = (n + 1) & ~1;  // even number of players (one dummy when n is odd)
   // rotate unless the pair is orthogonal to working precision, |cos| <= m eps (the singular
   // values then carry a relative error of order cos^2)
-  // (tol_in > 0: a looser test; the singular values then carry a relative error of order tol_in^2
-  // and the vectors of order tol_in)
-  const double tol = tol_in > 0.0 ? tol_in : (double)(m > 4 ? m : 4) * 2.220446049250313e-16;
+  const double tol = (double)(m > 4 ? m : 4) * 2.220446049250313e-16;
   const double tol2 = tol * tol;
   int sweep = 0;
   if (n > 1) {

@@ -402,15 +402,17 @@ __device__ int rc_general_pair(int bi, int bj, int b, int cap, int r1, int ri, i
   return rn;
 }
 
+// The mixed path uses this kernel as it stands.  Three ways of making it cheaper there were measured
+// on the N = 50,000 bench workload and withdrawn: one Gram-Schmidt pass without re-orthogonalising
+// Q3 (5.53 against 5.09 evals/s, but 0.024 nats and 2e-3 of the gradient from FP64, over the
+// budget), a core Jacobi that stops at |cos| <= 1e-10 (no faster, 0.0079 nats, over budget on three
+// N = 20,000 sweep fields), and 128-thread CTAs at 6 or 8 per SM (recompression 279 / 318 ms
+// against 175 ms per evaluation).
 constexpr int kRcSmemS = 32;  // cores with s <= 32 are solved in shared memory
 constexpr int kRcT = 256;     // threads per pair
 constexpr int kRcW = kRcT / 32;
 constexpr int kRcMinBlocks = 4;
 
-// kMixed: the mixed path's core SVD stops rotating at |cos| <= 1e-10 (singular values to 1e-20
-// relative, vectors to 1e-10).  A single Gram-Schmidt pass was measured for that path too and
-// withdrawn: 0.024 nats and 2e-3 (gradient) from FP64 at N = 50,000, over the budget.
-template <bool kMixed>
 __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b, int k, int nB, double* TLR_RESTRICT U,
                                                    double* TLR_RESTRICT V, int* TLR_RESTRICT rank, int cap,
                                                    int rule_fixed, double thr_rel, double thr_abs,
@@ -628,7 +630,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     __syncthreads();
     // columns below 1e-14 of the largest singular value (the projections' rounding noise) are not
     // rotated: their relative orthogonality test would otherwise run to the sweep limit
-    cta_jacobi_svd(Zc, lc, s, s, Vc, lc, sig, perm, &iflag, 40, 1e-28, kMixed ? 1e-10 : 0.0);
+    cta_jacobi_svd(Zc, lc, s, s, Vc, lc, sig, perm, &iflag, 40, 1e-28);
     // Vc <- normalised Z (right singular vectors of M), in place of the rotation matrix
     for (int c = warp; c < s; c += kRcW) {
       const double inv = sig[c] > 0.0 ? 1.0 / sig[c] : 0.0;
@@ -739,23 +741,16 @@ int launch_trsm(const double* D, int n, int b, int k, int nB, double* U, double*
 int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, int rule_fixed,
                       double thr_rel, double thr_abs, double* scratch, size_t slot_doubles, int nslots,
                       int* next_pair, int* rlog_step, int* blog_step, int rmode, int general, int round_store,
-                      int mixed, int* status, cudaStream_t s) {
+                      int* status, cudaStream_t s) {
   const long mB = nB - k - 1;
   const long npairs = mB * (mB - 1) / 2;
   if (npairs <= 0) return 0;
   const int grid = (int)std::min<long>(npairs, nslots);
   const size_t sm = (size_t)3 * kRcSmemS * kRcSmemS * 8;
-  if (mixed) {
-    cudaFuncSetAttribute(k_recompress<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_recompress<true><<<grid, kRcT, sm, s>>>(n, b, k, nB, U, V, rank, cap, rule_fixed, thr_rel, thr_abs, scratch,
-                                           slot_doubles, next_pair, rlog_step, blog_step, rmode, general,
-                                           round_store, status);
-  } else {
-    cudaFuncSetAttribute(k_recompress<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_recompress<false><<<grid, kRcT, sm, s>>>(n, b, k, nB, U, V, rank, cap, rule_fixed, thr_rel, thr_abs, scratch,
-                                           slot_doubles, next_pair, rlog_step, blog_step, rmode, general,
-                                           round_store, status);
-  }
+  cudaFuncSetAttribute(k_recompress, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_recompress<<<grid, kRcT, sm, s>>>(n, b, k, nB, U, V, rank, cap, rule_fixed, thr_rel, thr_abs, scratch,
+                                     slot_doubles, next_pair, rlog_step, blog_step, rmode, general, round_store,
+                                     status);
   return (int)cudaGetLastError();
 }
 

@@ -61,7 +61,7 @@ size_t rc_slot_doubles(int b, int cap);
 int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, int rule_fixed,
                       double thr_rel, double thr_abs, double* scratch, size_t slot_doubles, int nslots,
                       int* next_pair, int* rlog_step, int* blog_step, int rmode, int general, int round_store,
-                      int mixed, int* status, cudaStream_t s);
+                      int* status, cudaStream_t s);
 // assembled-matrix rule: dense Sigma^TLR from the initial compression (N x N, leading dimension ldk)
 int launch_assemble(const double* xy, int n, int b, double sigma2, double inv_range, int nu5, double nugget,
                     const double* U, const double* V, const int* rank, int cap, double* K, long long ldk,
