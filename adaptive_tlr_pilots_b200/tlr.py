@@ -384,8 +384,8 @@ class PlanBatch:
     latency-bound factorization steps.  The batch of MCMC chains or optimizer restarts of one
     iteration.
 
-    `workspaces` (default: count, at most count) is the number of device workspaces (plans, one
-    stream each) that run at once; with fewer workspaces than parameter vectors the vectors go
+    `workspaces` (default: count, at most count; "auto": the autotuner's measured best) is the
+    number of device workspaces (plans, one stream each) that run at once; with fewer workspaces than parameter vectors the vectors go
     through them in consecutive groups, so memory is workspaces x (one plan) whatever the count
     (at N = 50,000, b = 500 a plan holds about 10 GB: 64 chains through 8 workspaces fit one
     B200)."""
@@ -393,6 +393,9 @@ class PlanBatch:
     def __init__(self, n, b, count, cap=64, device=0, precision="mixed", workspaces=None):
         torch = _torch()
         self.n, self.b, self.count, self.device = int(n), int(b), int(count), int(device)
+        if workspaces == "auto":  # the autotuner's table (adaptive_tlr_pilots_b200/autotune.py)
+            from .autotune import best_workspaces
+            workspaces = best_workspaces(self.n, self.b, self.count, precision=precision)
         self.workspaces = self.count if workspaces is None else max(1, min(int(workspaces), self.count))
         self.lib = _lib.load()
         self.streams = [torch.cuda.Stream(device=self.device) for _ in range(self.workspaces)]

@@ -130,3 +130,24 @@ def test_split_rhat_ess_matches_direct_sums_and_ar1_theory():
     assert abs(rh - rh_d) < 1e-12 and abs(ess - ess_d) < 1e-8 * ess_d
     # AR(1): integrated autocorrelation time (1 + phi) / (1 - phi) = 9
     assert 0.75 < ess / (M * n / 9.0) < 1.3
+
+
+def test_autotune_table_lookup(tmp_path):
+    """best_workspaces takes the fastest measured count for the nearest tuned N with the same tile
+    size, rule and precision, capped at the batch; the default without a matching entry."""
+    import json as _json
+
+    from adaptive_tlr_pilots_b200 import autotune as A
+    path = str(tmp_path / "t.json")
+    assert A.best_workspaces(50000, 500, 64, path=path) == A.DEFAULT_WORKSPACES
+    table = {"a": dict(n=50000, b=500, rule="adaptive", value=0.9, precision="mixed", best=6,
+                       evals_per_s={"4": 5.0, "6": 6.0}),
+             "b": dict(n=20000, b=500, rule="adaptive", value=0.9, precision="mixed", best=2,
+                       evals_per_s={"2": 9.0}),
+             "c": dict(n=50000, b=250, rule="adaptive", value=0.9, precision="mixed", best=8,
+                       evals_per_s={"8": 1.0})}
+    _json.dump(table, open(path, "w"))
+    assert A.best_workspaces(60000, 500, 64, path=path) == 6
+    assert A.best_workspaces(18000, 500, 64, path=path) == 2
+    assert A.best_workspaces(50000, 500, 3, path=path) == 3
+    assert A.best_workspaces(50000, 500, 64, precision="fp64", path=path) == A.DEFAULT_WORKSPACES
