@@ -91,6 +91,7 @@ SIGNATURES = {
                                           ctypes.POINTER(TlrTileStats), ctypes.POINTER(ctypes.c_int)]),
     "tlr_plan_set_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "tlr_plan_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tlr_plan_set_graphs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tlr_plan_kernel_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int]),

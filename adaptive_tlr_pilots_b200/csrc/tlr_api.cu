@@ -130,6 +130,12 @@ struct tlr_plan {
   size_t d_split_cap = 0;
   tlr::TcOperands* d_tcops = nullptr;
   size_t d_tcops_cap = 0;
+  // forward pass (compression, factorization, solve) captured once per precision in a CUDA graph
+  // on a private stream and replayed on `stream`; the launch sequence depends only on the plan
+  bool use_graphs = true;
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t fwd_exec[2] = {nullptr, nullptr};
+  long long fwd_launch[2][TLR_NKINDS] = {};
 };
 
 namespace {
@@ -198,14 +204,14 @@ cudaEvent_t next_event(tlr_plan* p) {
   } while (0)
 #define LAUNCH(kind, x) LAUNCH_ON(p->stream, kind, x)
 
-int run_compression(tlr_plan* p, double sigma2, double inv_range, int rule_fixed, double thr_rel,
-                    double thr_abs) {
+// The kernels read theta, the rule and the thresholds from the EvalParams of the control block.
+int run_compression(tlr_plan* p) {
   cudaStream_t s = p->stream;
   const int ldp = kMaxK;
   for (int base = 0; base < p->ntiles; base += p->chunk) {
     const int nc = std::min(p->chunk, p->ntiles - base);
     LAUNCH(TLR_K_FILL, tlr::launch_fill_int(p->need, 1, nc, s));
-    LAUNCH(TLR_K_GEN, tlr::launch_gen_offdiag(p->xy, p->n, p->b, base, p->ti, p->tj, p->T, nc, sigma2, inv_range, p->nu5, p->status, s));
+    LAUNCH(TLR_K_GEN, tlr::launch_gen_offdiag(p->xy, p->n, p->b, base, p->ti, p->tj, p->T, nc, p->status, s));
     for (int lev = 0; lev < kLevels; ++lev) {
       const int k = 16 << lev;
       double* Pp = p->P;
@@ -228,46 +234,114 @@ int run_compression(tlr_plan* p, double sigma2, double inv_range, int rule_fixed
                                               p->fparts, p->nblk, nc, p->status, s));
       }
       LAUNCH(TLR_K_FINALIZE, tlr::launch_finalize(p->n, p->b, k, ldp, p->cap,
-                                p->precision == TLR_PRECISION_MIXED ? kMarginMixed : kMargin, rule_fixed, thr_rel, thr_abs, base, p->ti,
-                                p->tj, p->need, Pp, p->C, p->parts, p->fparts, fused ? 1 : p->nblk, p->gscr, p->gsv, p->U,
-                                p->V, p->rank, lev == kLevels - 1 ? 1 : 0, nc, p->rlog, p->rmode, p->tail0, p->fro0,
-                                p->round_store, p->blog, p->status, s));
+                                p->precision == TLR_PRECISION_MIXED ? kMarginMixed : kMargin, base, p->ti, p->tj,
+                                p->need, Pp, p->C, p->parts, p->fparts, fused ? 1 : p->nblk, p->gscr, p->gsv, p->U, p->V,
+                                p->rank, lev == kLevels - 1 ? 1 : 0, nc, p->rlog, p->tail0, p->fro0, p->blog, p->status,
+                                s));
     }
   }
   return 0;
 }
 
-int run_factorization(tlr_plan* p, double sigma2, double inv_range, double nugget, int rule_fixed, double thr_rel,
-                      double thr_abs) {
+int run_factorization(tlr_plan* p) {
   cudaStream_t s = p->stream, sd = p->side;
   TRY(cuda_check(cudaMemsetAsync(p->rc_next, 0, sizeof(int) * p->nB, s), "pair counters"));
-  LAUNCH(TLR_K_DIAG, tlr::launch_diag_build(p->xy, p->n, p->b, 0, sigma2, inv_range, p->nu5, nugget, p->U, p->Yd, p->rank,
-                                            p->cap, p->D, p->status, s));
+  LAUNCH(TLR_K_DIAG, tlr::launch_diag_build(p->xy, p->n, p->b, 0, p->U, p->Yd, p->rank, p->cap, p->D, p->status, s));
   LAUNCH(TLR_K_POTRF, tlr::launch_potrf(p->D, p->n, p->b, 0, p->rhs, p->z, p->ldpart, p->qpart, p->status, s));
   for (int k = 0; k < p->nB; ++k) {
     LAUNCH(TLR_K_TRSM, tlr::launch_trsm(p->D, p->n, p->b, k, p->nB, p->U, p->V, p->Wd, p->Yd, p->rank, p->cap, p->z, p->rhs,
-                                        p->round_store, thr_abs, p->prec, p->blog + p->rlog_off[p->nB], p->rmode,
-                                        p->status, s));
+                                        p->prec, p->blog + p->rlog_off[p->nB], p->status, s));
     const bool ahead = k + 1 < p->nB;
     if (ahead) {
       // A_{k+1,k+1} needs only the panels m <= k, all final once the panel solve of step k is
       // done; step k's recompression touches tiles (i, j) with j > k + 1 only.
       TRY(cuda_check(cudaEventRecord(p->ev_panel, s), "event"));
       TRY(cuda_check(cudaStreamWaitEvent(sd, p->ev_panel, 0), "wait"));
-      LAUNCH_ON(sd, TLR_K_DIAG, tlr::launch_diag_build(p->xy, p->n, p->b, k + 1, sigma2, inv_range, p->nu5, nugget, p->U,
-                                                       p->Yd, p->rank, p->cap, p->D, p->status, sd));
+      LAUNCH_ON(sd, TLR_K_DIAG, tlr::launch_diag_build(p->xy, p->n, p->b, k + 1, p->U, p->Yd, p->rank, p->cap,
+                                                       p->D, p->status, sd));
       LAUNCH_ON(sd, TLR_K_POTRF, tlr::launch_potrf(p->D, p->n, p->b, k + 1, p->rhs, p->z, p->ldpart, p->qpart,
                                                    p->status, sd));
       TRY(cuda_check(cudaEventRecord(p->ev_diag, sd), "event"));
     }
-    LAUNCH(TLR_K_RECOMPRESS, tlr::launch_recompress(p->n, p->b, k, p->nB, p->U, p->V, p->rank, p->cap, rule_fixed,
-                                                    thr_rel, thr_abs, p->rcs, p->slot_doubles, p->nslots,
-                                                    p->rc_next + k, p->rlog + p->rlog_off[k], p->blog + p->rlog_off[k], p->rmode,
-                                                    p->round_store, p->round_store, p->status, s));
+    LAUNCH(TLR_K_RECOMPRESS, tlr::launch_recompress(p->n, p->b, k, p->nB, p->U, p->V, p->rank, p->cap, p->rcs,
+                                                    p->slot_doubles, p->nslots, p->rc_next + k,
+                                                    p->rlog + p->rlog_off[k], p->blog + p->rlog_off[k], p->status, s));
     if (ahead) TRY(cuda_check(cudaStreamWaitEvent(s, p->ev_diag, 0), "wait"));
   }
   LAUNCH(TLR_K_FINISH, tlr::launch_finish(p->nB, p->n, p->ldpart, p->qpart, p->out, p->status, s));
   return 0;
+}
+
+// The forward pass after launch_set_params: ranks cleared, right-hand side, compression (the
+// initial ranks kept in rank0), factorization with the fused forward solve.
+int forward_sequence(tlr_plan* p) {
+  cudaStream_t s = p->stream;
+  TRY(cuda_check(cudaMemsetAsync(p->rank, 0, sizeof(int) * std::max(p->ntiles, 1), s), "reset ranks"));
+  TRY(cuda_check(cudaMemcpyAsync(p->rhs, p->y, sizeof(double) * p->n, cudaMemcpyDeviceToDevice, s), "rhs"));
+  TRY(run_compression(p));
+  if (p->ntiles > 0)
+    TRY(cuda_check(cudaMemcpyAsync(p->rank0, p->rank, sizeof(int) * p->ntiles, cudaMemcpyDeviceToDevice, s),
+                   "rank0"));
+  TRY(run_factorization(p));
+  return 0;
+}
+
+// Capture forward_sequence on the plan's private stream (nothing runs) and instantiate it.  The
+// launches counted during the capture become the graph's per-replay counts.
+int capture_forward(tlr_plan* p, int g) {
+  if (!p->cap_stream)
+    TRY(cuda_check(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking), "capture stream"));
+  long long before[TLR_NKINDS];
+  std::memcpy(before, p->klaunch, sizeof(before));
+  cudaStream_t user = p->stream;
+  p->stream = p->cap_stream;
+  int rc = cuda_check(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeRelaxed), "begin capture");
+  if (!rc) {
+    rc = forward_sequence(p);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(p->cap_stream, &graph);
+    if (!rc && e != cudaSuccess) rc = cuda_check(e, "end capture");
+    if (!rc) rc = cuda_check(cudaGraphInstantiate(&p->fwd_exec[g], graph, 0), "instantiate forward graph");
+    if (graph) cudaGraphDestroy(graph);
+  }
+  p->stream = user;
+  for (int i = 0; i < TLR_NKINDS; ++i) {
+    p->fwd_launch[g][i] = p->klaunch[i] - before[i];
+    p->klaunch[i] = before[i];
+  }
+  if (rc) {
+    cudaGetLastError();
+    p->fwd_exec[g] = nullptr;
+  }
+  return rc;
+}
+
+// One forward pass on the plan's stream: the captured graph of the plan's precision (captured on
+// first use), or the launches themselves while per-kernel event timing is on or graphs are off.
+int run_forward(tlr_plan* p) {
+  if (!p->use_graphs || p->prof) return forward_sequence(p);
+  const int g = p->precision == TLR_PRECISION_MIXED ? 1 : 0;
+  if (!p->fwd_exec[g]) TRY(capture_forward(p, g));
+  TRY(cuda_check(cudaGraphLaunch(p->fwd_exec[g], p->stream), "forward graph launch"));
+  for (int i = 0; i < TLR_NKINDS; ++i) p->klaunch[i] += p->fwd_launch[g][i];
+  return 0;
+}
+
+// The evaluation's parameters (thresholds: codes/17_tlr_cholesky_pilot.py:143-150 and
+// codes/11_tlr_rank_rules.py:81-98, emax = tau b m_theta / N with b the largest tile).
+tlr::EvalParams make_params(const tlr_plan* p, const double theta[3], int rule, double value) {
+  tlr::EvalParams prm{};
+  const double sigma2 = theta[0], range = theta[1], eta = theta[2];
+  prm.sigma2 = sigma2;
+  prm.inv_range = 1.0 / range;
+  prm.nugget = sigma2 * eta;
+  prm.rule_fixed = rule == TLR_RULE_FIXED ? 1 : 0;
+  prm.thr_rel = prm.rule_fixed ? value : 0.0;
+  prm.thr_abs = prm.rule_fixed ? 0.0 : value * (double)std::min(p->b, p->n) * sigma2 * eta / (double)p->n;
+  prm.rmode = p->rmode;
+  prm.round_store = rule == TLR_RULE_MIXED ? 1 : 0;
+  prm.nu5 = p->nu5;
+  return prm;
 }
 
 }  // namespace
@@ -663,7 +737,7 @@ int tlr_plan_create(tlr_plan** plan, int n, int b, int cap, int device, void* st
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
   p->nsm = nsm;
-  p->nslots = nsm * 4;  // resident recompression CTAs (k_recompress: four per SM)
+  p->nslots = nsm * tlr::rc_blocks_per_sm();  // resident recompression CTAs
   p->slot_doubles = tlr::rc_slot_doubles(b, cap);
   A(dalloc(p, &p->rcs, (size_t)p->nslots * p->slot_doubles));
   A(dalloc(p, &p->rc_next, (size_t)p->nB));
@@ -689,8 +763,8 @@ int tlr_plan_create(tlr_plan** plan, int n, int b, int cap, int device, void* st
   A(dalloc(p, &p->ldpart, (size_t)p->nB));
   A(dalloc(p, &p->qpart, (size_t)p->nB));
   A(dalloc(p, &p->out, 4));
-  // control block: status, padding, [flops, bytes] per kernel kind
-  A(dalloc(p, &p->status, 4 + 4 * TLR_NKINDS));
+  // control block: status, padding, [flops, bytes] per kernel kind, the evaluation's parameters
+  A(dalloc(p, &p->status, (tlr::kControlBytes + sizeof(int) - 1) / sizeof(int)));
   if (rc != 0) {
     free_all(p);
     delete p;
@@ -740,6 +814,9 @@ void tlr_plan_destroy(tlr_plan* plan) {
   if (plan->ev_panel) cudaEventDestroy(plan->ev_panel);
   if (plan->ev_diag) cudaEventDestroy(plan->ev_diag);
   if (plan->side) cudaStreamDestroy(plan->side);
+  for (cudaGraphExec_t g : plan->fwd_exec)
+    if (g) cudaGraphExecDestroy(g);
+  if (plan->cap_stream) cudaStreamDestroy(plan->cap_stream);
   if (plan->h_rank) cudaFreeHost(plan->h_rank);
   if (plan->h_rank0) cudaFreeHost(plan->h_rank0);
   if (plan->hb) cudaFreeHost(plan->hb);
@@ -843,18 +920,8 @@ int enqueue_forward(tlr_plan* p, const double theta[3], int rule, double value) 
   p->factor_ok = false;
   // rule 'mixed' (17:145-148): the adaptive thresholds, every stored factor pair rounded
   p->round_store = rule == TLR_RULE_MIXED ? 1 : 0;
-  // thresholds: codes/17_tlr_cholesky_pilot.py:143-150 (b = largest tile = b)
-  const int rule_fixed = rule == TLR_RULE_FIXED;
-  const double thr_rel = rule_fixed ? value : 0.0;
-  const double thr_abs = rule_fixed ? 0.0 : value * (double)std::min(p->b, p->n) * sigma2 * eta / (double)p->n;
-  TRY(cuda_check(cudaMemsetAsync(p->status, 0, sizeof(int) * (4 + 4 * TLR_NKINDS), s), "reset status"));
-  TRY(cuda_check(cudaMemsetAsync(p->rank, 0, sizeof(int) * std::max(p->ntiles, 1), s), "reset ranks"));
-  TRY(cuda_check(cudaMemcpyAsync(p->rhs, p->y, sizeof(double) * p->n, cudaMemcpyDeviceToDevice, s), "rhs"));
-  TRY(run_compression(p, sigma2, 1.0 / range, rule_fixed, thr_rel, thr_abs));
-  if (p->ntiles > 0)
-    TRY(cuda_check(cudaMemcpyAsync(p->rank0, p->rank, sizeof(int) * p->ntiles, cudaMemcpyDeviceToDevice, s),
-                   "rank0"));
-  TRY(run_factorization(p, sigma2, 1.0 / range, sigma2 * eta, rule_fixed, thr_rel, thr_abs));
+  LAUNCH(TLR_K_FILL, tlr::launch_set_params(p->status, make_params(p, theta, rule, value), s));
+  TRY(run_forward(p));
   TRY(cuda_check(cudaMemcpyAsync(&p->hb->status, p->status, sizeof(int), cudaMemcpyDeviceToHost, s), "status"));
   TRY(cuda_check(cudaMemcpyAsync(p->hb->out, p->out, sizeof(double) * 3, cudaMemcpyDeviceToHost, s), "out"));
   TRY(cuda_check(cudaMemcpyAsync(p->hb->work, p->status + 4, sizeof(double) * 2 * TLR_NKINDS,
@@ -976,13 +1043,9 @@ int tlr_truncate_tiles(tlr_plan* p, const double theta[3], int rule, double valu
   TRY(cuda_check(cudaSetDevice(p->device), "cudaSetDevice"));
   cudaStream_t s = p->stream;
   p->factor_ok = false;
-  // thresholds: codes/11_tlr_rank_rules.py:81-98 (emax = tau * b * m_theta / N, b the largest tile)
-  const int rule_fixed = rule == TLR_RULE_FIXED;
-  const double thr_rel = rule_fixed ? value : 0.0;
-  const double thr_abs = rule_fixed ? 0.0 : value * (double)std::min(p->b, p->n) * sigma2 * eta / (double)p->n;
-  TRY(cuda_check(cudaMemsetAsync(p->status, 0, sizeof(int) * (4 + 4 * TLR_NKINDS), s), "reset status"));
+  LAUNCH(TLR_K_FILL, tlr::launch_set_params(p->status, make_params(p, theta, rule, value), s));
   TRY(cuda_check(cudaMemsetAsync(p->rank, 0, sizeof(int) * std::max(p->ntiles, 1), s), "reset ranks"));
-  TRY(run_compression(p, sigma2, 1.0 / range, rule_fixed, thr_rel, thr_abs));
+  TRY(run_compression(p));
   if (K_dev)
     LAUNCH(TLR_K_GEN, tlr::launch_assemble(p->xy, p->n, p->b, sigma2, 1.0 / range, p->nu5, sigma2 * eta, p->U, p->V,
                                            p->rank, p->cap, K_dev, ldk, p->status, s));
@@ -1192,6 +1255,12 @@ int tlr_plan_set_profiling(tlr_plan* p, int on) {
   if (!p) return fail(TLR_ERR_ARG, "plan is NULL");
   p->prof = on != 0;
   p->prof_kind = on < 0 ? -on - 1 : -1;  // on < 0: only the launches of kind -on - 1
+  return 0;
+}
+
+int tlr_plan_set_graphs(tlr_plan* p, int on) {
+  if (!p) return fail(TLR_ERR_ARG, "plan is NULL");
+  p->use_graphs = on != 0;
   return 0;
 }
 

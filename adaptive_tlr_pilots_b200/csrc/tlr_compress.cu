@@ -34,8 +34,11 @@ __device__ __forceinline__ double omega_entry(uint32_t tile, uint32_t row, uint3
 // T[c] = sigma2 * matern32(dist(S_i, S_j)), row-major with leading dimension b.
 __global__ void k_gen_offdiag(const double* TLR_RESTRICT xy, int n, int b, int tile_base,
                               const int* TLR_RESTRICT ti, const int* TLR_RESTRICT tj, double* TLR_RESTRICT T,
-                              double sigma2, double inv_range, int nu5, const int* TLR_RESTRICT status) {
+                              const int* TLR_RESTRICT status) {
   if (*status != 0) return;
+  const EvalParams& prm = *eval_params(status);
+  const double sigma2 = prm.sigma2, inv_range = prm.inv_range;
+  const int nu5 = prm.nu5;
   const int c = blockIdx.y;
   const int t = (tile_base + c);
   const int i = ti[t], j = tj[t];
@@ -630,7 +633,6 @@ __global__ void __launch_bounds__(256) k_resid(const double* TLR_RESTRICT T, int
 // ----------------------------------------------------------------------------------------
 // Rank decision and output of the truncated pair for every tile still in need.
 __global__ void __launch_bounds__(1024) k_finalize(int n, int b, int k, int ldp, int cap, int margin,
-                                                 int rule_fixed, double thr_rel, double thr_abs,
                                                  int tile_base, const int* TLR_RESTRICT ti,
                                                  const int* TLR_RESTRICT tj, int* TLR_RESTRICT need,
                                                  const double* TLR_RESTRICT P, const double* TLR_RESTRICT C,
@@ -640,10 +642,12 @@ __global__ void __launch_bounds__(1024) k_finalize(int n, int b, int k, int ldp,
                                                  double* TLR_RESTRICT Uo,
                                                  double* TLR_RESTRICT Vo, int* TLR_RESTRICT rank,
                                                  int last_level, int w_in_smem, int* TLR_RESTRICT rlog,
-                                                 int rmode, double* TLR_RESTRICT tail0, double* TLR_RESTRICT fro0,
-                                                 int round_store, int* TLR_RESTRICT blog,
-                                                 int* TLR_RESTRICT status) {
+                                                 double* TLR_RESTRICT tail0, double* TLR_RESTRICT fro0,
+                                                 int* TLR_RESTRICT blog, int* TLR_RESTRICT status) {
   if (*status != 0) return;
+  const EvalParams& prm = *eval_params(status);
+  const int rule_fixed = prm.rule_fixed, rmode = prm.rmode, round_store = prm.round_store;
+  const double thr_rel = prm.thr_rel, thr_abs = prm.thr_abs;
   const int c = blockIdx.x;
   if (!need[c]) return;
   const int t = (tile_base + c);
@@ -734,10 +738,9 @@ __global__ void __launch_bounds__(1024) k_finalize(int n, int b, int k, int ldp,
 // ----------------------------------------------------------------------------------------
 // launchers
 int launch_gen_offdiag(const double* xy, int n, int b, int tile_base, const int* ti, const int* tj,
-                       double* T, int nchunk, double sigma2, double inv_range, int nu5, const int* status,
-                       cudaStream_t s) {
+                       double* T, int nchunk, const int* status, cudaStream_t s) {
   dim3 grid((unsigned)((b * b + 1023) / 1024), (unsigned)nchunk);
-  k_gen_offdiag<<<grid, 256, 0, s>>>(xy, n, b, tile_base, ti, tj, T, sigma2, inv_range, nu5, status);
+  k_gen_offdiag<<<grid, 256, 0, s>>>(xy, n, b, tile_base, ti, tj, T, status);
   return (int)cudaGetLastError();
 }
 
@@ -813,19 +816,17 @@ int launch_resid(const double* T, int n, int b, int k, int ldp, int tile_base, c
   return (int)cudaGetLastError();
 }
 
-int launch_finalize(int n, int b, int k, int ldp, int cap, int margin, int rule_fixed, double thr_rel,
-                    double thr_abs, int tile_base, const int* ti, const int* tj, int* need, const double* P,
-                    const double* C, const double* parts, const double* fparts, int nblk, double* gscratch,
-                    double* gsv, double* U, double* V, int* rank, int last_level, int nchunk, int* rlog,
-                    int rmode, double* tail0, double* fro0, int round_store, int* blog, int* status,
-                    cudaStream_t s) {
+int launch_finalize(int n, int b, int k, int ldp, int cap, int margin, int tile_base, const int* ti, const int* tj,
+                    int* need, const double* P, const double* C, const double* parts, const double* fparts,
+                    int nblk, double* gscratch, double* gsv, double* U, double* V, int* rank, int last_level,
+                    int nchunk, int* rlog, double* tail0, double* fro0, int* blog, int* status, cudaStream_t s) {
   size_t sm = (40 + 136 * 3 + 8 + (k <= 64 ? 2 * (size_t)k * k : 0)) * 8;
   const int w_in_smem = k <= 64 && (size_t)b * k * 8 <= 160 * 1024;
   if (w_in_smem) sm += (size_t)b * k * 8;
   cudaFuncSetAttribute(k_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_finalize<<<nchunk, k >= 32 ? 1024 : 256, sm, s>>>(n, b, k, ldp, cap, margin, rule_fixed, thr_rel, thr_abs, tile_base, ti, tj, need,
-                                     P, C, parts, fparts, nblk, gscratch, gsv, U, V, rank, last_level, w_in_smem,
-                                     rlog, rmode, tail0, fro0, round_store, blog, status);
+  k_finalize<<<nchunk, k >= 32 ? 1024 : 256, sm, s>>>(n, b, k, ldp, cap, margin, tile_base, ti, tj, need, P, C, parts,
+                                                      fparts, nblk, gscratch, gsv, U, V, rank, last_level,
+                                                      w_in_smem, rlog, tail0, fro0, blog, status);
   return (int)cudaGetLastError();
 }
 

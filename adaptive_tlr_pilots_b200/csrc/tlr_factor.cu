@@ -25,11 +25,13 @@ __device__ __forceinline__ int tidx(int i, int j) { return i * (i - 1) / 2 + j; 
 // lower-triangular 32 x 32 block; the inner index runs over (m, q) in ascending order, 32 at a
 // time through shared memory.
 __global__ void __launch_bounds__(256) k_diag_build(const double* TLR_RESTRICT xy, int n, int b, int k,
-                                                   double sigma2, double inv_range, int nu5, double nugget,
                                                    const double* TLR_RESTRICT U, const double* TLR_RESTRICT Y,
                                                    const int* TLR_RESTRICT rank, int cap, double* TLR_RESTRICT D,
                                                    const int* TLR_RESTRICT status) {
   if (*status != 0) return;
+  const EvalParams& prm = *eval_params(status);
+  const double sigma2 = prm.sigma2, inv_range = prm.inv_range, nugget = prm.nugget;
+  const int nu5 = prm.nu5;
   int blk = blockIdx.x, rb = 0;
   while (blk > rb) { blk -= rb + 1; ++rb; }
   const int cb = blk;
@@ -113,10 +115,12 @@ __global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int 
                                              double* TLR_RESTRICT Wd, double* TLR_RESTRICT Y,
                                              const int* TLR_RESTRICT rank, int cap,
                                              const double* TLR_RESTRICT z, double* TLR_RESTRICT rhs,
-                                             int round_store, double thr_abs, int* TLR_RESTRICT prec,
-                                             int* TLR_RESTRICT blog_trsm, int rmode,
+                                             int* TLR_RESTRICT prec, int* TLR_RESTRICT blog_trsm,
                                              const int* TLR_RESTRICT status) {
   if (*status != 0) return;
+  const EvalParams& prm = *eval_params(status);
+  const int round_store = prm.round_store, rmode = prm.rmode;
+  const double thr_abs = prm.thr_abs;
   const int i = k + 1 + blockIdx.x;
   if (i >= nB) return;
   const int t = tidx(i, k);
@@ -406,21 +410,30 @@ __device__ int rc_general_pair(int bi, int bj, int b, int cap, int r1, int ri, i
 // on the N = 50,000 bench workload and withdrawn: one Gram-Schmidt pass without re-orthogonalising
 // Q3 (5.53 against 5.09 evals/s, but 0.024 nats and 2e-3 of the gradient from FP64, over the
 // budget), a core Jacobi that stops at |cos| <= 1e-10 (no faster, 0.0079 nats, over budget on three
-// N = 20,000 sweep fields), and 128-thread CTAs at 6 or 8 per SM (recompression 279 / 318 ms
-// against 175 ms per evaluation).
+// N = 20,000 sweep fields), 128-thread CTAs at 6 or 8 per SM (recompression 279 / 318 ms
+// against 175 ms per evaluation), and 256-thread CTAs at 5 or 6 per SM (48 / 40 registers, which
+// spill: 237 / 272 ms against 188 ms in the same run, batched mixed 4.30 / 4.05 against 4.83
+// evals/s).
 constexpr int kRcSmemS = 32;  // cores with s <= 32 are solved in shared memory
 constexpr int kRcT = 256;     // threads per pair
 constexpr int kRcW = kRcT / 32;
-constexpr int kRcMinBlocks = 4;
+#ifndef TLR_RC_BLOCKS
+#define TLR_RC_BLOCKS 4
+#endif
+constexpr int kRcMinBlocks = TLR_RC_BLOCKS;  // resident CTAs per SM (the register cap follows)
+
+int rc_blocks_per_sm() { return kRcMinBlocks; }
 
 __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b, int k, int nB, double* TLR_RESTRICT U,
                                                    double* TLR_RESTRICT V, int* TLR_RESTRICT rank, int cap,
-                                                   int rule_fixed, double thr_rel, double thr_abs,
                                                    double* TLR_RESTRICT scratch, size_t slot_doubles,
                                                    int* TLR_RESTRICT next_pair, int* TLR_RESTRICT rlog,
-                                                   int* TLR_RESTRICT blog, int rmode, int general, int round_store,
-                                                   int* TLR_RESTRICT status) {
+                                                   int* TLR_RESTRICT blog, int* TLR_RESTRICT status) {
   if (*status != 0) return;
+  const EvalParams& prm = *eval_params(status);
+  const int rule_fixed = prm.rule_fixed, rmode = prm.rmode, round_store = prm.round_store;
+  const int general = round_store;  // rounded factors are not orthogonal: the general recompression
+  const double thr_rel = prm.thr_rel, thr_abs = prm.thr_abs;
   const int mB = nB - k - 1;  // trailing tiles
   const long npairs = (long)mB * (mB - 1) / 2;  // every trailing pair (i, j), k < j < i
   RcScratch S = rc_slot(scratch + (size_t)blockIdx.x * slot_doubles, b, cap);
@@ -719,38 +732,33 @@ __global__ void k_finish(int nB, int n, const double* ldpart, const double* qpar
 }
 
 // ----------------------------------------------------------------------------------------
-int launch_diag_build(const double* xy, int n, int b, int k, double sigma2, double inv_range, int nu5,
-                      double nugget, const double* U, const double* Y, const int* rank, int cap, double* D,
-                      const int* status, cudaStream_t s) {
+int launch_diag_build(const double* xy, int n, int b, int k, const double* U, const double* Y, const int* rank,
+                      int cap, double* D, const int* status, cudaStream_t s) {
   const int bk = std::min(b, n - k * b);
   const int nb = (bk + 31) / 32;
-  k_diag_build<<<nb * (nb + 1) / 2, 256, 0, s>>>(xy, n, b, k, sigma2, inv_range, nu5, nugget, U, Y, rank, cap, D,
-                                                 status);
+  k_diag_build<<<nb * (nb + 1) / 2, 256, 0, s>>>(xy, n, b, k, U, Y, rank, cap, D, status);
   return (int)cudaGetLastError();
 }
 
 int launch_trsm(const double* D, int n, int b, int k, int nB, double* U, double* V, double* Wd, double* Y,
-                const int* rank, int cap, const double* z, double* rhs, int round_store, double thr_abs, int* prec,
-                int* blog_trsm, int rmode, const int* status, cudaStream_t s) {
+                const int* rank, int cap, const double* z, double* rhs, int* prec, int* blog_trsm, const int* status,
+                cudaStream_t s) {
   if (nB - k - 1 <= 0) return 0;
-  k_trsm<<<nB - k - 1, 256, 0, s>>>(D, n, b, k, nB, U, V, Wd, Y, rank, cap, z, rhs, round_store, thr_abs, prec,
-                                    blog_trsm, rmode, status);
+  k_trsm<<<nB - k - 1, 256, 0, s>>>(D, n, b, k, nB, U, V, Wd, Y, rank, cap, z, rhs, prec, blog_trsm, status);
   return (int)cudaGetLastError();
 }
 
-int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, int rule_fixed,
-                      double thr_rel, double thr_abs, double* scratch, size_t slot_doubles, int nslots,
-                      int* next_pair, int* rlog_step, int* blog_step, int rmode, int general, int round_store,
-                      int* status, cudaStream_t s) {
+int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, double* scratch,
+                      size_t slot_doubles, int nslots, int* next_pair, int* rlog_step, int* blog_step, int* status,
+                      cudaStream_t s) {
   const long mB = nB - k - 1;
   const long npairs = mB * (mB - 1) / 2;
   if (npairs <= 0) return 0;
   const int grid = (int)std::min<long>(npairs, nslots);
   const size_t sm = (size_t)3 * kRcSmemS * kRcSmemS * 8;
   cudaFuncSetAttribute(k_recompress, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_recompress<<<grid, kRcT, sm, s>>>(n, b, k, nB, U, V, rank, cap, rule_fixed, thr_rel, thr_abs, scratch,
-                                     slot_doubles, next_pair, rlog_step, blog_step, rmode, general, round_store,
-                                     status);
+  k_recompress<<<grid, kRcT, sm, s>>>(n, b, k, nB, U, V, rank, cap, scratch, slot_doubles, next_pair, rlog_step,
+                                     blog_step, status);
   return (int)cudaGetLastError();
 }
 

@@ -4,7 +4,28 @@
 #include <stddef.h>
 #include <algorithm>
 
+#include "../../include/tlr_b200.h"
+
 namespace tlr {
+
+// The parameters of one evaluation that change with theta, the rule and the plan's modes.  They
+// live in the plan's control block (after the status word and the per-kernel work counters), so
+// the forward pass reads them on the device: a launch sequence captured once in a CUDA graph then
+// serves every theta.  launch_set_params writes them (kernel arguments, so the host copy is free
+// at once) and clears the status word and the counters, ahead of the captured sequence.
+struct EvalParams {
+  double sigma2, inv_range, nugget;  // covariance: sigma2, 1 / range, sigma2 eta
+  double thr_rel, thr_abs;           // rank rule thresholds (17:143-150)
+  int rule_fixed;                    // 1: relative rule, 0: absolute budget
+  int rmode;                         // rank map: kRankOff / kRankRecord / kRankReplay
+  int round_store;                   // storage rule 'mixed': round every stored pair
+  int nu5;                           // 0: Matern 3/2, 1: Matern 5/2
+};
+constexpr size_t kControlInts = 4 + 4 * TLR_NKINDS;                       // status, pad, work counters
+constexpr size_t kControlBytes = kControlInts * sizeof(int) + sizeof(EvalParams);
+__host__ __device__ inline const EvalParams* eval_params(const int* control) {
+  return reinterpret_cast<const EvalParams*>(control + kControlInts);
+}
 
 // Rank map: every rank the rule picks (initial compression of tile t at rlog[t], recompression of
 // trailing pair p of step k at rlog[ntiles + off_k + p]) is recorded, or replayed instead of the
@@ -21,7 +42,7 @@ int launch_gather_sites(const double* xy_in, const double* y_in, const long long
 
 // initial compression
 int launch_gen_offdiag(const double* xy, int n, int b, int tile_base, const int* ti, const int* tj, double* T,
-                       int nchunk, double sigma2, double inv_range, int nu5, const int* status, cudaStream_t s);
+                       int nchunk, const int* status, cudaStream_t s);
 int launch_sketch(const double* T, int n, int b, int k, int tile_base, const int* ti, const int* tj, const int* need,
                   const double* P, double* out, int ldp, int omega, int mode, int nchunk, const int* status,
                   cudaStream_t s);
@@ -36,32 +57,29 @@ int launch_project_resid(const double* T, int n, int b, int tile_base, const int
 int launch_resid(const double* T, int n, int b, int k, int ldp, int tile_base, const int* ti, const int* tj,
                  const int* need, const double* P, const double* C, double* parts, double* fparts, int nblk,
                  int nchunk, const int* status, cudaStream_t s);
-int launch_finalize(int n, int b, int k, int ldp, int cap, int margin, int rule_fixed, double thr_rel,
-                    double thr_abs, int tile_base, const int* ti, const int* tj, int* need, const double* P,
-                    const double* C, const double* parts, const double* fparts, int nblk, double* gscratch,
-                    double* gsv, double* U, double* V, int* rank, int last_level, int nchunk, int* rlog,
-                    int rmode, double* tail0, double* fro0, int round_store, int* blog, int* status,
-                    cudaStream_t s);
+int launch_finalize(int n, int b, int k, int ldp, int cap, int margin, int tile_base, const int* ti, const int* tj,
+                    int* need, const double* P, const double* C, const double* parts, const double* fparts,
+                    int nblk, double* gscratch, double* gsv, double* U, double* V, int* rank, int last_level,
+                    int nchunk, int* rlog, double* tail0, double* fro0, int* blog, int* status, cudaStream_t s);
 
 // factorization
-int launch_diag_build(const double* xy, int n, int b, int k, double sigma2, double inv_range, int nu5,
-                      double nugget, const double* U, const double* Y, const int* rank, int cap, double* D,
-                      const int* status, cudaStream_t s);
+int launch_diag_build(const double* xy, int n, int b, int k, const double* U, const double* Y, const int* rank,
+                      int cap, double* D, const int* status, cudaStream_t s);
 int launch_potrf(double* D, int n, int b, int k, double* rhs, double* z, double* ldpart, double* qpart,
                  int* status, cudaStream_t s);
 // nbatch tiles, tile q at D + q sD, rhs / z + q sV, ldpart / qpart / status + q sS
 int launch_potrf_batched(double* D, int n, int b, int k, double* rhs, double* z, double* ldpart, double* qpart,
                          int* status, int nbatch, size_t sD, size_t sV, int sS, cudaStream_t s);
 int launch_trsm(const double* D, int n, int b, int k, int nB, double* U, double* V, double* Wd, double* Y,
-                const int* rank, int cap, const double* z, double* rhs, int round_store, double thr_abs, int* prec,
-                int* blog_trsm, int rmode, const int* status, cudaStream_t s);
+                const int* rank, int cap, const double* z, double* rhs, int* prec, int* blog_trsm, const int* status,
+                cudaStream_t s);
 size_t rc_slot_doubles(int b, int cap);
 // every trailing pair of step k; next_pair: a counter that is zero at launch (the CTAs claim
 // pairs past the grid through it)
-int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, int rule_fixed,
-                      double thr_rel, double thr_abs, double* scratch, size_t slot_doubles, int nslots,
-                      int* next_pair, int* rlog_step, int* blog_step, int rmode, int general, int round_store,
-                      int* status, cudaStream_t s);
+int rc_blocks_per_sm();  // k_recompress CTAs resident per SM
+int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, double* scratch,
+                      size_t slot_doubles, int nslots, int* next_pair, int* rlog_step, int* blog_step, int* status,
+                      cudaStream_t s);
 // assembled-matrix rule: dense Sigma^TLR from the initial compression (N x N, leading dimension ldk)
 int launch_assemble(const double* xy, int n, int b, double sigma2, double inv_range, int nu5, double nugget,
                     const double* U, const double* V, const int* rank, int cap, double* K, long long ldk,
@@ -129,5 +147,7 @@ int set_error(int code, const char* msg);
 
 // small utilities
 int launch_fill_int(int* p, int v, int count, cudaStream_t s);
+// control block: zero the status word and the work counters, store the evaluation's parameters
+int launch_set_params(int* control, EvalParams prm, cudaStream_t s);
 
 }  // namespace tlr

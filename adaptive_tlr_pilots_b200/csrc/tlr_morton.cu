@@ -196,4 +196,14 @@ int launch_fill_int(int* p, int v, int count, cudaStream_t s) {
   return (int)cudaGetLastError();
 }
 
+__global__ void k_set_params(int* control, EvalParams prm) {
+  for (int i = threadIdx.x; i < (int)kControlInts; i += blockDim.x) control[i] = 0;
+  if (threadIdx.x == 0) *reinterpret_cast<EvalParams*>(control + kControlInts) = prm;
+}
+
+int launch_set_params(int* control, EvalParams prm, cudaStream_t s) {
+  k_set_params<<<1, 128, 0, s>>>(control, prm);
+  return (int)cudaGetLastError();
+}
+
 }  // namespace tlr

@@ -113,6 +113,7 @@ class Plan:
         self.generation = 0
         self._data = None
         self.precision = "fp64"
+        self.graphs = True      # forward pass replayed from a CUDA graph (set_graphs)
         self.nu = None          # None: follow set_kernel; else this plan's own smoothness
         self._create()
 
@@ -135,6 +136,8 @@ class Plan:
         self._create()
         if self.precision != "fp64":
             _lib.check(self.lib.tlr_plan_set_precision(self.handle, _lib.PRECISIONS[self.precision]))
+        if not getattr(self, "graphs", True):
+            _lib.check(self.lib.tlr_plan_set_graphs(self.handle, 0))
         self._apply_kernel()
         if getattr(self, "rank_mode", "rule") != "rule":
             # a recorded map does not survive the new workspace: record again
@@ -319,6 +322,12 @@ class Plan:
         only the launches of one kernel kind (a key of kernel_stats) when `kind` is given."""
         code = (-(_lib.KERNEL_KINDS.index(kind) + 1) if kind is not None else 1) if on else 0
         _lib.check(self.lib.tlr_plan_set_profiling(self.handle, code))
+
+    def set_graphs(self, on=True):
+        """Replay the forward pass from a CUDA graph captured once per precision (default), or
+        issue its launches one by one (off).  Results are bit-identical either way."""
+        _lib.check(self.lib.tlr_plan_set_graphs(self.handle, 1 if on else 0))
+        self.graphs = bool(on)
 
     def kernel_stats(self, reset=False):
         """{kernel kind: dict(ms, launches, flops, bytes)} accumulated since the last reset

@@ -234,6 +234,15 @@ int tlr_plan_set_kernel(tlr_plan* plan, double nu);
  * per-kind device time is accumulated (no effect on results); on < 0 brackets only the launches
  * of kernel kind -on - 1 (the order of tlr_plan_kernel_stats).  No reference counterpart. */
 int tlr_plan_set_profiling(tlr_plan* plan, int on);
+
+/* CUDA graphs (default on): the forward pass of an evaluation (compression, factorization and the
+ * forward solve, about 1,000 launches at N = 50,000, b = 500) is captured once per precision on a
+ * private stream and replayed on the plan's stream for every theta; theta, the rule and the
+ * thresholds reach the kernels through the plan's device control block, written by one launch
+ * before each replay.  Off: the same launches are issued one by one.  Results are bit-identical
+ * either way; while profiling is on the launches are issued one by one.  No reference counterpart
+ * (the reference is a Python loop, codes/17_tlr_cholesky_pilot.py:259-266). */
+int tlr_plan_set_graphs(tlr_plan* plan, int on);
 /* Per-kind accumulated device milliseconds (profiling on), launch counts and algorithmic work
  * (FP64 flops and HBM bytes the kernels count for themselves) since the last reset.  Any output
  * pointer may be NULL.  No reference counterpart. */
