@@ -18,6 +18,7 @@ TLR_RULE_MIXED = 2
 PRECISIONS = {"fp64": 0, "mixed": 1}
 RANK_MAP = {"rule": 0, "record": 1, "replay": 2}
 ERR_RANK_CAP = -2  # TLR_ERR_RANK_CAP: a tile rank exceeded the plan's capacity
+DIST_DIAG, DIST_PANEL, DIST_SUMS = 0, 1, 2  # tlr_dist_buffer_doubles: the three exchange buffers
 
 _lib = None
 
@@ -92,6 +93,20 @@ SIGNATURES = {
     "tlr_plan_set_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "tlr_plan_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tlr_plan_set_graphs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tlr_plan_set_partition": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "tlr_dist_buffer_doubles": (ctypes.c_longlong, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "tlr_dist_begin": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                                      ctypes.c_double]),
+    "tlr_dist_pack_diag": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "tlr_dist_unpack_diag": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "tlr_dist_solve_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tlr_dist_pack_panel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "tlr_dist_unpack_panel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "tlr_dist_update_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tlr_dist_pack_sums": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "tlr_dist_finish": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                       ctypes.POINTER(TlrInfo), ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int)]),
     "tlr_plan_kernel_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int]),

@@ -11,7 +11,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-SOURCES = ["tlr_api.cu", "tlr_compress.cu", "tlr_factor.cu", "tlr_morton.cu", "tlr_noalloc.cu", "tlr_potrf.cu", "tlr_backward.cu", "tlr_tc.cu", "tlr_solve.cu", "tlr_assemble.cu"]
+SOURCES = ["tlr_api.cu", "tlr_compress.cu", "tlr_factor.cu", "tlr_morton.cu", "tlr_noalloc.cu", "tlr_potrf.cu", "tlr_backward.cu", "tlr_tc.cu", "tlr_solve.cu", "tlr_assemble.cu",
+           "tlr_dist.cu"]
 OUT = os.path.join(HERE, "libtlr_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

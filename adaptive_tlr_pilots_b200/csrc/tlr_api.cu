@@ -136,6 +136,11 @@ struct tlr_plan {
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t fwd_exec[2] = {nullptr, nullptr};
   long long fwd_launch[2][TLR_NKINDS] = {};
+  // block-row cyclic partition (tlr_plan_set_partition): this plan holds block rows i with
+  // i % pworld == prank; tmap lists their tiles (nown of them) for the compression
+  int prank = 0, pworld = 1;
+  int* tmap = nullptr;
+  int nown = 0;
 };
 
 namespace {
@@ -208,8 +213,9 @@ cudaEvent_t next_event(tlr_plan* p) {
 int run_compression(tlr_plan* p) {
   cudaStream_t s = p->stream;
   const int ldp = kMaxK;
-  for (int base = 0; base < p->ntiles; base += p->chunk) {
-    const int nc = std::min(p->chunk, p->ntiles - base);
+  const int count = p->pworld > 1 ? p->nown : p->ntiles;  // the tiles this plan compresses
+  for (int base = 0; base < count; base += p->chunk) {
+    const int nc = std::min(p->chunk, count - base);
     LAUNCH(TLR_K_FILL, tlr::launch_fill_int(p->need, 1, nc, s));
     LAUNCH(TLR_K_GEN, tlr::launch_gen_offdiag(p->xy, p->n, p->b, base, p->ti, p->tj, p->T, nc, p->status, s));
     for (int lev = 0; lev < kLevels; ++lev) {
@@ -250,7 +256,7 @@ int run_factorization(tlr_plan* p) {
   LAUNCH(TLR_K_POTRF, tlr::launch_potrf(p->D, p->n, p->b, 0, p->rhs, p->z, p->ldpart, p->qpart, p->status, s));
   for (int k = 0; k < p->nB; ++k) {
     LAUNCH(TLR_K_TRSM, tlr::launch_trsm(p->D, p->n, p->b, k, p->nB, p->U, p->V, p->Wd, p->Yd, p->rank, p->cap, p->z, p->rhs,
-                                        p->prec, p->blog + p->rlog_off[p->nB], p->status, s));
+                                        p->prec, p->blog + p->rlog_off[p->nB], 0, 1, p->status, s));
     const bool ahead = k + 1 < p->nB;
     if (ahead) {
       // A_{k+1,k+1} needs only the panels m <= k, all final once the panel solve of step k is
@@ -265,7 +271,8 @@ int run_factorization(tlr_plan* p) {
     }
     LAUNCH(TLR_K_RECOMPRESS, tlr::launch_recompress(p->n, p->b, k, p->nB, p->U, p->V, p->rank, p->cap, p->rcs,
                                                     p->slot_doubles, p->nslots, p->rc_next + k,
-                                                    p->rlog + p->rlog_off[k], p->blog + p->rlog_off[k], p->status, s));
+                                                    p->rlog + p->rlog_off[k], p->blog + p->rlog_off[k], 0, 1,
+                                                    p->status, s));
     if (ahead) TRY(cuda_check(cudaStreamWaitEvent(s, p->ev_diag, 0), "wait"));
   }
   LAUNCH(TLR_K_FINISH, tlr::launch_finish(p->nB, p->n, p->ldpart, p->qpart, p->out, p->status, s));
@@ -341,6 +348,7 @@ tlr::EvalParams make_params(const tlr_plan* p, const double theta[3], int rule, 
   prm.rmode = p->rmode;
   prm.round_store = rule == TLR_RULE_MIXED ? 1 : 0;
   prm.nu5 = p->nu5;
+  prm.tmap = p->pworld > 1 ? p->tmap : nullptr;
   return prm;
 }
 
@@ -907,9 +915,12 @@ namespace {
 
 // Queue one forward evaluation (compression, factorization, solve) on the plan's stream; the
 // status, log-likelihood, work counters and ranks are copied to pinned host memory at the end.
+int enqueue_results(tlr_plan* p);
+
 int enqueue_forward(tlr_plan* p, const double theta[3], int rule, double value) {
   if (!p || !theta) return fail(TLR_ERR_ARG, "invalid arguments to tlr_loglik");
   if (!p->has_data) return fail(TLR_ERR_NOT_READY, "tlr_set_data has not been called");
+  if (p->pworld > 1) return fail(TLR_ERR_ARG, "the plan is partitioned: evaluate it through the tlr_dist_* steps");
   if (rule != TLR_RULE_FIXED && rule != TLR_RULE_ADAPTIVE && rule != TLR_RULE_MIXED)
     return fail(TLR_ERR_ARG, "rule must be fixed, adaptive or mixed");
   const double sigma2 = theta[0], range = theta[1], eta = theta[2];
@@ -922,6 +933,16 @@ int enqueue_forward(tlr_plan* p, const double theta[3], int rule, double value) 
   p->round_store = rule == TLR_RULE_MIXED ? 1 : 0;
   LAUNCH(TLR_K_FILL, tlr::launch_set_params(p->status, make_params(p, theta, rule, value), s));
   TRY(run_forward(p));
+  TRY(enqueue_results(p));
+  p->bw_sigma2 = sigma2;
+  p->bw_inv_range = 1.0 / range;
+  p->bw_eta = eta;
+  return 0;
+}
+
+// Copy the status, log-likelihood parts, work counters and ranks to pinned host memory.
+int enqueue_results(tlr_plan* p) {
+  cudaStream_t s = p->stream;
   TRY(cuda_check(cudaMemcpyAsync(&p->hb->status, p->status, sizeof(int), cudaMemcpyDeviceToHost, s), "status"));
   TRY(cuda_check(cudaMemcpyAsync(p->hb->out, p->out, sizeof(double) * 3, cudaMemcpyDeviceToHost, s), "out"));
   TRY(cuda_check(cudaMemcpyAsync(p->hb->work, p->status + 4, sizeof(double) * 2 * TLR_NKINDS,
@@ -933,9 +954,6 @@ int enqueue_forward(tlr_plan* p, const double theta[3], int rule, double value) 
     TRY(cuda_check(cudaMemcpyAsync(p->h_rank0, p->rank0, sizeof(int) * p->ntiles, cudaMemcpyDeviceToHost, s),
                    "ranks0"));
   }
-  p->bw_sigma2 = sigma2;
-  p->bw_inv_range = 1.0 / range;
-  p->bw_eta = eta;
   return 0;
 }
 
@@ -1033,6 +1051,7 @@ int tlr_truncate_tiles(tlr_plan* p, const double theta[3], int rule, double valu
   if (!p || !theta) return fail(TLR_ERR_ARG, "invalid arguments to tlr_truncate_tiles");
   if (!p->has_data) return fail(TLR_ERR_NOT_READY, "tlr_set_data has not been called");
   if (rule != TLR_RULE_FIXED && rule != TLR_RULE_ADAPTIVE) return fail(TLR_ERR_ARG, "rule must be fixed or adaptive");
+  if (p->pworld > 1) return fail(TLR_ERR_ARG, "the plan is partitioned");
   const double sigma2 = theta[0], range = theta[1], eta = theta[2];
   if (!(range > 0.0) || !std::isfinite(sigma2) || !std::isfinite(eta) || !std::isfinite(range))
     return fail(TLR_ERR_ARG, "theta must be finite with range > 0");
@@ -1262,6 +1281,160 @@ int tlr_plan_set_graphs(tlr_plan* p, int on) {
   if (!p) return fail(TLR_ERR_ARG, "plan is NULL");
   p->use_graphs = on != 0;
   return 0;
+}
+
+// ------------------------------------------------------------------------------------------
+// Block-row cyclic factorization (codes/13_multigpu_tile_cholesky.py:45-79 with the TLR tiles of
+// codes/17_tlr_cholesky_pilot.py:137-215): the host runs the steps and moves the buffers.
+
+int tlr_plan_set_partition(tlr_plan* p, int rank, int world) {
+  if (!p) return fail(TLR_ERR_ARG, "plan is NULL");
+  if (world < 1 || rank < 0 || rank >= world) return fail(TLR_ERR_ARG, "need 0 <= rank < world");
+  TRY(cuda_check(cudaSetDevice(p->device), "cudaSetDevice"));
+  TRY(cuda_check(cudaStreamSynchronize(p->stream), "partition"));
+  if (world > 1 && !p->tmap) TRY(dalloc(p, &p->tmap, (size_t)std::max(p->ntiles, 1)));
+  std::vector<int> own;
+  for (int t = 0; t < p->ntiles; ++t)
+    if (p->h_ti[t] % world == rank) own.push_back(t);
+  if (world > 1 && !own.empty())
+    TRY(cuda_check(cudaMemcpy(p->tmap, own.data(), sizeof(int) * own.size(), cudaMemcpyHostToDevice), "tile map"));
+  p->prank = world > 1 ? rank : 0;
+  p->pworld = world;
+  p->nown = (int)own.size();
+  p->factor_ok = false;
+  return 0;
+}
+
+long long tlr_dist_buffer_doubles(const tlr_plan* p, int which, int k) {
+  if (!p) return -1;
+  if (which == TLR_DIST_DIAG) return 8 + (long long)p->b * p->b + p->b;
+  if (which == TLR_DIST_PANEL) return (long long)tlr::dist_panel_doubles(p->b, p->cap, k, p->nB, p->pworld);
+  if (which == TLR_DIST_SUMS) return 2LL * p->nB + p->ntiles + p->pworld;
+  return -1;
+}
+
+namespace {
+int dist_ready(tlr_plan* p, int k) {
+  if (!p) return fail(TLR_ERR_ARG, "plan is NULL");
+  if (k < 0 || k >= p->nB) return fail(TLR_ERR_ARG, "step out of range");
+  return cuda_check(cudaSetDevice(p->device), "cudaSetDevice");
+}
+
+// Step k's diagonal tile on its owner: A_kk with the deferred updates, then POTRF and z_k.
+int dist_diag(tlr_plan* p, int k, cudaStream_t st) {
+  if (k % p->pworld != p->prank) return 0;
+  LAUNCH_ON(st, TLR_K_DIAG, tlr::launch_diag_build(p->xy, p->n, p->b, k, p->U, p->Yd, p->rank, p->cap, p->D,
+                                                   p->status, st));
+  LAUNCH_ON(st, TLR_K_POTRF, tlr::launch_potrf(p->D, p->n, p->b, k, p->rhs, p->z, p->ldpart, p->qpart, p->status,
+                                               st));
+  return 0;
+}
+}  // namespace
+
+int tlr_dist_begin(tlr_plan* p, const double theta[3], int rule, double value) {
+  if (!p || !theta) return fail(TLR_ERR_ARG, "invalid arguments to tlr_dist_begin");
+  if (!p->has_data) return fail(TLR_ERR_NOT_READY, "tlr_set_data has not been called");
+  if (rule != TLR_RULE_FIXED && rule != TLR_RULE_ADAPTIVE)
+    return fail(TLR_ERR_ARG, "the partitioned factorization takes the fixed and adaptive rules");
+  if (p->rmode != tlr::kRankOff) return fail(TLR_ERR_ARG, "the partitioned factorization keeps no rank map");
+  const double sigma2 = theta[0], range = theta[1], eta = theta[2];
+  if (!(range > 0.0) || !std::isfinite(sigma2) || !std::isfinite(eta) || !std::isfinite(range))
+    return fail(TLR_ERR_ARG, "theta must be finite with range > 0");
+  TRY(cuda_check(cudaSetDevice(p->device), "cudaSetDevice"));
+  cudaStream_t s = p->stream;
+  p->factor_ok = false;
+  p->round_store = 0;
+  LAUNCH(TLR_K_FILL, tlr::launch_set_params(p->status, make_params(p, theta, rule, value), s));
+  TRY(cuda_check(cudaMemsetAsync(p->rank, 0, sizeof(int) * std::max(p->ntiles, 1), s), "reset ranks"));
+  TRY(cuda_check(cudaMemsetAsync(p->ldpart, 0, sizeof(double) * p->nB, s), "log det parts"));
+  TRY(cuda_check(cudaMemsetAsync(p->qpart, 0, sizeof(double) * p->nB, s), "quadratic parts"));
+  TRY(cuda_check(cudaMemsetAsync(p->rc_next, 0, sizeof(int) * p->nB, s), "pair counters"));
+  TRY(cuda_check(cudaMemcpyAsync(p->rhs, p->y, sizeof(double) * p->n, cudaMemcpyDeviceToDevice, s), "rhs"));
+  TRY(run_compression(p));
+  if (p->ntiles > 0)
+    TRY(cuda_check(cudaMemcpyAsync(p->rank0, p->rank, sizeof(int) * p->ntiles, cudaMemcpyDeviceToDevice, s),
+                   "rank0"));
+  return dist_diag(p, 0, s);
+}
+
+int tlr_dist_pack_diag(tlr_plan* p, int k, double* buf) {
+  TRY(dist_ready(p, k));
+  if (!buf) return fail(TLR_ERR_ARG, "buffer is NULL");
+  LAUNCH(TLR_K_FILL, tlr::launch_dist_pack_diag(p->D, p->z, p->status, p->n, p->b, k, buf, p->stream));
+  return 0;
+}
+
+int tlr_dist_unpack_diag(tlr_plan* p, int k, const double* buf) {
+  TRY(dist_ready(p, k));
+  if (!buf) return fail(TLR_ERR_ARG, "buffer is NULL");
+  if (k % p->pworld == p->prank) return 0;  // the owner keeps its own
+  LAUNCH(TLR_K_FILL, tlr::launch_dist_unpack_diag(p->D, p->z, p->status, p->n, p->b, k, buf, p->stream));
+  return 0;
+}
+
+int tlr_dist_solve_step(tlr_plan* p, int k) {
+  TRY(dist_ready(p, k));
+  LAUNCH(TLR_K_TRSM, tlr::launch_trsm(p->D, p->n, p->b, k, p->nB, p->U, p->V, p->Wd, p->Yd, p->rank, p->cap, p->z,
+                                      p->rhs, p->prec, p->blog + p->rlog_off[p->nB], p->prank, p->pworld, p->status,
+                                      p->stream));
+  return 0;
+}
+
+int tlr_dist_pack_panel(tlr_plan* p, int k, double* buf) {
+  TRY(dist_ready(p, k));
+  if (!buf) return fail(TLR_ERR_ARG, "buffer is NULL");
+  LAUNCH(TLR_K_FILL, tlr::launch_dist_pack_panel(p->U, p->V, p->rank, p->status, p->n, p->b, k, p->nB, p->cap,
+                                                 p->prank, p->pworld, buf, p->stream));
+  return 0;
+}
+
+int tlr_dist_unpack_panel(tlr_plan* p, int k, const double* gathered) {
+  TRY(dist_ready(p, k));
+  if (!gathered) return fail(TLR_ERR_ARG, "buffer is NULL");
+  if (p->pworld == 1) return 0;
+  const size_t len = tlr::dist_panel_doubles(p->b, p->cap, k, p->nB, p->pworld);
+  LAUNCH(TLR_K_FILL, tlr::launch_dist_unpack_panel(p->U, p->V, p->rank, p->status, p->n, p->b, k, p->nB, p->cap,
+                                                   p->prank, p->pworld, gathered, len, p->stream));
+  return 0;
+}
+
+int tlr_dist_update_step(tlr_plan* p, int k) {
+  TRY(dist_ready(p, k));
+  cudaStream_t s = p->stream, sd = p->side;
+  const bool ahead = k + 1 < p->nB && (k + 1) % p->pworld == p->prank;
+  if (ahead) {  // the next diagonal tile on the side stream, beside this step's recompression
+    TRY(cuda_check(cudaEventRecord(p->ev_panel, s), "event"));
+    TRY(cuda_check(cudaStreamWaitEvent(sd, p->ev_panel, 0), "wait"));
+    TRY(dist_diag(p, k + 1, sd));
+    TRY(cuda_check(cudaEventRecord(p->ev_diag, sd), "event"));
+  }
+  LAUNCH(TLR_K_RECOMPRESS, tlr::launch_recompress(p->n, p->b, k, p->nB, p->U, p->V, p->rank, p->cap, p->rcs,
+                                                  p->slot_doubles, p->nslots, p->rc_next + k, p->rlog + p->rlog_off[k],
+                                                  p->blog + p->rlog_off[k], p->prank, p->pworld, p->status, s));
+  if (ahead) TRY(cuda_check(cudaStreamWaitEvent(s, p->ev_diag, 0), "wait"));
+  return 0;
+}
+
+int tlr_dist_pack_sums(tlr_plan* p, double* buf) {
+  TRY(dist_ready(p, 0));
+  if (!buf) return fail(TLR_ERR_ARG, "buffer is NULL");
+  LAUNCH(TLR_K_FILL, tlr::launch_dist_pack_sums(p->ldpart, p->qpart, p->rank0, p->ti, p->status, p->nB, p->ntiles,
+                                                p->prank, p->pworld, buf, p->stream));
+  return 0;
+}
+
+int tlr_dist_finish(tlr_plan* p, const double* sums, double* loglik, tlr_info* info, int* factor_ranks,
+                    int* sigma_ranks) {
+  TRY(dist_ready(p, 0));
+  if (!sums) return fail(TLR_ERR_ARG, "buffer is NULL");
+  cudaStream_t s = p->stream;
+  LAUNCH(TLR_K_FILL, tlr::launch_dist_unpack_sums(p->ldpart, p->qpart, p->rank0, p->status, p->nB, p->ntiles,
+                                                  p->pworld, sums, s));
+  LAUNCH(TLR_K_FINISH, tlr::launch_finish(p->nB, p->n, p->ldpart, p->qpart, p->out, p->status, s));
+  TRY(enqueue_results(p));
+  const int rc = finish_forward(p, loglik, info, factor_ranks, sigma_ranks);
+  p->factor_ok = false;  // each rank holds its own block rows only
+  return rc;
 }
 
 int tlr_plan_kernel_stats(tlr_plan* p, double* ms, long long* launches, double* flops, double* bytes, int nkinds,

@@ -40,7 +40,7 @@ __global__ void k_gen_offdiag(const double* TLR_RESTRICT xy, int n, int b, int t
   const double sigma2 = prm.sigma2, inv_range = prm.inv_range;
   const int nu5 = prm.nu5;
   const int c = blockIdx.y;
-  const int t = (tile_base + c);
+  const int t = tile_at(status, tile_base + c);
   const int i = ti[t], j = tj[t];
   const int i0 = i * b, j0 = j * b;
   const int bi = min(b, n - i0), bj = min(b, n - j0);
@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(256) k_sketch(const double* TLR_RESTRICT T, in
   if (*status != 0) return;
   const int c = blockIdx.x, g = blockIdx.y;
   if (!need[c]) return;
-  const int t = (tile_base + c);
+  const int t = tile_at(status, tile_base + c);
   const int bi = min(b, n - ti[t] * b), bj = min(b, n - tj[t] * b);
   if (threadIdx.x == 0)
     add_work(status, mode == 0 ? 2 : 4, (mode == 0 ? 4.0 : 2.0) * bi * bj * 16,
@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(kSkW * 32, 1)
   if (*status != 0) return;
   const int c = blockIdx.x, grp = blockIdx.y;
   if (!need[c]) return;
-  const int t = tile_base + c;
+  const int t = tile_at(status, tile_base + c);
   const int bi = min(b, n - ti[t] * b), bj = min(b, n - tj[t] * b);
   if (threadIdx.x == 0) {
     add_work(status, mode == 0 ? 2 : 4, (mode == 0 ? 4.0 : 2.0) * bi * bj * 16,
@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(1024) k_orth(double* TLR_RESTRICT Z, int n, in
   if (*status != 0) return;
   const int c = blockIdx.x;
   if (!need[c]) return;
-  const int bj = min(b, n - tj[(tile_base + c)] * b);
+  const int bj = min(b, n - tj[tile_at(status, tile_base + c)] * b);
   const int ke = min(k, bj);  // a tile narrower than k gets a full basis and zero columns
   if (threadIdx.x == 0) add_work(status, 3, 4.0 * bj * ke * ke, 16.0 * bj * k);
   extern __shared__ double smem[];
@@ -481,7 +481,7 @@ __global__ void __launch_bounds__(WARPS * 32, 16 / WARPS) k_orth_reg(double* TLR
   const int c = blockIdx.x;
   if (!need[c]) return;
   constexpr int k = WARPS * kOrCpw;
-  const int bj = min(b, n - tj[(tile_base + c)] * b);
+  const int bj = min(b, n - tj[tile_at(status, tile_base + c)] * b);
   const int ke = min(k, bj);  // a tile narrower than k gets a full basis and zero columns
   if (threadIdx.x == 0) add_work(status, 3, 4.0 * bj * ke * ke, 16.0 * bj * k);
   __shared__ double vs[32 * kOrRpl];  // the current reflector, zero above its pivot
@@ -570,7 +570,7 @@ __global__ void __launch_bounds__(256) k_resid(const double* TLR_RESTRICT T, int
   if (*status != 0) return;
   const int c = blockIdx.x, blk = blockIdx.y;
   if (!need[c]) return;
-  const int t = (tile_base + c);
+  const int t = tile_at(status, tile_base + c);
   const int bi = min(b, n - ti[t] * b), bj = min(b, n - tj[t] * b);
   const int q0 = blk * 64;
   if (q0 >= bj) {
@@ -650,7 +650,7 @@ __global__ void __launch_bounds__(1024) k_finalize(int n, int b, int k, int ldp,
   const double thr_rel = prm.thr_rel, thr_abs = prm.thr_abs;
   const int c = blockIdx.x;
   if (!need[c]) return;
-  const int t = (tile_base + c);
+  const int t = tile_at(status, tile_base + c);
   const int bi = min(b, n - ti[t] * b), bj = min(b, n - tj[t] * b);
   if (threadIdx.x == 0) add_work(status, 6, 4.0 * bi * k * k + 6.0 * 8.0 * k * k * k, 8.0 * (bi + bj) * k);
   extern __shared__ double smem[];

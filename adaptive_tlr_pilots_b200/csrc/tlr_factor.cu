@@ -115,14 +115,14 @@ __global__ void __launch_bounds__(256) k_trsm(const double* TLR_RESTRICT D, int 
                                              double* TLR_RESTRICT Wd, double* TLR_RESTRICT Y,
                                              const int* TLR_RESTRICT rank, int cap,
                                              const double* TLR_RESTRICT z, double* TLR_RESTRICT rhs,
-                                             int* TLR_RESTRICT prec, int* TLR_RESTRICT blog_trsm,
-                                             const int* TLR_RESTRICT status) {
+                                             int* TLR_RESTRICT prec, int* TLR_RESTRICT blog_trsm, int prank,
+                                             int pworld, const int* TLR_RESTRICT status) {
   if (*status != 0) return;
   const EvalParams& prm = *eval_params(status);
   const int round_store = prm.round_store, rmode = prm.rmode;
   const double thr_abs = prm.thr_abs;
   const int i = k + 1 + blockIdx.x;
-  if (i >= nB) return;
+  if (i >= nB || i % pworld != prank) return;  // block-row partition: this rank's rows only
   const int t = tidx(i, k);
   const int r = rank[t];
   if (r == 0) return;
@@ -424,18 +424,27 @@ constexpr int kRcMinBlocks = TLR_RC_BLOCKS;  // resident CTAs per SM (the regist
 
 int rc_blocks_per_sm() { return kRcMinBlocks; }
 
+// Trailing pairs held by the first m of a rank's rows ii0, ii0 + w, ... (row ii holds ii pairs).
+__host__ __device__ inline long rc_pairs_before(long m, long ii0, long w) { return m * ii0 + w * m * (m - 1) / 2; }
+
 __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b, int k, int nB, double* TLR_RESTRICT U,
                                                    double* TLR_RESTRICT V, int* TLR_RESTRICT rank, int cap,
                                                    double* TLR_RESTRICT scratch, size_t slot_doubles,
                                                    int* TLR_RESTRICT next_pair, int* TLR_RESTRICT rlog,
-                                                   int* TLR_RESTRICT blog, int* TLR_RESTRICT status) {
+                                                   int* TLR_RESTRICT blog, int prank, int pworld,
+                                                   int* TLR_RESTRICT status) {
   if (*status != 0) return;
   const EvalParams& prm = *eval_params(status);
   const int rule_fixed = prm.rule_fixed, rmode = prm.rmode, round_store = prm.round_store;
   const int general = round_store;  // rounded factors are not orthogonal: the general recompression
   const double thr_rel = prm.thr_rel, thr_abs = prm.thr_abs;
   const int mB = nB - k - 1;  // trailing tiles
-  const long npairs = (long)mB * (mB - 1) / 2;  // every trailing pair (i, j), k < j < i
+  // the pairs (i, j), k < j < i, of this rank's trailing rows ii = ii0 + m pworld (i = k + 1 + ii,
+  // i % pworld == prank; every row when pworld = 1): row ii holds ii pairs, so rows 0..m-1 of the
+  // rank hold C(m) = m ii0 + pworld m (m - 1) / 2
+  const long ii0 = ((prank - (k + 1)) % pworld + pworld) % pworld;
+  const long mown = ii0 < mB ? (mB - 1 - ii0) / pworld + 1 : 0;
+  const long npairs = rc_pairs_before(mown, ii0, pworld);
   RcScratch S = rc_slot(scratch + (size_t)blockIdx.x * slot_doubles, b, cap);
   extern __shared__ double rc_smem[];
   double* Msm = rc_smem;                            // kRcSmemS^2
@@ -469,12 +478,14 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     return q_next;
   };
   for (long qq = blockIdx.x; qq < npairs; qq = claim()) {
-    const long pp = qq;
-    // decode pp -> (ii, jj), ii > jj >= 0 within the trailing block
-    int ii = (int)((1.0 + sqrt(1.0 + 8.0 * (double)pp)) * 0.5);
-    while ((long)ii * (ii - 1) / 2 > pp) --ii;
-    while ((long)(ii + 1) * ii / 2 <= pp) ++ii;
-    const int jj = (int)(pp - (long)ii * (ii - 1) / 2);
+    // decode qq -> (row m of the rank, jj), then pp = the pair's index among all trailing pairs
+    const double hb = (double)ii0 - 0.5 * pworld;
+    long m = (long)((-hb + sqrt(hb * hb + 2.0 * pworld * (double)qq)) / pworld);
+    while (m > 0 && rc_pairs_before(m, ii0, pworld) > qq) --m;
+    while (rc_pairs_before(m + 1, ii0, pworld) <= qq) ++m;
+    const int ii = (int)(ii0 + m * pworld);
+    const int jj = (int)(qq - rc_pairs_before(m, ii0, pworld));
+    const long pp = (long)ii * (ii - 1) / 2 + jj;
     const int i = k + 1 + ii, j = k + 1 + jj;
     const int tij = tidx(i, j), tik = tidx(i, k), tjk = tidx(j, k);
     const int r1 = rank[tij], ri = rank[tik], rj = rank[tjk];
@@ -741,24 +752,26 @@ int launch_diag_build(const double* xy, int n, int b, int k, const double* U, co
 }
 
 int launch_trsm(const double* D, int n, int b, int k, int nB, double* U, double* V, double* Wd, double* Y,
-                const int* rank, int cap, const double* z, double* rhs, int* prec, int* blog_trsm, const int* status,
-                cudaStream_t s) {
+                const int* rank, int cap, const double* z, double* rhs, int* prec, int* blog_trsm, int prank,
+                int pworld, const int* status, cudaStream_t s) {
   if (nB - k - 1 <= 0) return 0;
-  k_trsm<<<nB - k - 1, 256, 0, s>>>(D, n, b, k, nB, U, V, Wd, Y, rank, cap, z, rhs, prec, blog_trsm, status);
+  k_trsm<<<nB - k - 1, 256, 0, s>>>(D, n, b, k, nB, U, V, Wd, Y, rank, cap, z, rhs, prec, blog_trsm, prank, pworld,
+                                    status);
   return (int)cudaGetLastError();
 }
 
 int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, double* scratch,
-                      size_t slot_doubles, int nslots, int* next_pair, int* rlog_step, int* blog_step, int* status,
-                      cudaStream_t s) {
+                      size_t slot_doubles, int nslots, int* next_pair, int* rlog_step, int* blog_step, int prank,
+                      int pworld, int* status, cudaStream_t s) {
   const long mB = nB - k - 1;
-  const long npairs = mB * (mB - 1) / 2;
+  const long ii0 = ((prank - (k + 1)) % pworld + pworld) % pworld;
+  const long npairs = rc_pairs_before(ii0 < mB ? (mB - 1 - ii0) / pworld + 1 : 0, ii0, pworld);
   if (npairs <= 0) return 0;
   const int grid = (int)std::min<long>(npairs, nslots);
   const size_t sm = (size_t)3 * kRcSmemS * kRcSmemS * 8;
   cudaFuncSetAttribute(k_recompress, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   k_recompress<<<grid, kRcT, sm, s>>>(n, b, k, nB, U, V, rank, cap, scratch, slot_doubles, next_pair, rlog_step,
-                                     blog_step, status);
+                                     blog_step, prank, pworld, status);
   return (int)cudaGetLastError();
 }
 

@@ -20,11 +20,18 @@ struct EvalParams {
   int rmode;                         // rank map: kRankOff / kRankRecord / kRankReplay
   int round_store;                   // storage rule 'mixed': round every stored pair
   int nu5;                           // 0: Matern 3/2, 1: Matern 5/2
+  const int* tmap;                   // block-row partition: the tiles this rank compresses (else all)
 };
 constexpr size_t kControlInts = 4 + 4 * TLR_NKINDS;                       // status, pad, work counters
 constexpr size_t kControlBytes = kControlInts * sizeof(int) + sizeof(EvalParams);
 __host__ __device__ inline const EvalParams* eval_params(const int* control) {
   return reinterpret_cast<const EvalParams*>(control + kControlInts);
+}
+// Storage index of the q-th tile the compression visits: every tile in order, or the rank's own
+// tiles under a block-row partition.
+__device__ __forceinline__ int tile_at(const int* control, int q) {
+  const int* m = eval_params(control)->tmap;
+  return m ? m[q] : q;
 }
 
 // Rank map: every rank the rule picks (initial compression of tile t at rlog[t], recompression of
@@ -71,15 +78,15 @@ int launch_potrf(double* D, int n, int b, int k, double* rhs, double* z, double*
 int launch_potrf_batched(double* D, int n, int b, int k, double* rhs, double* z, double* ldpart, double* qpart,
                          int* status, int nbatch, size_t sD, size_t sV, int sS, cudaStream_t s);
 int launch_trsm(const double* D, int n, int b, int k, int nB, double* U, double* V, double* Wd, double* Y,
-                const int* rank, int cap, const double* z, double* rhs, int* prec, int* blog_trsm, const int* status,
-                cudaStream_t s);
+                const int* rank, int cap, const double* z, double* rhs, int* prec, int* blog_trsm, int prank,
+                int pworld, const int* status, cudaStream_t s);
 size_t rc_slot_doubles(int b, int cap);
 // every trailing pair of step k; next_pair: a counter that is zero at launch (the CTAs claim
 // pairs past the grid through it)
 int rc_blocks_per_sm();  // k_recompress CTAs resident per SM
 int launch_recompress(int n, int b, int k, int nB, double* U, double* V, int* rank, int cap, double* scratch,
-                      size_t slot_doubles, int nslots, int* next_pair, int* rlog_step, int* blog_step, int* status,
-                      cudaStream_t s);
+                      size_t slot_doubles, int nslots, int* next_pair, int* rlog_step, int* blog_step, int prank,
+                      int pworld, int* status, cudaStream_t s);
 // assembled-matrix rule: dense Sigma^TLR from the initial compression (N x N, leading dimension ldk)
 int launch_assemble(const double* xy, int n, int b, double sigma2, double inv_range, int nu5, double nugget,
                     const double* U, const double* V, const int* rank, int cap, double* K, long long ldk,
@@ -147,6 +154,20 @@ int set_error(int code, const char* msg);
 
 // small utilities
 int launch_fill_int(int* p, int v, int count, cudaStream_t s);
+// block-row cyclic factorization: exchange buffers (layouts in tlr_dist.cu)
+size_t dist_panel_doubles(int b, int cap, int k, int nB, int pworld);
+int launch_dist_pack_diag(const double* D, const double* z, const int* status, int n, int b, int k, double* buf,
+                          cudaStream_t s);
+int launch_dist_unpack_diag(double* D, double* z, int* status, int n, int b, int k, const double* buf,
+                            cudaStream_t s);
+int launch_dist_pack_panel(const double* U, const double* V, const int* rank, const int* status, int n, int b, int k,
+                           int nB, int cap, int prank, int pworld, double* buf, cudaStream_t s);
+int launch_dist_unpack_panel(double* U, double* V, int* rank, int* status, int n, int b, int k, int nB, int cap,
+                             int prank, int pworld, const double* gathered, size_t len, cudaStream_t s);
+int launch_dist_pack_sums(const double* ldpart, const double* qpart, const int* rank0, const int* ti,
+                          const int* status, int nB, int ntiles, int prank, int pworld, double* buf, cudaStream_t s);
+int launch_dist_unpack_sums(double* ldpart, double* qpart, int* rank0, int* status, int nB, int ntiles, int pworld,
+                            const double* sums, cudaStream_t s);
 // control block: zero the status word and the work counters, store the evaluation's parameters
 int launch_set_params(int* control, EvalParams prm, cudaStream_t s);
 

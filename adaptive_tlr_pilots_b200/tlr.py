@@ -138,6 +138,8 @@ class Plan:
             _lib.check(self.lib.tlr_plan_set_precision(self.handle, _lib.PRECISIONS[self.precision]))
         if not getattr(self, "graphs", True):
             _lib.check(self.lib.tlr_plan_set_graphs(self.handle, 0))
+        if getattr(self, "partition", (0, 1))[1] > 1:
+            self.set_partition(*self.partition)
         self._apply_kernel()
         if getattr(self, "rank_mode", "rule") != "rule":
             # a recorded map does not survive the new workspace: record again
@@ -322,6 +324,12 @@ class Plan:
         only the launches of one kernel kind (a key of kernel_stats) when `kind` is given."""
         code = (-(_lib.KERNEL_KINDS.index(kind) + 1) if kind is not None else 1) if on else 0
         _lib.check(self.lib.tlr_plan_set_profiling(self.handle, code))
+
+    def set_partition(self, rank, world):
+        """Hold block rows i with i % world == rank only (the block-row cyclic factorization of
+        blockrow.py; world = 1 lifts it).  A partitioned plan is evaluated through blockrow."""
+        _lib.check(self.lib.tlr_plan_set_partition(self.handle, int(rank), int(world)))
+        self.partition = (int(rank), int(world))
 
     def set_graphs(self, on=True):
         """Replay the forward pass from a CUDA graph captured once per precision (default), or

@@ -243,6 +243,49 @@ int tlr_plan_set_profiling(tlr_plan* plan, int on);
  * either way; while profiling is on the launches are issued one by one.  No reference counterpart
  * (the reference is a Python loop, codes/17_tlr_cholesky_pilot.py:259-266). */
 int tlr_plan_set_graphs(tlr_plan* plan, int on);
+
+/* Block-row cyclic factorization over `world` ranks (codes/13_multigpu_tile_cholesky.py:45-79,
+ * tile_cholesky_multi, with the TLR tiles and rank rule of codes/17_tlr_cholesky_pilot.py:137-215).
+ * A partitioned plan holds block rows i with i % world == rank: it compresses their tiles and
+ * factors them; the diagonal tile of step k lives on rank k % world.  One process (or plan) per
+ * rank; the host moves three kinds of device buffers between them and every rank takes the same
+ * steps in the same order:
+ *
+ *   tlr_dist_begin(plan, theta, rule, value)            compression of the rank's tiles; step 0's
+ *                                                        diagonal tile on its owner
+ *   for k in 0 .. nB-1:
+ *     owner of k:  tlr_dist_pack_diag(plan, k, dbuf)     then broadcast dbuf from rank k % world
+ *     the others:  tlr_dist_unpack_diag(plan, k, dbuf)   (13:63-66)
+ *     tlr_dist_solve_step(plan, k)                       panel solve of the rank's tiles (i, k)
+ *     tlr_dist_pack_panel(plan, k, pbuf)                 then all-gather pbuf (length
+ *     tlr_dist_unpack_panel(plan, k, gathered)           tlr_dist_buffer_doubles(PANEL, k), rank order)
+ *     tlr_dist_update_step(plan, k)                      recompression of the rank's trailing pairs,
+ *                                                        and the next diagonal tile on its owner
+ *   tlr_dist_pack_sums(plan, sbuf)                       then all-reduce (sum) sbuf
+ *   tlr_dist_finish(plan, summed, &loglik, &info, ...)   tlr_loglik's outputs on every rank
+ *
+ * Every tile is computed by the same kernels as on one plan, so the log-likelihood, ranks and
+ * stored sizes are bit-identical to tlr_loglik's (the sums add zeros).  A failure on any rank
+ * (a non-positive pivot, a rank past the capacity) travels in the buffers' status word and every
+ * rank returns the first one in rank order.  Rules fixed and adaptive; no rank map; a partitioned
+ * plan refuses tlr_loglik and the factor-based calls (world = 1 lifts the partition).  Buffer
+ * sizes in doubles: tlr_dist_buffer_doubles(plan, TLR_DIST_DIAG | TLR_DIST_PANEL | TLR_DIST_SUMS,
+ * k) (PANEL with k < 0: the largest step).  Device buffers, on the plan's stream. */
+#define TLR_DIST_DIAG 0
+#define TLR_DIST_PANEL 1
+#define TLR_DIST_SUMS 2
+int tlr_plan_set_partition(tlr_plan* plan, int rank, int world);
+long long tlr_dist_buffer_doubles(const tlr_plan* plan, int which, int k);
+int tlr_dist_begin(tlr_plan* plan, const double theta[3], int rule, double value);
+int tlr_dist_pack_diag(tlr_plan* plan, int k, double* buf);
+int tlr_dist_unpack_diag(tlr_plan* plan, int k, const double* buf);
+int tlr_dist_solve_step(tlr_plan* plan, int k);
+int tlr_dist_pack_panel(tlr_plan* plan, int k, double* buf);
+int tlr_dist_unpack_panel(tlr_plan* plan, int k, const double* gathered);
+int tlr_dist_update_step(tlr_plan* plan, int k);
+int tlr_dist_pack_sums(tlr_plan* plan, double* buf);
+int tlr_dist_finish(tlr_plan* plan, const double* sums, double* loglik, tlr_info* info, int* factor_ranks,
+                    int* sigma_ranks);
 /* Per-kind accumulated device milliseconds (profiling on), launch counts and algorithmic work
  * (FP64 flops and HBM bytes the kernels count for themselves) since the last reset.  Any output
  * pointer may be NULL.  No reference counterpart. */

@@ -1,0 +1,101 @@
+"""The block-row cyclic TLR factorization through the library (tlr_dist_*), with its ranks run in
+lockstep on one GPU (blockrow.evaluate_lockstep: one partitioned plan per rank, the exchanges
+device copies).  Every tile is computed by the same kernels as on one plan, so the result must be
+the single plan's bit for bit: log-likelihood, log-determinant, quadratic form, initial and factor
+ranks, stored sizes, and the failing tile when the factorization breaks down."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def tlr():
+    import adaptive_tlr_pilots_b200 as m
+    yield m
+    m.release_plans()
+
+
+def _same(single, ranks):
+    for ev in ranks:
+        assert ev.status == single.status
+        assert ev.info["completed"] == single.info["completed"]
+        assert ev.info["stored_sigma"] == single.info["stored_sigma"]
+        assert np.array_equal(ev.sigma_ranks, single.sigma_ranks)
+        if single.status != 0:
+            assert ev.info["failed_at"] == single.info["failed_at"]
+            continue
+        assert ev.loglik == single.loglik
+        for key in ("logdet", "quad", "stored_factor", "max_rank_factor", "mean_rank_factor"):
+            assert ev.info[key] == single.info[key], key
+        assert np.array_equal(ev.factor_ranks, single.factor_ranks)
+
+
+def _plans(tlr, n, b, world, S, y, cap=64):
+    ps = []
+    for _ in range(world):
+        p = tlr.Plan(n, b, cap=cap)
+        p.set_data(S, y)
+        ps.append(p)
+    return ps
+
+
+@pytest.mark.parametrize("world", [2, 3, 5])
+@pytest.mark.parametrize("rule,value", [("adaptive", 0.9), ("fixed", 1e-4), ("fixed", 1e-3)])
+def test_lockstep_equals_single_plan(tlr, world, rule, value):
+    from adaptive_tlr_pilots_b200 import blockrow
+    d = np.load(os.path.join(GOLD, "n4000_b250_data.npz"))
+    S, y = d["S"], d["y"]
+    theta = (1.0, 0.3, 0.05)
+    single = tlr.Plan(4000, 250)
+    single.set_data(S, y)
+    ref = single.evaluate(theta, rule, value)
+    plans = _plans(tlr, 4000, 250, world, S, y)
+    out = blockrow.evaluate_lockstep(plans, theta, rule, value)
+    _same(ref, out)
+    if rule == "fixed" and value == 1e-3:
+        assert ref.status == 4  # the reference's verdict on this field: diagonal tile 3
+    # a partitioned plan refuses the one-plan calls
+    from adaptive_tlr_pilots_b200 import _lib
+    with pytest.raises(_lib.TlrError):
+        plans[0].evaluate(theta, rule, value)
+    for p in plans + [single]:
+        p.close()
+
+
+def test_lockstep_at_n20000_and_capacity_growth(tlr):
+    """N = 20,000, b = 500 (40 block rows) on 4 ranks, against the single plan and the reference's
+    fixture; then plans of capacity 8 (adaptive ranks reach 18 on the N = 4,000 field) grow
+    together and still agree."""
+    from adaptive_tlr_pilots_b200 import blockrow
+    g = json.load(open(os.path.join(GOLD, "golden_c2.json")))
+    d = np.load(os.path.join(GOLD, g["data"]))
+    rec = g["cases"][0]
+    S, y = d["S"], d["y_" + rec["name"]]
+    single = tlr.Plan(g["n"], g["b"])
+    single.set_data(S, y)
+    ref = single.evaluate(rec["theta"], g["rule"], g["value"])
+    plans = _plans(tlr, g["n"], g["b"], 4, S, y)
+    out = blockrow.evaluate_lockstep(plans, rec["theta"], g["rule"], g["value"])
+    _same(ref, out)
+    assert np.array_equal(out[0].sigma_ranks, np.asarray(rec["sigma_ranks"]))
+    if rec["completed"]:
+        assert np.array_equal(out[2].factor_ranks, np.asarray(rec["factor_ranks"]))
+        assert abs(out[1].loglik - rec["loglik"]) <= 1e-10 * abs(rec["loglik"])
+    for p in plans + [single]:
+        p.close()
+    d = np.load(os.path.join(GOLD, "n4000_b250_data.npz"))
+    S, y = d["S"], d["y"]
+    single = tlr.Plan(4000, 250)
+    single.set_data(S, y)
+    ref = single.evaluate((1.0, 0.3, 0.05), "adaptive", 0.9)
+    plans = _plans(tlr, 4000, 250, 2, S, y, cap=8)
+    out = blockrow.evaluate_lockstep(plans, (1.0, 0.3, 0.05), "adaptive", 0.9)
+    assert all(p.cap > 8 for p in plans)
+    _same(ref, out)
+    for p in plans + [single]:
+        p.close()
