@@ -311,6 +311,43 @@ __device__ void cta_atb(const double* A, int lda, const double* B, int ldb, int 
   }
 }
 
+// C[v][u] = (sum_t A[u][t] B[v][t]) (times scale[u] when scale is given) for u < p, v < q, column v
+// of C at C + v ldc.  One warp per (u, four consecutive v), so A's column is read once for four
+// dots; every entry is summed as in cta_atb (lane t = lane, lane + 32, ..., then the butterfly),
+// so the results are cta_atb's bit for bit.
+__device__ void cta_atb4(const double* A, int lda, const double* B, int ldb, int m, int p, int q, double* C,
+                         int ldc, const double* scale) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int nq = (q + 3) >> 2;
+  for (int e = warp; e < p * nq; e += nwarp) {
+    const int u = e % p, v0 = (e / p) * 4;
+    const double* a = A + (size_t)u * lda;
+    const double* b0 = B + (size_t)v0 * ldb;
+    const double* b1 = B + (size_t)min(v0 + 1, q - 1) * ldb;
+    const double* b2 = B + (size_t)min(v0 + 2, q - 1) * ldb;
+    const double* b3 = B + (size_t)min(v0 + 3, q - 1) * ldb;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    for (int t = lane; t < m; t += 32) {
+      const double x = a[t];
+      s0 += x * b0[t];
+      s1 += x * b1[t];
+      s2 += x * b2[t];
+      s3 += x * b3[t];
+    }
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    s2 = warp_sum(s2);
+    s3 = warp_sum(s3);
+    if (lane == 0) {
+      const double sc = scale ? scale[u] : 1.0;
+      C[(size_t)v0 * ldc + u] = scale ? s0 * sc : s0;
+      if (v0 + 1 < q) C[(size_t)(v0 + 1) * ldc + u] = scale ? s1 * sc : s1;
+      if (v0 + 2 < q) C[(size_t)(v0 + 2) * ldc + u] = scale ? s2 * sc : s2;
+      if (v0 + 3 < q) C[(size_t)(v0 + 3) * ldc + u] = scale ? s3 * sc : s3;
+    }
+  }
+}
+
 // General recompression of one trailing pair, the reference's recompress as written
 // (codes/17_tlr_cholesky_pilot.py:119-133): Householder QR of A = [U_ij, -U_ik W] and
 // B = [V_ij, U_jk] (no orthogonality assumed), SVD of the core R_u R_v^T by one-sided Jacobi on
@@ -505,7 +542,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     const int lc = core_in_smem ? kRcSmemS : ls;
     __syncthreads();
     // W = V_ik^T V_jk (ri x rj); column norms of U_ij
-    cta_atb(Vik, b, Vjk, b, bk, ri, rj, S.W, cap);
+    cta_atb4(Vik, b, Vjk, b, bk, ri, rj, S.W, cap, nullptr);
     for (int c = warp; c < r1; c += kRcW) {
       const double* u = Uij + (size_t)c * b;
       const double* v = Vij + (size_t)c * b;
@@ -535,32 +572,36 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
       __syncthreads();
       continue;
     }
-    // X = -U_ik W (bi x rj)
-    for (int q = 0; q < rj; ++q)
-      for (int a = tid; a < bi; a += kRcT) {
-        double acc = 0.0;
-        for (int p = 0; p < ri; ++p) acc = fma(Uik[(size_t)p * b + a], S.W[(size_t)q * cap + p], acc);
-        S.X[(size_t)q * b + a] = -acc;
+    // X = -U_ik W (bi x rj), four columns per pass over a row of U_ik
+    for (int a = tid; a < bi; a += kRcT)
+      for (int q0 = 0; q0 < rj; q0 += 4) {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int p = 0; p < ri; ++p) {
+          const double x = Uik[(size_t)p * b + a];
+#pragma unroll
+          for (int w = 0; w < 4; ++w) acc[w] = fma(x, S.W[(size_t)min(q0 + w, rj - 1) * cap + p], acc[w]);
+        }
+#pragma unroll
+        for (int w = 0; w < 4; ++w)
+          if (q0 + w < rj) S.X[(size_t)(q0 + w) * b + a] = -acc[w];
       }
     __syncthreads();
     // block Gram-Schmidt twice against Q1 = U_ij diag(1/n1): C = Q1^T X, X -= Q1 C
     for (int pass = 0; pass < 2; ++pass) {
       if (r1 > 0) {
-        for (int e = warp; e < r1 * rj; e += kRcW) {
-          const int u = e % r1, v = e / r1;
-          const double* a = Uij + (size_t)u * b;
-          const double* x = S.X + (size_t)v * b;
-          double acc = 0.0;
-          for (int t = lane; t < bi; t += 32) acc += a[t] * x[t];
-          acc = warp_sum(acc);
-          if (lane == 0) S.G[(size_t)v * cap + u] = acc * ninv[u];  // C increment
-        }
+        cta_atb4(Uij, b, S.X, b, bi, r1, rj, S.G, cap, ninv);  // C increment
         __syncthreads();
-        for (int v = 0; v < rj; ++v)
-          for (int a = tid; a < bi; a += kRcT) {
-            double acc = 0.0;
-            for (int u = 0; u < r1; ++u) acc = fma(Uij[(size_t)u * b + a] * ninv[u], S.G[(size_t)v * cap + u], acc);
-            S.X[(size_t)v * b + a] -= acc;
+        for (int a = tid; a < bi; a += kRcT)
+          for (int v0 = 0; v0 < rj; v0 += 4) {
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int u = 0; u < r1; ++u) {
+              const double x = Uij[(size_t)u * b + a] * ninv[u];
+#pragma unroll
+              for (int w = 0; w < 4; ++w) acc[w] = fma(x, S.G[(size_t)min(v0 + w, rj - 1) * cap + u], acc[w]);
+            }
+#pragma unroll
+            for (int w = 0; w < 4; ++w)
+              if (v0 + w < rj) S.X[(size_t)(v0 + w) * b + a] -= acc[w];
           }
         for (int e = tid; e < r1 * rj; e += kRcT) {
           const int u = e % r1, v = e / r1;
@@ -578,15 +619,19 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     __syncthreads();
     for (int pass = 0; pass < 2; ++pass) {
       if (r1 > 0) {
-        cta_atb(Vij, b, S.Y, b, bj, r1, rj, S.G, cap);
+        cta_atb4(Vij, b, S.Y, b, bj, r1, rj, S.G, cap, nvinv);
         __syncthreads();
-        for (int e = tid; e < r1 * rj; e += kRcT) S.G[(size_t)(e / r1) * cap + (e % r1)] *= nvinv[e % r1];
-        __syncthreads();
-        for (int v = 0; v < rj; ++v)
-          for (int a = tid; a < bj; a += kRcT) {
-            double acc = 0.0;
-            for (int u = 0; u < r1; ++u) acc = fma(Vij[(size_t)u * b + a] * nvinv[u], S.G[(size_t)v * cap + u], acc);
-            S.Y[(size_t)v * b + a] -= acc;
+        for (int a = tid; a < bj; a += kRcT)
+          for (int v0 = 0; v0 < rj; v0 += 4) {
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int u = 0; u < r1; ++u) {
+              const double x = Vij[(size_t)u * b + a] * nvinv[u];
+#pragma unroll
+              for (int w = 0; w < 4; ++w) acc[w] = fma(x, S.G[(size_t)min(v0 + w, rj - 1) * cap + u], acc[w]);
+            }
+#pragma unroll
+            for (int w = 0; w < 4; ++w)
+              if (v0 + w < rj) S.Y[(size_t)(v0 + w) * b + a] -= acc[w];
           }
         for (int e = tid; e < r1 * rj; e += kRcT) {
           const int u = e % r1, v = e / r1;
@@ -624,14 +669,20 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     }
     // re-orthogonalise Q3 against the normalised V_ij once
     if (r1 > 0) {
-      cta_atb(Vij, b, S.Y, b, bj, r1, rj, S.G, cap);
+      cta_atb4(Vij, b, S.Y, b, bj, r1, rj, S.G, cap, nullptr);
       __syncthreads();
-      for (int v = 0; v < rj; ++v)
-        for (int a = tid; a < bj; a += kRcT) {
-          double acc = 0.0;
-          for (int u = 0; u < r1; ++u)
-            acc = fma(Vij[(size_t)u * b + a] * nvinv[u], S.G[(size_t)v * cap + u] * nvinv[u], acc);
-          S.Y[(size_t)v * b + a] -= acc;
+      for (int a = tid; a < bj; a += kRcT)
+        for (int v0 = 0; v0 < rj; v0 += 4) {
+          double acc[4] = {0.0, 0.0, 0.0, 0.0};
+          for (int u = 0; u < r1; ++u) {
+            const double x = Vij[(size_t)u * b + a] * nvinv[u];
+#pragma unroll
+            for (int w = 0; w < 4; ++w)
+              acc[w] = fma(x, S.G[(size_t)min(v0 + w, rj - 1) * cap + u] * nvinv[u], acc[w]);
+          }
+#pragma unroll
+          for (int w = 0; w < 4; ++w)
+            if (v0 + w < rj) S.Y[(size_t)(v0 + w) * b + a] -= acc[w];
         }
       __syncthreads();
     }
@@ -699,24 +750,44 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
       S.Hh[(size_t)c * cap + p] = acc;
     }
     __syncthreads();
-    // U' = U_ij G_top - U_ik H ; V' = V_ij Vs_top + Q3 Vs_bottom
-    for (int c = 0; c < rn; ++c) {
-      const double* gc = S.G + (size_t)c * ls;
-      const double* hc = S.Hh + (size_t)c * cap;
-      const double* vc = Vc + (size_t)perm[c] * lc;
-      for (int a = tid; a < bi; a += kRcT) {
-        double acc = 0.0;
-        for (int t = 0; t < r1; ++t) acc = fma(Uij[(size_t)t * b + a], gc[t], acc);
-        for (int p = 0; p < ri; ++p) acc = fma(-Uik[(size_t)p * b + a], hc[p], acc);
-        S.Uo[(size_t)c * b + a] = acc;
+    // U' = U_ij G_top - U_ik H ; V' = V_ij Vs_top + Q3 Vs_bottom, four columns per pass over a row
+    for (int a = tid; a < bi; a += kRcT)
+      for (int c0 = 0; c0 < rn; c0 += 4) {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int t = 0; t < r1; ++t) {
+          const double x = Uij[(size_t)t * b + a];
+#pragma unroll
+          for (int w = 0; w < 4; ++w) acc[w] = fma(x, S.G[(size_t)min(c0 + w, rn - 1) * ls + t], acc[w]);
+        }
+        for (int p = 0; p < ri; ++p) {
+          const double x = -Uik[(size_t)p * b + a];
+#pragma unroll
+          for (int w = 0; w < 4; ++w) acc[w] = fma(x, S.Hh[(size_t)min(c0 + w, rn - 1) * cap + p], acc[w]);
+        }
+#pragma unroll
+        for (int w = 0; w < 4; ++w)
+          if (c0 + w < rn) S.Uo[(size_t)(c0 + w) * b + a] = acc[w];
       }
-      for (int a = tid; a < bj; a += kRcT) {
-        double acc = 0.0;
-        for (int t = 0; t < r1; ++t) acc = fma(Vij[(size_t)t * b + a] * nvinv[t], vc[t], acc);
-        for (int t = 0; t < rj; ++t) acc = fma(S.Y[(size_t)t * b + a], vc[r1 + t], acc);
-        S.Vo[(size_t)c * b + a] = acc;
+    for (int a = tid; a < bj; a += kRcT)
+      for (int c0 = 0; c0 < rn; c0 += 4) {
+        int vo[4];  // offsets of the four right singular vectors in Vc
+#pragma unroll
+        for (int w = 0; w < 4; ++w) vo[w] = perm[min(c0 + w, rn - 1)] * lc;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int t = 0; t < r1; ++t) {
+          const double x = Vij[(size_t)t * b + a] * nvinv[t];
+#pragma unroll
+          for (int w = 0; w < 4; ++w) acc[w] = fma(x, Vc[vo[w] + t], acc[w]);
+        }
+        for (int t = 0; t < rj; ++t) {
+          const double x = S.Y[(size_t)t * b + a];
+#pragma unroll
+          for (int w = 0; w < 4; ++w) acc[w] = fma(x, Vc[vo[w] + r1 + t], acc[w]);
+        }
+#pragma unroll
+        for (int w = 0; w < 4; ++w)
+          if (c0 + w < rn) S.Vo[(size_t)(c0 + w) * b + a] = acc[w];
       }
-    }
     __syncthreads();
     double* Uw = U + (size_t)tij * b * cap;
     double* Vw = V + (size_t)tij * b * cap;
