@@ -659,7 +659,7 @@ __global__ void __launch_bounds__(1024) k_finalize(int n, int b, int k, int ldp,
   double* sig = tau + 136;        // k
   int* perm = reinterpret_cast<int*>(sig + 136);  // k
   int* iflag = perm + 136;
-  int* rsel = iflag + 1;
+  int* rsel = iflag + 2;
   double* M = (k <= 64) ? smem + 40 + 136 * 3 + 8 : gsv + (size_t)c * 2 * k * k;  // k x k
   double* Vw = M + k * k;                                                             // k x k
   const size_t pbase = (size_t)c * b * ldp;

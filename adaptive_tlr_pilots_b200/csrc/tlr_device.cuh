@@ -241,6 +241,8 @@ __device__ inline void cta_geqr2(double* A, int lda, int m, int n, double* tau, 
     if (tc != 0.0)
       for (int t = c + 1 + threadIdx.x; t < m; t += blockDim.x) col[t] *= scale;
     __syncthreads();
+    // every thread has read alpha; the updates below read only col[t > c]
+    if (threadIdx.x == 0) { col[c] = beta; tau[c] = tc; }
     for (int j = c + 1 + warp; j < n; j += nwarp) {
       double* aj = A + (size_t)j * lda;
       double w = 0.0;
@@ -250,8 +252,6 @@ __device__ inline void cta_geqr2(double* A, int lda, int m, int n, double* tau, 
       __syncwarp();
       if (lane == 0) aj[c] -= w;
     }
-    __syncthreads();
-    if (threadIdx.x == 0) { col[c] = beta; tau[c] = tc; }
     __syncthreads();
   }
   for (int c = kmax + threadIdx.x; c < n; c += blockDim.x) tau[c] = 0.0;
@@ -306,7 +306,7 @@ __device__ inline void cta_org2r(double* A, int lda, int m, int n, const double*
 // singular value (ties by index).  Round-robin parallel ordering, one warp per pair; squared
 // column norms are computed afresh at the start of every sweep and updated by the rotation
 // formulas within it (a_pp' = a_pp - t a_pq, a_qq' = a_qq + t a_pq), so a pair costs one inner
-// product.  `sig` needs n doubles, `iflag` one int of shared memory.  Returns the sweeps used.
+// product.  `sig` needs n doubles, `iflag` two ints of shared memory.  Returns the sweeps used.
 // With floor_rel > 0, a column whose squared norm is at most floor_rel times the largest squared
 // column norm counts as zero and is not rotated: columns at the rounding level of the others
 // (from cores assembled out of Gram matrices) would otherwise keep the relative test of their
@@ -334,7 +334,7 @@ __device__ inline int cta_jacobi_svd(double* M, int ldm, int m, int n, double* V
       }
       if (floor_rel > 0.0) __syncthreads();  // the column norms above come from every warp
       if (threadIdx.x == 0) {
-        *iflag = 0;
+        iflag[sweep & 1] = 0;  // two flags, alternating: no barrier between a sweep's read and the next clear
         double mx = 0.0;
         if (floor_rel > 0.0)
           for (int c = 0; c < n; ++c) mx = fmax(mx, sig[c]);
@@ -382,15 +382,13 @@ __device__ inline int cta_jacobi_svd(double* M, int ldm, int m, int n, double* V
             if (lane == 0) {
               sig[p] = app - t * apq;
               sig[q] = aqq + t * apq;
-              *iflag = 1;
+              iflag[sweep & 1] = 1;
             }
           }
         }
         __syncthreads();
       }
-      const int any = *iflag;
-      __syncthreads();
-      if (!any) break;
+      if (!iflag[sweep & 1]) break;
     }
   }
   // singular values = column norms

@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
   __shared__ double nvinv[128];
   __shared__ double sig[256];
   __shared__ int perm[256];
-  __shared__ int iflag;
+  __shared__ int iflag[2];
   __shared__ int rsel;
   __shared__ __align__(8) int gsel[4];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -561,7 +561,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     __syncthreads();
     if (general) {  // storage rule 'mixed': the reference's recompression as written
       const int rn = rc_general_pair(bi, bj, b, cap, r1, ri, rj, Uik, Ujk, S.W, U + (size_t)tij * b * cap,
-                                     V + (size_t)tij * b * cap, S, sig, perm, &iflag, red, gsel, rule_fixed,
+                                     V + (size_t)tij * b * cap, S, sig, perm, iflag, red, gsel, rule_fixed,
                                      thr_rel, thr_abs, round_store, rlog + pp, blog + pp, rmode, status);
       if (rn < 0) return;
       if (tid == 0) {
@@ -642,8 +642,8 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
       __syncthreads();
     }
     // R_u = [[diag(n1), C], [0, R2]] (s x s, ld ls)
-    for (int c = 0; c < s; ++c)
-      for (int a = tid; a < s; a += kRcT) {
+    for (int e = tid; e < s * s; e += kRcT) {  // entry (a, c); every small loop below is flat too
+        const int a = e % s, c = e / s;
         double vu = 0.0;
         if (a < r1) vu = (c < r1) ? (a == c ? n1[a] : 0.0) : S.Cc[(size_t)(c - r1) * cap + a];
         else if (c >= r1 && a <= c && a - r1 < bi) vu = S.X[(size_t)(c - r1) * b + (a - r1)];
@@ -653,8 +653,8 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     double* tau3 = sig + 128;
     cta_geqr2(S.Y, b, bj, rj, tau3, red);
     // R_v = [[I, D], [0, R3]]
-    for (int c = 0; c < s; ++c)
-      for (int a = tid; a < s; a += kRcT) {
+    for (int e = tid; e < s * s; e += kRcT) {
+        const int a = e % s, c = e / s;
         double vv = 0.0;
         if (a < r1) vv = (c < r1) ? (a == c ? nvv[a] : 0.0) : S.Dd[(size_t)(c - r1) * cap + a];
         else if (c >= r1 && a <= c && a - r1 < bj) vv = S.Y[(size_t)(c - r1) * b + (a - r1)];
@@ -687,8 +687,8 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
       __syncthreads();
     }
     // core M = R_u R_v^T (s x s); both factors are upper triangular
-    for (int c = 0; c < s; ++c)
-      for (int a = tid; a < s; a += kRcT) {
+    for (int e = tid; e < s * s; e += kRcT) {
+        const int a = e % s, c = e / s;
         double acc = 0.0;
         const int t0 = a > c ? a : c;
         for (int t = t0; t < s; ++t) acc = fma(S.Ru[(size_t)t * ls + a], S.Rv[(size_t)t * ls + c], acc);
@@ -700,12 +700,14 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     // are the normalised columns of Z.  The QR grades the columns, so the Jacobi needs 3-5 sweeps
     // instead of 6-16 on M itself.
     cta_geqr2(Mc, lc, s, s, sig, red);
-    for (int c = 0; c < s; ++c)
-      for (int a = tid; a < s; a += kRcT) Zc[(size_t)c * lc + a] = (a >= c) ? Mc[(size_t)a * lc + c] : 0.0;
+    for (int e = tid; e < s * s; e += kRcT) {
+      const int a = e % s, c = e / s;
+      Zc[(size_t)c * lc + a] = (a >= c) ? Mc[(size_t)a * lc + c] : 0.0;
+    }
     __syncthreads();
     // columns below 1e-14 of the largest singular value (the projections' rounding noise) are not
     // rotated: their relative orthogonality test would otherwise run to the sweep limit
-    cta_jacobi_svd(Zc, lc, s, s, Vc, lc, sig, perm, &iflag, 40, 1e-28);
+    cta_jacobi_svd(Zc, lc, s, s, Vc, lc, sig, perm, iflag, 40, 1e-28);
     // Vc <- normalised Z (right singular vectors of M), in place of the rotation matrix
     for (int c = warp; c < s; c += kRcW) {
       const double inv = sig[c] > 0.0 ? 1.0 / sig[c] : 0.0;
@@ -735,8 +737,8 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
       add_work(status, 10, 4.0 * b * ri * rj + 8.0 * b * s * s + 4.0 * b * s * rn,
                8.0 * ((double)(bi + bj) * r1 + (double)(bi + bj) * rn));
     // G = R_v^T Vs_r (s x rn), H = W G_bottom (ri x rn)
-    for (int c = 0; c < rn; ++c)
-      for (int t = tid; t < s; t += kRcT) {
+    for (int e = tid; e < s * rn; e += kRcT) {
+        const int t = e % s, c = e / s;
         const double* vc = Vc + (size_t)perm[c] * lc;
         double acc = 0.0;
         for (int a = 0; a <= t; ++a) acc = fma(S.Rv[(size_t)t * ls + a], vc[a], acc);
