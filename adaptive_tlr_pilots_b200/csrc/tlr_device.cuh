@@ -222,6 +222,19 @@ __device__ inline int cta_round_pair(double* U, double* V, int mu, int mv, int r
 // In-place Householder QR of the m x n column-major A (lda): R in the upper triangle,
 // reflector vectors below the diagonal (implicit unit leading entry), tau[0..n).
 // Same reflector convention as LAPACK dgeqr2/dlarfg.  One warp per trailing column.
+// block_sum's value without its broadcast barrier: every warp finishes the reduction itself (the
+// same inputs through the same butterfly, so the same bits as block_sum).  The leading barrier,
+// which orders this call's writes of red[0..warps) after earlier readers, may be skipped (lead =
+// false, uniform over the CTA) when every thread has passed a barrier since its last read of red.
+__device__ __forceinline__ double block_sum_nb(double v, double* red, bool lead) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_sum(v);
+  if (lead) __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  return warp_sum(lane < nw ? red[lane] : 0.0);
+}
+
 __device__ inline void cta_geqr2(double* A, int lda, int m, int n, double* tau, double* red) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   const int kmax = n < m ? n : m;
@@ -229,7 +242,8 @@ __device__ inline void cta_geqr2(double* A, int lda, int m, int n, double* tau, 
     double* col = A + (size_t)c * lda;
     double s = 0.0;
     for (int t = c + 1 + threadIdx.x; t < m; t += blockDim.x) { const double x = col[t]; s += x * x; }
-    const double sig2 = block_sum(s, red);
+    // columns after the first: the previous column's two barriers follow every read of red
+    const double sig2 = block_sum_nb(s, red, c == 0);
     const double alpha = col[c];
     double beta, tc, scale;
     if (sig2 == 0.0) { tc = 0.0; beta = alpha; scale = 1.0; }
@@ -313,7 +327,9 @@ __device__ inline void cta_org2r(double* A, int lda, int m, int n, const double*
 // pairs failing forever.
 __device__ inline int cta_jacobi_svd(double* M, int ldm, int m, int n, double* V, int ldv, double* sig,
                                      int* perm, int* iflag, int max_sweeps = 40, double floor_rel = 0.0) {
-  __shared__ double s_floor2;
+  // largest squared column norm of a sweep, as the bits of a double >= 0 (their integer order is
+  // the doubles' order); two slots, alternating like the flags
+  __shared__ unsigned long long s_mx[2];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   for (int j = warp; j < n; j += nwarp)
     for (int i = lane; i < n; i += 32) V[(size_t)j * ldv + i] = (i == j) ? 1.0 : 0.0;
@@ -324,24 +340,30 @@ __device__ inline int cta_jacobi_svd(double* M, int ldm, int m, int n, double* V
   const double tol2 = tol * tol;
   int sweep = 0;
   if (n > 1) {
+    // two flags, alternating: the flag of sweep s + 1 is cleared during sweep s, after the barrier
+    // that follows every read of it at the end of sweep s - 1
+    if (threadIdx.x == 0) {
+      iflag[0] = 0;
+      s_mx[0] = 0ull;
+    }
+    __syncthreads();
     for (sweep = 0; sweep < max_sweeps; ++sweep) {
       for (int c = warp; c < n; c += nwarp) {
         const double* mc = M + (size_t)c * ldm;
         double a = 0.0;
         for (int t = lane; t < m; t += 32) a += mc[t] * mc[t];
         a = warp_sum(a);
-        if (lane == 0) sig[c] = a;
+        if (lane == 0) {
+          sig[c] = a;
+          if (floor_rel > 0.0) atomicMax(&s_mx[sweep & 1], (unsigned long long)__double_as_longlong(a));
+        }
       }
-      if (floor_rel > 0.0) __syncthreads();  // the column norms above come from every warp
+      __syncthreads();  // the column norms above come from every warp
       if (threadIdx.x == 0) {
-        iflag[sweep & 1] = 0;  // two flags, alternating: no barrier between a sweep's read and the next clear
-        double mx = 0.0;
-        if (floor_rel > 0.0)
-          for (int c = 0; c < n; ++c) mx = fmax(mx, sig[c]);
-        s_floor2 = floor_rel * mx;
+        iflag[(sweep + 1) & 1] = 0;
+        s_mx[(sweep + 1) & 1] = 0ull;
       }
-      __syncthreads();
-      const double floor2 = s_floor2;
+      const double floor2 = floor_rel * __longlong_as_double((long long)s_mx[sweep & 1]);
       for (int round = 0; round < np - 1; ++round) {
         for (int pr = warp; pr < np / 2; pr += nwarp) {
           // circle method: player 0 fixed, the others rotate
