@@ -613,13 +613,16 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     }
     // R2 from Householder QR of the projected X (bi x rj); its reflectors are not needed
     cta_geqr2(S.X, b, bi, rj, sig, red);
-    // V side: D = V_ij^T U_jk, Y = U_jk - V_ij D (twice)
-    for (int v = 0; v < rj; ++v)
-      for (int a = tid; a < bj; a += kRcT) S.Y[(size_t)v * b + a] = Ujk[(size_t)v * b + a];
-    __syncthreads();
+    // V side: D = V_ij^T U_jk, Y = U_jk - V_ij D (twice; the first pass reads U_jk itself)
+    if (r1 == 0) {
+      for (int v = 0; v < rj; ++v)
+        for (int a = tid; a < bj; a += kRcT) S.Y[(size_t)v * b + a] = Ujk[(size_t)v * b + a];
+      __syncthreads();
+    }
     for (int pass = 0; pass < 2; ++pass) {
       if (r1 > 0) {
-        cta_atb4(Vij, b, S.Y, b, bj, r1, rj, S.G, cap, nvinv);
+        const double* Yin = pass == 0 ? Ujk : S.Y;
+        cta_atb4(Vij, b, Yin, b, bj, r1, rj, S.G, cap, nvinv);
         __syncthreads();
         for (int a = tid; a < bj; a += kRcT)
           for (int v0 = 0; v0 < rj; v0 += 4) {
@@ -631,7 +634,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
             }
 #pragma unroll
             for (int w = 0; w < 4; ++w)
-              if (v0 + w < rj) S.Y[(size_t)(v0 + w) * b + a] -= acc[w];
+              if (v0 + w < rj) S.Y[(size_t)(v0 + w) * b + a] = Yin[(size_t)(v0 + w) * b + a] - acc[w];
           }
         for (int e = tid; e < r1 * rj; e += kRcT) {
           const int u = e % r1, v = e / r1;
@@ -752,7 +755,14 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
       S.Hh[(size_t)c * cap + p] = acc;
     }
     __syncthreads();
-    // U' = U_ij G_top - U_ik H ; V' = V_ij Vs_top + Q3 Vs_bottom, four columns per pass over a row
+    // U' = U_ij G_top - U_ik H ; V' = V_ij Vs_top + Q3 Vs_bottom, four columns per pass over a row.
+    // With rn <= 4 one pass makes a row's every output after reading all its inputs (each thread
+    // reads and writes its own rows only), so the new pair goes straight over the old one.
+    double* Uw = U + (size_t)tij * b * cap;
+    double* Vw = V + (size_t)tij * b * cap;
+    const bool direct = rn <= 4;
+    double* Uout = direct ? Uw : S.Uo;
+    double* Vout = direct ? Vw : S.Vo;
     for (int a = tid; a < bi; a += kRcT)
       for (int c0 = 0; c0 < rn; c0 += 4) {
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
@@ -768,7 +778,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
         }
 #pragma unroll
         for (int w = 0; w < 4; ++w)
-          if (c0 + w < rn) S.Uo[(size_t)(c0 + w) * b + a] = acc[w];
+          if (c0 + w < rn) Uout[(size_t)(c0 + w) * b + a] = acc[w];
       }
     for (int a = tid; a < bj; a += kRcT)
       for (int c0 = 0; c0 < rn; c0 += 4) {
@@ -788,14 +798,14 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
         }
 #pragma unroll
         for (int w = 0; w < 4; ++w)
-          if (c0 + w < rn) S.Vo[(size_t)(c0 + w) * b + a] = acc[w];
+          if (c0 + w < rn) Vout[(size_t)(c0 + w) * b + a] = acc[w];
       }
-    __syncthreads();
-    double* Uw = U + (size_t)tij * b * cap;
-    double* Vw = V + (size_t)tij * b * cap;
-    for (int c = 0; c < rn; ++c) {
-      for (int a = tid; a < bi; a += kRcT) Uw[(size_t)c * b + a] = S.Uo[(size_t)c * b + a];
-      for (int a = tid; a < bj; a += kRcT) Vw[(size_t)c * b + a] = S.Vo[(size_t)c * b + a];
+    if (!direct) {
+      __syncthreads();
+      for (int c = 0; c < rn; ++c) {
+        for (int a = tid; a < bi; a += kRcT) Uw[(size_t)c * b + a] = S.Uo[(size_t)c * b + a];
+        for (int a = tid; a < bj; a += kRcT) Vw[(size_t)c * b + a] = S.Vo[(size_t)c * b + a];
+      }
     }
     if (tid == 0) rank[tij] = rn;
     __syncthreads();
