@@ -452,11 +452,18 @@ __device__ int rc_general_pair(int bi, int bj, int b, int cap, int r1, int ri, i
 // spill: 237 / 272 ms against 188 ms in the same run, batched mixed 4.30 / 4.05 against 4.83
 // evals/s).
 constexpr int kRcSmemS = 32;  // cores with s <= 32 are solved in shared memory
-constexpr int kRcT = 256;     // threads per pair
+#ifndef TLR_RC_THREADS
+#define TLR_RC_THREADS 256
+#endif
+constexpr int kRcT = TLR_RC_THREADS;  // threads per pair
 constexpr int kRcW = kRcT / 32;
 #ifndef TLR_RC_BLOCKS
-#define TLR_RC_BLOCKS 4
+#define TLR_RC_BLOCKS 3
 #endif
+#ifndef TLR_RC_CHUNK
+#define TLR_RC_CHUNK 8
+#endif
+constexpr int kRcCW = TLR_RC_CHUNK;  // output columns per pass over a row in the row loops
 constexpr int kRcMinBlocks = TLR_RC_BLOCKS;  // resident CTAs per SM (the register cap follows)
 
 int rc_blocks_per_sm() { return kRcMinBlocks; }
@@ -572,17 +579,17 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
       __syncthreads();
       continue;
     }
-    // X = -U_ik W (bi x rj), four columns per pass over a row of U_ik
+    // X = -U_ik W (bi x rj), kRcCW columns per pass over a row of U_ik
     for (int a = tid; a < bi; a += kRcT)
-      for (int q0 = 0; q0 < rj; q0 += 4) {
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int q0 = 0; q0 < rj; q0 += kRcCW) {
+        double acc[kRcCW] = {};
         for (int p = 0; p < ri; ++p) {
           const double x = Uik[(size_t)p * b + a];
 #pragma unroll
-          for (int w = 0; w < 4; ++w) acc[w] = fma(x, S.W[(size_t)min(q0 + w, rj - 1) * cap + p], acc[w]);
+          for (int w = 0; w < kRcCW; ++w) acc[w] = fma(x, S.W[(size_t)min(q0 + w, rj - 1) * cap + p], acc[w]);
         }
 #pragma unroll
-        for (int w = 0; w < 4; ++w)
+        for (int w = 0; w < kRcCW; ++w)
           if (q0 + w < rj) S.X[(size_t)(q0 + w) * b + a] = -acc[w];
       }
     __syncthreads();
@@ -592,15 +599,15 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
         cta_atb4(Uij, b, S.X, b, bi, r1, rj, S.G, cap, ninv);  // C increment
         __syncthreads();
         for (int a = tid; a < bi; a += kRcT)
-          for (int v0 = 0; v0 < rj; v0 += 4) {
-            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+          for (int v0 = 0; v0 < rj; v0 += kRcCW) {
+            double acc[kRcCW] = {};
             for (int u = 0; u < r1; ++u) {
               const double x = Uij[(size_t)u * b + a] * ninv[u];
 #pragma unroll
-              for (int w = 0; w < 4; ++w) acc[w] = fma(x, S.G[(size_t)min(v0 + w, rj - 1) * cap + u], acc[w]);
+              for (int w = 0; w < kRcCW; ++w) acc[w] = fma(x, S.G[(size_t)min(v0 + w, rj - 1) * cap + u], acc[w]);
             }
 #pragma unroll
-            for (int w = 0; w < 4; ++w)
+            for (int w = 0; w < kRcCW; ++w)
               if (v0 + w < rj) S.X[(size_t)(v0 + w) * b + a] -= acc[w];
           }
         for (int e = tid; e < r1 * rj; e += kRcT) {
@@ -625,15 +632,15 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
         cta_atb4(Vij, b, Yin, b, bj, r1, rj, S.G, cap, nvinv);
         __syncthreads();
         for (int a = tid; a < bj; a += kRcT)
-          for (int v0 = 0; v0 < rj; v0 += 4) {
-            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+          for (int v0 = 0; v0 < rj; v0 += kRcCW) {
+            double acc[kRcCW] = {};
             for (int u = 0; u < r1; ++u) {
               const double x = Vij[(size_t)u * b + a] * nvinv[u];
 #pragma unroll
-              for (int w = 0; w < 4; ++w) acc[w] = fma(x, S.G[(size_t)min(v0 + w, rj - 1) * cap + u], acc[w]);
+              for (int w = 0; w < kRcCW; ++w) acc[w] = fma(x, S.G[(size_t)min(v0 + w, rj - 1) * cap + u], acc[w]);
             }
 #pragma unroll
-            for (int w = 0; w < 4; ++w)
+            for (int w = 0; w < kRcCW; ++w)
               if (v0 + w < rj) S.Y[(size_t)(v0 + w) * b + a] = Yin[(size_t)(v0 + w) * b + a] - acc[w];
           }
         for (int e = tid; e < r1 * rj; e += kRcT) {
@@ -675,16 +682,16 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
       cta_atb4(Vij, b, S.Y, b, bj, r1, rj, S.G, cap, nullptr);
       __syncthreads();
       for (int a = tid; a < bj; a += kRcT)
-        for (int v0 = 0; v0 < rj; v0 += 4) {
-          double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int v0 = 0; v0 < rj; v0 += kRcCW) {
+          double acc[kRcCW] = {};
           for (int u = 0; u < r1; ++u) {
             const double x = Vij[(size_t)u * b + a] * nvinv[u];
 #pragma unroll
-            for (int w = 0; w < 4; ++w)
+            for (int w = 0; w < kRcCW; ++w)
               acc[w] = fma(x, S.G[(size_t)min(v0 + w, rj - 1) * cap + u] * nvinv[u], acc[w]);
           }
 #pragma unroll
-          for (int w = 0; w < 4; ++w)
+          for (int w = 0; w < kRcCW; ++w)
             if (v0 + w < rj) S.Y[(size_t)(v0 + w) * b + a] -= acc[w];
         }
       __syncthreads();
@@ -755,49 +762,49 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
       S.Hh[(size_t)c * cap + p] = acc;
     }
     __syncthreads();
-    // U' = U_ij G_top - U_ik H ; V' = V_ij Vs_top + Q3 Vs_bottom, four columns per pass over a row.
-    // With rn <= 4 one pass makes a row's every output after reading all its inputs (each thread
+    // U' = U_ij G_top - U_ik H ; V' = V_ij Vs_top + Q3 Vs_bottom, kRcCW columns per pass over a row.
+    // With rn <= kRcCW one pass makes a row's every output after reading all its inputs (each thread
     // reads and writes its own rows only), so the new pair goes straight over the old one.
     double* Uw = U + (size_t)tij * b * cap;
     double* Vw = V + (size_t)tij * b * cap;
-    const bool direct = rn <= 4;
+    const bool direct = rn <= kRcCW;
     double* Uout = direct ? Uw : S.Uo;
     double* Vout = direct ? Vw : S.Vo;
     for (int a = tid; a < bi; a += kRcT)
-      for (int c0 = 0; c0 < rn; c0 += 4) {
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int c0 = 0; c0 < rn; c0 += kRcCW) {
+        double acc[kRcCW] = {};
         for (int t = 0; t < r1; ++t) {
           const double x = Uij[(size_t)t * b + a];
 #pragma unroll
-          for (int w = 0; w < 4; ++w) acc[w] = fma(x, S.G[(size_t)min(c0 + w, rn - 1) * ls + t], acc[w]);
+          for (int w = 0; w < kRcCW; ++w) acc[w] = fma(x, S.G[(size_t)min(c0 + w, rn - 1) * ls + t], acc[w]);
         }
         for (int p = 0; p < ri; ++p) {
           const double x = -Uik[(size_t)p * b + a];
 #pragma unroll
-          for (int w = 0; w < 4; ++w) acc[w] = fma(x, S.Hh[(size_t)min(c0 + w, rn - 1) * cap + p], acc[w]);
+          for (int w = 0; w < kRcCW; ++w) acc[w] = fma(x, S.Hh[(size_t)min(c0 + w, rn - 1) * cap + p], acc[w]);
         }
 #pragma unroll
-        for (int w = 0; w < 4; ++w)
+        for (int w = 0; w < kRcCW; ++w)
           if (c0 + w < rn) Uout[(size_t)(c0 + w) * b + a] = acc[w];
       }
     for (int a = tid; a < bj; a += kRcT)
-      for (int c0 = 0; c0 < rn; c0 += 4) {
-        int vo[4];  // offsets of the four right singular vectors in Vc
+      for (int c0 = 0; c0 < rn; c0 += kRcCW) {
+        int vo[kRcCW];  // offsets of the chunk's right singular vectors in Vc
 #pragma unroll
-        for (int w = 0; w < 4; ++w) vo[w] = perm[min(c0 + w, rn - 1)] * lc;
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int w = 0; w < kRcCW; ++w) vo[w] = perm[min(c0 + w, rn - 1)] * lc;
+        double acc[kRcCW] = {};
         for (int t = 0; t < r1; ++t) {
           const double x = Vij[(size_t)t * b + a] * nvinv[t];
 #pragma unroll
-          for (int w = 0; w < 4; ++w) acc[w] = fma(x, Vc[vo[w] + t], acc[w]);
+          for (int w = 0; w < kRcCW; ++w) acc[w] = fma(x, Vc[vo[w] + t], acc[w]);
         }
         for (int t = 0; t < rj; ++t) {
           const double x = S.Y[(size_t)t * b + a];
 #pragma unroll
-          for (int w = 0; w < 4; ++w) acc[w] = fma(x, Vc[vo[w] + r1 + t], acc[w]);
+          for (int w = 0; w < kRcCW; ++w) acc[w] = fma(x, Vc[vo[w] + r1 + t], acc[w]);
         }
 #pragma unroll
-        for (int w = 0; w < 4; ++w)
+        for (int w = 0; w < kRcCW; ++w)
           if (c0 + w < rn) Vout[(size_t)(c0 + w) * b + a] = acc[w];
       }
     if (!direct) {
