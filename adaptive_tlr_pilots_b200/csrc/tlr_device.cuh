@@ -272,6 +272,57 @@ __device__ inline void cta_geqr2(double* A, int lda, int m, int n, double* tau, 
   __syncthreads();
 }
 
+// The R of cta_geqr2, bit for bit, when neither the reflectors nor tau are wanted: on return the
+// entries of A on and above the diagonal hold R, those below it are left as they were.  The
+// reflector is applied as column x 1 / (alpha - beta), the very product cta_geqr2 stores (scale is
+// 1 exactly when tau is 0), so no scaling pass and its barrier.  With m <= 32 only warp 0 holds
+// entries of a column norm, so block_sum's value is warp 0's butterfly: every warp forms that itself
+// and a column costs one barrier.
+__device__ inline void cta_geqr2_r(double* A, int lda, int m, int n, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int kmax = n < m ? n : m;
+  for (int c = 0; c < kmax; ++c) {
+    double* col = A + (size_t)c * lda;
+    double sig2;
+    if (m <= 32) {
+      const int t = c + 1 + lane;
+      const double x = t < m ? col[t] : 0.0;
+      sig2 = warp_sum(x * x);
+    } else {
+      double s = 0.0;
+      for (int t = c + 1 + threadIdx.x; t < m; t += blockDim.x) { const double x = col[t]; s += x * x; }
+      sig2 = block_sum_nb(s, red, c == 0);  // later columns: the barrier below follows every read of red
+    }
+    const double alpha = col[c];
+    double beta, tc, scale;
+    if (sig2 == 0.0) { tc = 0.0; beta = alpha; scale = 1.0; }
+    else {
+      beta = -copysign(sqrt(alpha * alpha + sig2), alpha);
+      tc = (beta - alpha) / beta;
+      scale = 1.0 / (alpha - beta);
+    }
+    for (int j = c + 1 + warp; j < n; j += nwarp) {
+      double* aj = A + (size_t)j * lda;
+      double w = 0.0;
+      for (int t = c + 1 + lane; t < m; t += 32) {
+        const double v = col[t] * scale;
+        w += v * aj[t];
+      }
+      w = (warp_sum(w) + aj[c]) * tc;
+      for (int t = c + 1 + lane; t < m; t += 32) {
+        const double v = col[t] * scale;
+        aj[t] -= w * v;
+      }
+      __syncwarp();
+      if (lane == 0) aj[c] -= w;
+    }
+    __syncthreads();
+    // every thread has read alpha; no later column reads this entry
+    if (threadIdx.x == 0) col[c] = beta;
+  }
+  __syncthreads();
+}
+
 // Copy the upper-triangular R (n x n, or kmax rows) out of a factored A into Rout (ldr),
 // zeroing the strictly lower part.
 __device__ inline void cta_copy_r(const double* A, int lda, int m, int n, double* R, int ldr) {
@@ -315,7 +366,7 @@ __device__ inline void cta_org2r(double* A, int lda, int m, int n, const double*
 
 // ---------------------------------------------------------------- one-sided Jacobi SVD
 // Hestenes one-sided Jacobi on the m x n column-major M (ldm): on return M <- M V has
-// mutually orthogonal columns, V (n x n, ldv) holds the right singular vectors, sig[c] the
+// mutually orthogonal columns, V (n x n, ldv; NULL: not formed) holds the right singular vectors, sig[c] the
 // column norms (singular values, unsorted) and perm[0..n) the column order by descending
 // singular value (ties by index).  Round-robin parallel ordering, one warp per pair; squared
 // column norms are computed afresh at the start of every sweep and updated by the rotation
@@ -331,8 +382,9 @@ __device__ inline int cta_jacobi_svd(double* M, int ldm, int m, int n, double* V
   // the doubles' order); two slots, alternating like the flags
   __shared__ unsigned long long s_mx[2];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  for (int j = warp; j < n; j += nwarp)
-    for (int i = lane; i < n; i += 32) V[(size_t)j * ldv + i] = (i == j) ? 1.0 : 0.0;
+  if (V)
+    for (int j = warp; j < n; j += nwarp)
+      for (int i = lane; i < n; i += 32) V[(size_t)j * ldv + i] = (i == j) ? 1.0 : 0.0;
   const int np = (n + 1) & ~1;  // even number of players (one dummy when n is odd)
   // rotate unless the pair is orthogonal to working precision, |cos| <= m eps (the singular
   // values then carry a relative error of order cos^2)
@@ -393,12 +445,14 @@ __device__ inline int cta_jacobi_svd(double* M, int ldm, int m, int n, double* V
               mp[r] = cs * x - sn * y;
               mq[r] = sn * x + cs * y;
             }
-            double* vp = V + (size_t)p * ldv;
-            double* vq = V + (size_t)q * ldv;
-            for (int r = lane; r < n; r += 32) {
-              const double x = vp[r], y = vq[r];
-              vp[r] = cs * x - sn * y;
-              vq[r] = sn * x + cs * y;
+            if (V) {
+              double* vp = V + (size_t)p * ldv;
+              double* vq = V + (size_t)q * ldv;
+              for (int r = lane; r < n; r += 32) {
+                const double x = vp[r], y = vq[r];
+                vp[r] = cs * x - sn * y;
+                vq[r] = sn * x + cs * y;
+              }
             }
             __syncwarp();
             if (lane == 0) {

@@ -619,7 +619,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
       __syncthreads();
     }
     // R2 from Householder QR of the projected X (bi x rj); its reflectors are not needed
-    cta_geqr2(S.X, b, bi, rj, sig, red);
+    cta_geqr2_r(S.X, b, bi, rj, red);
     // V side: D = V_ij^T U_jk, Y = U_jk - V_ij D (twice; the first pass reads U_jk itself)
     if (r1 == 0) {
       for (int v = 0; v < rj; ++v)
@@ -709,7 +709,7 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     // orthogonal columns, sigma = column norms), so M = Q_M W Z^T and the right singular vectors
     // are the normalised columns of Z.  The QR grades the columns, so the Jacobi needs 3-5 sweeps
     // instead of 6-16 on M itself.
-    cta_geqr2(Mc, lc, s, s, sig, red);
+    cta_geqr2_r(Mc, lc, s, s, red);
     for (int e = tid; e < s * s; e += kRcT) {
       const int a = e % s, c = e / s;
       Zc[(size_t)c * lc + a] = (a >= c) ? Mc[(size_t)a * lc + c] : 0.0;
@@ -717,8 +717,8 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     __syncthreads();
     // columns below 1e-14 of the largest singular value (the projections' rounding noise) are not
     // rotated: their relative orthogonality test would otherwise run to the sweep limit
-    cta_jacobi_svd(Zc, lc, s, s, Vc, lc, sig, perm, iflag, 40, 1e-28);
-    // Vc <- normalised Z (right singular vectors of M), in place of the rotation matrix
+    cta_jacobi_svd(Zc, lc, s, s, nullptr, lc, sig, perm, iflag, 40, 1e-28);  // only Z is used
+    // Vc <- normalised Z (right singular vectors of M); the rotation matrix is not formed
     for (int c = warp; c < s; c += kRcW) {
       const double inv = sig[c] > 0.0 ? 1.0 / sig[c] : 0.0;
       for (int a = lane; a < s; a += 32) Vc[(size_t)c * lc + a] = Zc[(size_t)c * lc + a] * inv;
