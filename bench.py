@@ -52,16 +52,19 @@ def parse():
                     help="> 0: instead of the headline, run this many lockstep random-walk chains (the 64-chain "
                          "configuration) for --chain-iters iterations through --workspaces device workspaces")
     ap.add_argument("--workspaces", type=int, default=8)
+    ap.add_argument("--graphs", type=int, default=1,
+                    help="1: forward pass replayed from a CUDA graph (the library default); 0: launches one by one")
     ap.add_argument("--chain-iters", type=int, default=3)
     return ap.parse_args()
 
 
 # k_recompress DRAM traffic per launch at N = 50,000, b = 500, adaptive tau = 0.9 (bytes): the mean of
 # dram__bytes_read.sum + dram__bytes_write.sum over the 98 launches of one evaluation, from an ncu
-# capture of `bench.py --steps 1 --warmup 1 --cpu-sample 0 --plain-steps 0 --batch 1 --dense 0`
-RC_TRAFFIC_N50K = 283.5e6
+# capture of `bench.py --steps 1 --warmup 1 --cpu-sample 0 --plain-steps 0 --batch 1 --dense 0 --graphs 0`
+# (the same kernels launched one by one: ncu's driver reported a failed launch replaying the graph)
+RC_TRAFFIC_N50K = 205.8e6
 RC_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, mean over the 98 k_recompress launches of "
-                     "one evaluation (batch 1, same workload, 1-pass capture)")
+                     "one evaluation (batch 1, same workload, launches one by one, 1-pass capture)")
 METRIC = "TLR loglik+grad evals/s at N=50k vs plain FP64 on B200; |dl| vs FP64 dense"
 
 
@@ -69,7 +72,8 @@ def workload(a):
     return {"workload": f"TLR log-likelihood, N={a.n}, b={a.b}, Matern-3/2 theta=(1,0.3,0.05), adaptive tau={a.tau}",
             "n": a.n, "b": a.b, "rule": "adaptive", "tau": a.tau, "precision": a.precision,
             "theta_per_step": a.batch, "batch": "theta_0 = (1, 0.3, 0.05), the others theta_0 exp(0.05 z), seeded",
-            "l2": "inputs larger than L2 (per-evaluation working set several GB)"}
+            "l2": "inputs larger than L2 (per-evaluation working set several GB)",
+            "forward": "CUDA graph replay" if a.graphs else "launches one by one"}
 
 
 class ClockSampler:
@@ -256,6 +260,7 @@ def main():
         plan = tlr.Plan(a.n, a.b, cap=64, device=local)
         plan.set_data(S, y)
         plan.set_precision("fp64")
+        plan.set_graphs(bool(a.graphs))
         ev64 = plan.evaluate(THETA, "adaptive", a.tau, grad=True)
         barrier()
         torch.cuda.synchronize()
@@ -277,6 +282,8 @@ def main():
     thetas = np.array(THETA)[None, :] * np.exp(0.05 * rng.standard_normal((B, 3)))
     thetas[0] = THETA
     pb = tlr.PlanBatch(a.n, a.b, B, cap=64, device=local, precision=a.precision)
+    for p in pb.plans:
+        p.set_graphs(bool(a.graphs))
     pb.set_data(S, y)
     free_b, total_b = torch.cuda.mem_get_info(local)
     for _ in range(a.warmup):
