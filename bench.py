@@ -44,7 +44,9 @@ def parse():
     ap.add_argument("--plain-steps", type=int, default=-1,
                     help="timed evaluations of the plain FP64 comparison (-1: as many as the batched leg, steps x "
                          "batch; 0: skip)")
-    ap.add_argument("--batch", type=int, default=4, help="parameter vectors per step (one batched call)")
+    ap.add_argument("--batch", type=int, default=8,
+                    help="parameter vectors per step (one batched call, one workspace each: the autotuner's best "
+                         "at N=50k, b=500)")
     ap.add_argument("--dense", type=int, default=1, help="0: skip the dense FP64 oracle")
     ap.add_argument("--sim", choices=["dense", "tlr"], default="dense",
                     help="field from a dense Cholesky, or from a tau = 0.02 TLR factor (large N)")
