@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(kMtThreads) k_digit_scatter(const unsigned* ke
                                                               int ntiles, unsigned* keys_out, unsigned* idx_out,
                                                               long long* perm_out) {
   __shared__ unsigned run[256];                        // pairs of each digit placed by earlier rounds
-  __shared__ unsigned wc[kMtThreads / 32][256];        // this round: pairs of each digit per warp
+  __shared__ unsigned wc[kMtThreads / 32][256];        // this pass: pairs of each digit per warp
   const int tile = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   unsigned lt;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
