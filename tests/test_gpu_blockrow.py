@@ -99,3 +99,28 @@ def test_lockstep_at_n20000_and_capacity_growth(tlr):
     _same(ref, out)
     for p in plans + [single]:
         p.close()
+
+
+def test_lockstep_ragged_tiles_more_ranks_than_rows_and_matern52(tlr):
+    """N = 1,030 with b = 100 (a last block row of 30 sites): 3 ranks, and 13 ranks (more ranks
+    than the 11 block rows: two own nothing); then the Matern 5/2 kernel on 4 ranks."""
+    from adaptive_tlr_pilots_b200 import blockrow
+    d = np.load(os.path.join(GOLD, "n1030_b100_data.npz"))
+    S, y = d["S"], d["y"]
+    theta = (1.0, 0.3, 0.05)
+    single = tlr.Plan(1030, 100)
+    single.set_data(S, y)
+    for world in (3, 13):
+        ref = single.evaluate(theta, "adaptive", 0.9)
+        plans = _plans(tlr, 1030, 100, world, S, y)
+        _same(ref, blockrow.evaluate_lockstep(plans, theta, "adaptive", 0.9))
+        for p in plans:
+            p.close()
+    single.set_kernel(2.5)
+    ref = single.evaluate(theta, "fixed", 1e-6)
+    plans = _plans(tlr, 1030, 100, 4, S, y)
+    for p in plans:
+        p.set_kernel(2.5)
+    _same(ref, blockrow.evaluate_lockstep(plans, theta, "fixed", 1e-6))
+    for p in plans + [single]:
+        p.close()
