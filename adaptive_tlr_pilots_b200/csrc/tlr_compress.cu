@@ -333,16 +333,18 @@ __global__ void __launch_bounds__(kSkW * 32, 1)
       }
       continue;
     }
+    if constexpr (MODE == 0) {  // the sketch's second product; the other modes left above
 #pragma unroll
-    for (int kq = 0; kq < kSkH / 4; ++kq) {
-      double bf[2];
+      for (int kq = 0; kq < kSkH / 4; ++kq) {
+        double bf[2];
 #pragma unroll
-      for (int nt = 0; nt < 2; ++nt) bf[nt] = Ys[(4 * kq + tg) * kSkYs + 8 * nt + g];
+        for (int nt = 0; nt < 2; ++nt) bf[nt] = Ys[(4 * kq + tg) * kSkYs + 8 * nt + g];
 #pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        const double a = Tsl[(size_t)(4 * kq + tg) * kSkPitch + col0 + 8 * m + g];
+        for (int m = 0; m < 4; ++m) {
+          const double a = Tsl[(size_t)(4 * kq + tg) * kSkPitch + col0 + 8 * m + g];
 #pragma unroll
-        for (int nt = 0; nt < 2; ++nt) dmma884(za[m][nt][0], za[m][nt][1], a, bf[nt]);
+          for (int nt = 0; nt < 2; ++nt) dmma884(za[m][nt][0], za[m][nt][1], a, bf[nt]);
+        }
       }
     }
   }
