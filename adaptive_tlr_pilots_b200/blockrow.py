@@ -131,20 +131,25 @@ def rank_steps(steps: RankSteps, theta, rule, value):
 
 class TorchExchange:
     """The exchanges over a torch.distributed process group (NCCL between GPUs; gloo moves CPU
-    tensors).  Ranks are the group's."""
+    tensors).  Ranks are the group's; without an initialised process group, one local rank."""
 
     def __init__(self, group=None):
         import torch.distributed as dist
         self.dist, self.group = dist, group
-        self.rank = dist.get_rank(group)
-        self.world = dist.get_world_size(group)
-        self._into = dist.get_backend(group) == "nccl"
+        self.local = not dist.is_initialized()  # no process group: one rank, every exchange local
+        self.rank = 0 if self.local else dist.get_rank(group)
+        self.world = 1 if self.local else dist.get_world_size(group)
+        self._into = not self.local and dist.get_backend(group) == "nccl"
 
     def _global(self, r):
         return r if self.group is None else self.dist.get_global_rank(self.group, r)
 
     def serve(self, req):
         kind = req[0]
+        if self.local:
+            if kind == "gather":
+                req[1].copy_(req[2])
+            return
         if kind == "bcast":
             self.dist.broadcast(req[1], src=self._global(req[2]), group=self.group)
         elif kind == "gather":

@@ -54,6 +54,8 @@ def parse():
                     help="> 0: instead of the headline, run this many lockstep random-walk chains (the 64-chain "
                          "configuration) for --chain-iters iterations through --workspaces device workspaces")
     ap.add_argument("--workspaces", type=int, default=8)
+    ap.add_argument("--blockrow", type=int, default=0,
+                    help="1: one log-likelihood split over the ranks, block rows cyclic (strong scaling)")
     ap.add_argument("--graphs", type=int, default=1,
                     help="1: forward pass replayed from a CUDA graph (the library default); 0: launches one by one")
     ap.add_argument("--chain-iters", type=int, default=3)
@@ -218,8 +220,54 @@ def run_chains_mode(a):
                       "device_used_gb": (total_b - free_b) / 1e9, "device_gb": total_b / 1e9}), flush=True)
 
 
+def run_blockrow_mode(a):
+    """One FP64 log-likelihood at the workload's size split over the ranks (blockrow.py: block row i
+    on rank i % world, one broadcast and one all-gather per step); every rank evaluates the same
+    theta and gets the same value.  Timed on the device, max over ranks; `value` = evaluations per
+    second of the whole job (strong scaling: the work per evaluation is fixed)."""
+    import torch
+
+    import adaptive_tlr_pilots_b200 as tlr
+    from adaptive_tlr_pilots_b200 import blockrow, synth
+    from adaptive_tlr_pilots_b200.replicas import Replicas
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    rep = Replicas("nccl")
+    S, y, _, _ = synth.simulate_field(a.n, THETA, device=local)
+    torch.cuda.empty_cache()
+    plan = tlr.Plan(a.n, a.b, cap=64, device=local)
+    plan.set_data(S, y)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(a.warmup):
+        ev = blockrow.evaluate_distributed(plan, THETA, "adaptive", a.tau)
+    rep.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(a.steps):
+        ev = blockrow.evaluate_distributed(plan, THETA, "adaptive", a.tau)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = rep.max_over_ranks(e0.elapsed_time(e1)) / a.steps
+    if rep.rank == 0:
+        print(json.dumps({"metric": "TLR log-likelihood evals/s, one evaluation over all GPUs (block rows cyclic)",
+                          "value": 1e3 / ms, "unit": "evals/s", "n_gpus": rep.world, "steps": a.steps,
+                          "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "config": {**{k: v for k, v in workload(a).items()
+                                        if k not in ("theta_per_step", "batch", "forward", "precision")},
+                                     "precision": "fp64", "parallelism": f"block-row cyclic x{rep.world}"},
+                          "loglik": ev.loglik, "stored_factor": ev.info.get("stored_factor")}), flush=True)
+    plan.close()
+    rep.close()
+
+
 def main():
     a = parse()
+    if a.blockrow:
+        run_blockrow_mode(a)
+        return
     if a.chains > 0:
         run_chains_mode(a)
         return

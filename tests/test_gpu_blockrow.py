@@ -124,3 +124,35 @@ def test_lockstep_ragged_tiles_more_ranks_than_rows_and_matern52(tlr):
     _same(ref, blockrow.evaluate_lockstep(plans, theta, "fixed", 1e-6))
     for p in plans + [single]:
         p.close()
+
+
+def test_distributed_driver_over_nccl_single_rank(tlr):
+    """evaluate_distributed through a real NCCL process group (one rank: broadcast,
+    all_gather_into_tensor and all_reduce on the device buffers), against the single plan."""
+    import socket
+    from datetime import timedelta
+
+    import torch
+    import torch.distributed as dist
+
+    from adaptive_tlr_pilots_b200 import blockrow
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=timedelta(seconds=120), device_id=torch.device("cuda", 0))
+    try:
+        d = np.load(os.path.join(GOLD, "n4000_b250_data.npz"))
+        S, y = d["S"], d["y"]
+        single = tlr.Plan(4000, 250)
+        single.set_data(S, y)
+        ref = single.evaluate((1.0, 0.3, 0.05), "adaptive", 0.9)
+        plan = tlr.Plan(4000, 250)
+        plan.set_data(S, y)
+        ex = blockrow.TorchExchange()
+        assert not ex.local and ex.world == 1
+        _same(ref, [blockrow.evaluate_distributed(plan, (1.0, 0.3, 0.05), "adaptive", 0.9)])
+        plan.close()
+        single.close()
+    finally:
+        dist.destroy_process_group()
