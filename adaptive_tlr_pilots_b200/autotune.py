@@ -12,6 +12,10 @@ takes the fastest entry for the nearest N with the same b, or falls back to min(
 No counterpart in the reference (it evaluates one parameter vector at a time).
 
 Usage:  python -m adaptive_tlr_pilots_b200.autotune --n 50000 --b 500   (writes tuning.json)
+        python -m adaptive_tlr_pilots_b200.autotune --n 50000 --b 250,500,1000 --candidates 4,8
+        (one entry per tile size, each with its log-likelihood at theta_0 and its stored factor:
+        tile_sizes() lists them; the tile size changes the approximation, so it is reported, not
+        chosen silently)
 """
 from __future__ import annotations
 
@@ -92,19 +96,43 @@ def tune_workspaces(S, y, b, candidates=(1, 2, 4, 6, 8), rule="adaptive", value=
             torch.cuda.empty_cache()
     if not rates:
         raise RuntimeError("no workspace count fitted the device")
+    # what the tile size does to the approximation at theta_0 (the tile size is the caller's
+    # modelling choice: the table reports, it does not pick b)
+    from .tlr import Plan
+    plan = Plan(n, b, device=device)
+    plan.set_precision(precision)
+    plan.set_data(S, y)
+    ev = plan.evaluate(theta0, rule, value)
+    plan.close()
+    torch.cuda.empty_cache()
     entry = dict(n=n, b=int(b), rule=rule, value=float(value), precision=precision,
                  evals_per_s={str(k): v for k, v in rates.items()}, best=int(max(rates, key=rates.get)),
-                 gpu=torch.cuda.get_device_name(device))
+                 gpu=torch.cuda.get_device_name(device), loglik_theta0=ev.loglik,
+                 stored_factor=ev.info.get("stored_factor"), mean_rank_factor=ev.info.get("mean_rank_factor"),
+                 max_rank_factor=ev.info.get("max_rank_factor"))
     table = load_table(path)
     table[_key(n, b, rule, value, precision)] = entry
     json.dump(table, open(path, "w"), indent=1, sort_keys=True)
     return entry
 
 
+def tile_sizes(n, rule="adaptive", value=0.9, precision="mixed", path=TABLE):
+    """{b: (best evals/s, loglik at theta_0, stored factor values)} of every tuned tile size at the
+    nearest tuned N, for choosing b knowingly: b changes the approximation as well as the speed."""
+    table = load_table(path)
+    rows = [e for e in table.values() if e["rule"] == rule and e["precision"] == precision
+            and abs(e["value"] - float(value)) <= 1e-12]
+    if not rows:
+        return {}
+    n0 = min({e["n"] for e in rows}, key=lambda m: abs(np.log(m / float(n))))
+    return {e["b"]: (max(e["evals_per_s"].values()), e.get("loglik_theta0"), e.get("stored_factor"))
+            for e in rows if e["n"] == n0}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=50000)
-    ap.add_argument("--b", type=int, default=500)
+    ap.add_argument("--b", default="500", help="tile size, or several separated by commas")
     ap.add_argument("--tau", type=float, default=0.9)
     ap.add_argument("--precision", default="mixed")
     ap.add_argument("--candidates", default="1,2,4,6,8")
@@ -112,9 +140,10 @@ def main():
     a = ap.parse_args()
     from . import synth
     S, y, _, _ = synth.simulate_field(a.n, (1.0, 0.3, 0.05))
-    entry = tune_workspaces(S, y, a.b, candidates=tuple(int(c) for c in a.candidates.split(",")),
-                            value=a.tau, precision=a.precision, steps=a.steps)
-    print(json.dumps(entry))
+    for b in (int(v) for v in a.b.split(",")):
+        entry = tune_workspaces(S, y, b, candidates=tuple(int(c) for c in a.candidates.split(",")),
+                                value=a.tau, precision=a.precision, steps=a.steps)
+        print(json.dumps(entry), flush=True)
 
 
 if __name__ == "__main__":
