@@ -18,6 +18,7 @@ TLR_RULE_MIXED = 2
 PRECISIONS = {"fp64": 0, "mixed": 1}
 RANK_MAP = {"rule": 0, "record": 1, "replay": 2}
 ERR_RANK_CAP = -2  # TLR_ERR_RANK_CAP: a tile rank exceeded the plan's capacity
+ERR_NOMEM = -4  # TLR_ERR_NOMEM: a device allocation failed
 DIST_DIAG, DIST_PANEL, DIST_SUMS = 0, 1, 2  # tlr_dist_buffer_doubles: the three exchange buffers
 
 _lib = None

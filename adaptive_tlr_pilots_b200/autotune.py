@@ -26,6 +26,8 @@ import time
 
 import numpy as np
 
+from . import _lib
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuning.json")
 DEFAULT_WORKSPACES = 4
@@ -91,6 +93,9 @@ def tune_workspaces(S, y, b, candidates=(1, 2, 4, 6, 8), rule="adaptive", value=
                 pb.evaluate(thetas, rule, value)
             torch.cuda.synchronize(device)
             rates[w] = w * steps / (time.perf_counter() - t0)
+        except _lib.TlrError as e:  # a workspace's arena did not fit beside the others
+            if e.code != _lib.ERR_NOMEM:
+                raise
         finally:
             pb.close()
             torch.cuda.empty_cache()
