@@ -220,7 +220,9 @@ def evaluate_distributed(plan: Plan, theta, rule, value, group=None) -> Evaluati
     """The TLR log-likelihood of `plan`'s data over the ranks of a torch.distributed group, block
     rows cyclic over the ranks.  Every rank calls this with its own plan (same n, b, data, theta)
     and receives the same Evaluation.  A tile rank above the capacity grows every rank's plan (the
-    failure reaches all ranks) and the evaluation is repeated."""
+    failure reaches all ranks) and the evaluation is repeated.  Any other error raises on the rank
+    that met it; the other ranks then wait in their next collective until the process group's
+    timeout ends it (create the group with a short timeout)."""
     ex = TorchExchange(group)
     while True:
         steps = _steps_for(plan, ex.rank, ex.world)
