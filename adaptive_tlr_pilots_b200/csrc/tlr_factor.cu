@@ -311,15 +311,11 @@ __device__ void cta_atb(const double* A, int lda, const double* B, int ldb, int 
   }
 }
 
-// C[v][u] = (sum_t A[u][t] B[v][t]) (times scale[u] when scale is given) for u < p, v < q, column v
-// of C at C + v ldc.  One warp per (u, four consecutive v), so A's column is read once for four
-// dots; every entry is summed as in cta_atb (lane t = lane, lane + 32, ..., then the butterfly),
-// so the results are cta_atb's bit for bit.
-__device__ void cta_atb4(const double* A, int lda, const double* B, int ldb, int m, int p, int q, double* C,
-                         int ldc, const double* scale) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  const int nq = (q + 3) >> 2;
-  for (int e = warp; e < p * nq; e += nwarp) {
+// One task of cta_atb4 (task e of p * ceil(q / 4): row u of C, four consecutive columns), by one warp.
+__device__ __forceinline__ void atb4_task(const double* A, int lda, const double* B, int ldb, int m, int p, int q,
+                                          double* C, int ldc, const double* scale, int e) {
+  const int lane = threadIdx.x & 31;
+  {
     const int u = e % p, v0 = (e / p) * 4;
     const double* a = A + (size_t)u * lda;
     const double* b0 = B + (size_t)v0 * ldb;
@@ -346,6 +342,17 @@ __device__ void cta_atb4(const double* A, int lda, const double* B, int ldb, int
       if (v0 + 3 < q) C[(size_t)(v0 + 3) * ldc + u] = scale ? s3 * sc : s3;
     }
   }
+}
+
+// C[v][u] = (sum_t A[u][t] B[v][t]) (times scale[u] when scale is given) for u < p, v < q, column v
+// of C at C + v ldc.  One warp per (u, four consecutive v), so A's column is read once for four
+// dots; every entry is summed as in cta_atb (lane t = lane, lane + 32, ..., then the butterfly),
+// so the results are cta_atb's bit for bit.
+__device__ void cta_atb4(const double* A, int lda, const double* B, int ldb, int m, int p, int q, double* C,
+                         int ldc, const double* scale) {
+  const int warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int ntask = p * ((q + 3) >> 2);
+  for (int e = warp; e < ntask; e += nwarp) atb4_task(A, lda, B, ldb, m, p, q, C, ldc, scale, e);
 }
 
 // General recompression of one trailing pair, the reference's recompress as written
@@ -549,8 +556,14 @@ __global__ void __launch_bounds__(kRcT, kRcMinBlocks) k_recompress(int n, int b,
     const int lc = core_in_smem ? kRcSmemS : ls;
     __syncthreads();
     // W = V_ik^T V_jk (ri x rj); column norms of U_ij
-    cta_atb4(Vik, b, Vjk, b, bk, ri, rj, S.W, cap, nullptr);
-    for (int c = warp; c < r1; c += kRcW) {
+    // W's dot tasks and the column norms share one round-robin over the warps
+    const int nW = ri * ((rj + 3) >> 2);
+    for (int e = warp; e < nW + r1; e += kRcW) {
+      if (e < nW) {
+        atb4_task(Vik, b, Vjk, b, bk, ri, rj, S.W, cap, nullptr, e);
+        continue;
+      }
+      const int c = e - nW;
       const double* u = Uij + (size_t)c * b;
       const double* v = Vij + (size_t)c * b;
       double a = 0.0, av = 0.0;
