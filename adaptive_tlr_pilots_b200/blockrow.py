@@ -44,10 +44,11 @@ class RankSteps:
         n_panel = int(lib.tlr_dist_buffer_doubles(h, _lib.DIST_PANEL, -1))
         n_sums = int(lib.tlr_dist_buffer_doubles(h, _lib.DIST_SUMS, 0))
         kw = dict(dtype=torch.float64, device=plan.dev)
-        self.diag = torch.zeros(n_diag, **kw)
-        self.panel = torch.zeros(n_panel, **kw)
-        self.gathered = torch.zeros(n_panel * self.world, **kw)
-        self.sums = torch.zeros(n_sums, **kw)
+        with torch.cuda.stream(plan.stream):  # filled on the stream the library then writes them on
+            self.diag = torch.zeros(n_diag, **kw)
+            self.panel = torch.zeros(n_panel, **kw)
+            self.gathered = torch.zeros(n_panel * self.world, **kw)
+            self.sums = torch.zeros(n_sums, **kw)
 
     def owner(self, k: int) -> int:
         return k % self.world
@@ -176,15 +177,19 @@ def run_rank(gen, exchange):
         return stop.value
 
 
-def run_lockstep(gens):
+def run_lockstep(gens, sync=False):
     """Drive the generators of all ranks in one process: each exchange is served by copies once
-    every rank has issued it.  Returns the ranks' results."""
+    every rank has issued it (on the current stream; with sync, between two device-wide
+    synchronisations, for ranks on different streams).  Returns the ranks' results."""
     world = len(gens)
     reqs = [next(g) for g in gens]
     while True:
         kinds = {r[0] for r in reqs}
         if len(kinds) != 1:
             raise RuntimeError(f"ranks out of step: {sorted(kinds)}")
+        fence = sync and reqs[0][1].device.type == "cuda"
+        if fence:
+            _torch().cuda.synchronize()
         kind = reqs[0][0]
         if kind == "bcast":
             src = reqs[0][2]
@@ -202,6 +207,8 @@ def run_lockstep(gens):
                 total += r[1]
             for r in reqs:
                 r[1].copy_(total)
+        if fence:
+            _torch().cuda.synchronize()
         results, nxt, done = [None] * world, [None] * world, 0
         for w, g in enumerate(gens):
             try:
@@ -227,7 +234,10 @@ def evaluate_distributed(plan: Plan, theta, rule, value, group=None) -> Evaluati
     while True:
         steps = _steps_for(plan, ex.rank, ex.world)
         try:
-            return run_rank(rank_steps(steps, theta, rule, value), ex)
+            # the collectives are ordered on the plan's stream (torch's NCCL calls wait for the
+            # current stream and make it wait for them)
+            with _torch().cuda.stream(plan.stream):
+                return run_rank(rank_steps(steps, theta, rule, value), ex)
         except _lib.TlrError as e:
             if e.code != _lib.ERR_RANK_CAP or not plan.grow():
                 raise
@@ -236,11 +246,16 @@ def evaluate_distributed(plan: Plan, theta, rule, value, group=None) -> Evaluati
 def evaluate_lockstep(plans, theta, rule, value):
     """The same factorization with len(plans) ranks in one process (every plan partitioned as one
     rank): the ranks' steps interleaved, the exchanges device copies.  Returns the ranks' results."""
+    torch = _torch()
     world = len(plans)
+    shared = len({p.stream for p in plans}) == 1
     while True:
         steps = [_steps_for(p, r, world) for r, p in enumerate(plans)]
         try:
-            return run_lockstep([rank_steps(s, theta, rule, value) for s in steps])
+            if shared:  # one stream orders the plans' launches and the copies between them
+                with torch.cuda.stream(plans[0].stream):
+                    return run_lockstep([rank_steps(s, theta, rule, value) for s in steps])
+            return run_lockstep([rank_steps(s, theta, rule, value) for s in steps], sync=True)
         except _lib.TlrError as e:
             if e.code != _lib.ERR_RANK_CAP or not all(p.grow() for p in plans):
                 raise

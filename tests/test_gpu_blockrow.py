@@ -156,3 +156,27 @@ def test_distributed_driver_over_nccl_single_rank(tlr):
         single.close()
     finally:
         dist.destroy_process_group()
+
+
+def test_lockstep_plans_on_their_own_streams(tlr):
+    """Ranks whose plans were created on different streams: the exchanges are fenced by
+    device-wide synchronisations, and the result is still the single plan's."""
+    import torch
+
+    from adaptive_tlr_pilots_b200 import blockrow
+    d = np.load(os.path.join(GOLD, "n4000_b250_data.npz"))
+    S, y = d["S"], d["y"]
+    single = tlr.Plan(4000, 250)
+    single.set_data(S, y)
+    ref = single.evaluate((1.0, 0.3, 0.05), "adaptive", 0.9)
+    plans = []
+    for _ in range(3):
+        with torch.cuda.stream(torch.cuda.Stream()):
+            p = tlr.Plan(4000, 250)
+            p.set_data(S, y)
+        plans.append(p)
+    torch.cuda.synchronize()
+    assert len({p.stream for p in plans}) == 3
+    _same(ref, blockrow.evaluate_lockstep(plans, (1.0, 0.3, 0.05), "adaptive", 0.9))
+    for p in plans + [single]:
+        p.close()
