@@ -176,10 +176,14 @@ class Plan:
             pass
 
     def set_data(self, S, y):
-        """Load Morton-ordered sites and observations (numpy or torch) onto the device."""
+        """Load Morton-ordered sites and observations (numpy or torch) onto the device.  The copies
+        run on the plan's stream after the work queued so far on the current stream (which may
+        have produced device inputs)."""
         torch = _torch()
-        S_t = torch.as_tensor(S, dtype=torch.float64).to(self.dev).contiguous()
-        y_t = torch.as_tensor(y, dtype=torch.float64).to(self.dev).contiguous()
+        self.stream.wait_stream(torch.cuda.current_stream(self.dev))
+        with torch.cuda.stream(self.stream):
+            S_t = torch.as_tensor(S, dtype=torch.float64).to(self.dev).contiguous()
+            y_t = torch.as_tensor(y, dtype=torch.float64).to(self.dev).contiguous()
         if S_t.shape != (self.n, 2) or y_t.shape != (self.n,):
             raise ValueError(f"expected S of shape ({self.n}, 2) and y of shape ({self.n},)")
         self._data = (S_t, y_t)
