@@ -1030,10 +1030,12 @@ int tlr_loglik_grad_batch(tlr_plan* const* plans, int count, const double* theta
     if (rc < 0 && !first_error) first_error = rc;
     st[q] = rc;
     if (loglik) loglik[q] = ll;
+    // each backward pass is queued as soon as its forward pass is done, beside the later plans'
+    // forward passes (after an error none is queued; those already queued finish on their streams)
+    if (!first_error && rc == 0)
+      TRY(run_backward(plans[q], thetas[3 * q], 1.0 / thetas[3 * q + 1], thetas[3 * q + 2]));
   }
   if (first_error) return first_error;
-  for (int q = 0; q < count; ++q)
-    if (st[q] == 0) TRY(run_backward(plans[q], thetas[3 * q], 1.0 / thetas[3 * q + 1], thetas[3 * q + 2]));
   for (int q = 0; q < count; ++q) {
     if (st[q] != 0) continue;
     double g[3];
